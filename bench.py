@@ -1,0 +1,320 @@
+"""Benchmark of the sparse D3Q19 MRT single-phase update on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): 256^3 overlapping-sphere mask, sphere radius uniform in
+4-10 lu, porosity 0.35, seed 20260101; periodic, tau = 0.8 (nu = 0.1),
+gx = 1e-6; populations stored as FP32 deviations f_i - w_i, FP32 collision
+arithmetic.  A step is one fused collide + pull-stream pass over every fluid
+node.  Inputs (2 x 19 x 4 B x 5.87 M nodes + table) are far larger than the
+126 MB L2, so no flush is needed between steps.
+
+value  fluid MLUPS, device-resident, CUDA events on the solver's stream
+       around the K timed steps, max over ranks; N ranks run N independent
+       replicas (the single-domain path has no data exchange: weak scaling).
+e2e    the same metric through the C ABI from host memory: lbm_create from
+       the host mask (compaction, table, upload), K steps with a diagnostics
+       read-back (lbm_reduce) every 100 steps, and lbm_get_fields of rho/u to
+       the host, all inside the timed region.
+roofline  achieved = (2*19*4 + 18*4) B per fluid update x nodes / step time,
+          against the measured HBM copy bandwidth.
+--impl reference  times the reference solver (SP3, compiled from its own
+       source with -O3 -march=native, oracle/_ref/libref_sp3_fast.so) on the
+       host cores: one process per core, each on a 64^3 sub-block of the same
+       geometry (a bounded sample of the workload).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "jianhui-lbm_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "fluid MLUPS (sparse D3Q19 MRT, FP32 deviation storage)"
+SHAPE = (256, 256, 256)
+PHI, RADIUS, SEED = 0.35, (4.0, 10.0), 20260101
+NU, GX = 0.1, 1e-6
+BYTES_PER_LU = 2 * 19 * 4 + 18 * 4
+
+
+def workload_mask():
+    from lbm_b200 import geometry as G
+
+    return G.overlapping_spheres(SHAPE, PHI, RADIUS, SEED)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch of the step kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "sp_step_f32_256cube.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch_full:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allmax(pg, x):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ------------------------------------------------------------ reference arm
+def _ref_worker(args):
+    sub, steps, warm = args
+    import oracle
+
+    ref = oracle.ReferenceSP3(fast=True)
+    count = ref.create(sub, NU, (GX, 0.0, 0.0), binary=True)
+    ref.step(warm)
+    t0 = time.perf_counter()
+    ref.step(steps)
+    return count, time.perf_counter() - t0
+
+
+def reference_sample(mask, steps, warmup, procs=None, edge=64):
+    """Reference SP3 (-O3 -march=native) on `procs` host cores, each process on
+    its own edge^3 periodic sub-block of the workload geometry."""
+    import multiprocessing as mp
+
+    try:
+        ncpu = len(os.sched_getaffinity(0))
+    except AttributeError:
+        ncpu = os.cpu_count() or 1
+    procs = procs or ncpu
+    nz, ny, nx = mask.shape
+    blocks = []
+    per = max(nx // edge, 1)
+    for b in range(procs):
+        i, j, k = b % per, (b // per) % per, (b // (per * per)) % per
+        sub = np.ascontiguousarray(mask[k * edge:(k + 1) * edge, j * edge:(j + 1) * edge, i * edge:(i + 1) * edge])
+        blocks.append((sub, steps, warmup))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, blocks)
+    wall = time.perf_counter() - t0
+    lu = sum(c for c, _ in res) * steps
+    tmax = max(t for _, t in res)
+    return {"value": lu / tmax / 1e6, "unit": "MLUPS", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x {edge}^3 sub-blocks of the workload geometry, {steps} steps each "
+                      f"after {warmup} warm-up; SP3 built -O3 -march=native; slowest process timed",
+            "wall_s": wall}
+
+
+def run_reference(a):
+    world, rank, local, pg = dist_setup()
+    if rank != 0:
+        return 0
+    import oracle
+
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference solver library oracle/_ref not built"}))
+        return 0
+    mask = workload_mask()
+    cb = reference_sample(mask, a.steps, a.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "256^3 overlapping spheres r=U[4,10], phi=0.35, tau=0.8, gx=1e-6 (bounded sample)",
+                       "sample": cb["sample"]},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------ our arm
+def run_ours(a):
+    world, rank, local, pg = dist_setup()
+    import lbm_b200
+
+    mask = workload_mask()
+    # pick ordering / block size once (not timed), then build the timed solver with them
+    tune = {}
+    with lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering="reference", device=local) as s0:
+        tune = s0.autotune(trial_steps=10)
+    order, block = tune["ordering"], tune["block"]
+
+    s = lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering=order, block_size=block, device=local)
+    count = s.count
+    s.step(a.warmup)
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        s.step(a.steps)  # lbm_step times the K steps with CUDA events on its stream
+    ms = s.last_step_ms()
+    diag = s.reduce()
+    s.close()
+    ms_max = allmax(pg, ms)
+    ms_step = ms_max / a.steps
+    value = world * count * a.steps / (ms_max * 1e-3) / 1e6
+
+    # end to end through the C ABI from host buffers
+    barrier(pg)
+    t0 = time.perf_counter()
+    e = lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering=order, block_size=block, device=local)
+    left, reads = a.steps, 0
+    while left > 0:
+        k = min(100, left)
+        e.step(k)
+        e.reduce()
+        reads += 1
+        left -= k
+    rho, u = e.fields()
+    t_e2e = time.perf_counter() - t0
+    npad = ((count + 255) // 256) * 256
+    e.close()
+    t_e2e = allmax(pg, t_e2e)
+    e2e_value = world * count * a.steps / t_e2e / 1e6
+    h2d = 18 * npad * 4 + count * 4  # pull table + node order
+    d2h = reads * 64 + rho.nbytes + u.nbytes
+
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_LU * count / (ms_step * 1e-3) / 1e9
+    traffic = profiled_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "256^3 overlapping spheres r=U[4,10], phi=0.35, seed 20260101, tau=0.8, gx=1e-6, "
+                               "FP32 deviation storage",
+                   "fluid_nodes": count, "ordering": order, "block": block, "parallelism": f"replicas x{world}",
+                   "l2": "inputs > L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind, "bytes_per_lu": BYTES_PER_LU},
+        "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d / a.steps,
+                "d2h_bytes_per_step": d2h / a.steps, "wall_s": t_e2e},
+        "gpu_launches": a.steps,
+        "clocks": clk.summary(),
+        "perm_x": diag["perm"][0],
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        try:
+            cb = reference_sample(mask, steps=a.cpu_steps, warmup=1)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as ex:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unavailable": str(ex)[:200]}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

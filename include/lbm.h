@@ -1,0 +1,232 @@
+/*
+ * lbm.h -- C ABI of liblbm.so, a B200 (sm_100a) implementation of the sparse
+ * D3Q19 MRT lattice Boltzmann update of the jianhui-lbm suite.
+ *
+ * The reference exposes no library API: each solver is one C++ program whose
+ * hot path is a pair of void functions over globals.  Every entry point below
+ * states which reference code it replaces (paths relative to the reference
+ * project root).  Abbreviations:
+ *   SP  = Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars.cpp
+ *   SP3 = Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
+ *   CG3 = MP_3D/Multi_Component_CG_MPI_SPARSE_Software_3DPartition.cpp
+ *   CG  = MP_3D/Multi_Component_CG_MPI_SPARSE_Software.cpp
+ *   ST7 = Single_Phase_3D/Solute_Transport_MPI_Software_Spars_6V.cpp
+ *
+ * Conventions
+ *   - Status: every function returns lbm_status (0 = OK, negative = error);
+ *     lbm_last_error() gives the message of the last failure on that thread.
+ *     Nothing calls exit() (the reference exits on a missing geometry file,
+ *     SP3:941-949).
+ *   - Ownership: a handle owns all device memory it allocates; caller buffers
+ *     are host memory and are copied synchronously.
+ *   - Node ids and layouts in and out of the library are the reference's:
+ *     fluid ids are 1-based in SP3 compaction order, row 0 is an unused dummy
+ *     row; populations are AoS double[(count+1)*19]; velocity double[(count+1)*3].
+ *   - Masks are uint8 [nz][ny][nx] (x fastest), 0 = pore, non-zero = solid,
+ *     the token order of the reference's ASCII geometry file.
+ *   - Threading: one handle is used by one host thread at a time and runs on
+ *     its own CUDA stream; distinct handles may run concurrently.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+typedef int lbm_status;
+enum {
+  LBM_OK = 0,
+  LBM_ERR_ARG = -1,            /* invalid argument or size */
+  LBM_ERR_IO = -2,             /* file missing / unreadable / short */
+  LBM_ERR_OOM = -3,            /* device or host allocation failed */
+  LBM_ERR_CUDA = -4,           /* CUDA runtime error */
+  LBM_ERR_NAN = -5,            /* non-finite velocity detected (SP3:733) */
+  LBM_ERR_NOT_CONVERGED = -6,  /* step cap reached before the tolerance */
+  LBM_ERR_FORMAT = -7,         /* malformed INPUT*.dat or geometry */
+  LBM_ERR_STATE = -8,          /* call not valid in the handle's state */
+  LBM_ERR_OVERSPEED = -9,      /* u_max >= 10 five times (SP3:722, 734) */
+  LBM_ERR_NO_DEVICE = -10      /* no CUDA device / kernel image */
+};
+
+typedef enum {
+  LBM_PREC_F64 = 0,       /* FP64, bit-exact with the reference's collision */
+  LBM_PREC_F32 = 1,       /* FP32 deviation storage f_i - w_i, FP32 math */
+  LBM_PREC_F16 = 2,       /* FP16 scaled-deviation storage, FP32 math */
+  LBM_PREC_F64_FAST = 3   /* FP64 deviation storage, sparse FMA moments */
+} lbm_precision;
+
+typedef enum {
+  LBM_ORDER_REFERENCE = 0, /* SP3 compaction order (x fastest) */
+  LBM_ORDER_MORTON = 1,    /* Z-order curve over (x,y,z) */
+  LBM_ORDER_HILBERT = 2,   /* 3-D Hilbert curve */
+  LBM_ORDER_BRICK = 3,     /* 16x4x4 bricks, x fastest inside, bricks x fastest */
+  LBM_ORDER_AUTO = -1      /* picked by lbm_autotune */
+} lbm_ordering;
+
+/* Run parameters of the single-phase solver (the physics subset of INPUT.dat,
+ * SP3:283-338).  lbm_params_default() fills reference defaults. */
+typedef struct lbm_params {
+  double nu;          /* kinematic viscosity in_vis; tau = 3 nu + 0.5 (SP3:1289-1296) */
+  double gx, gy, gz;  /* body force as acceleration (SP3:1423-1500) */
+  double u_init[3];   /* initial velocity inivx..inivz (SP3:1331-1333) */
+  int precision;      /* lbm_precision */
+  int ordering;       /* lbm_ordering (LBM_ORDER_AUTO allowed) */
+  int block_size;     /* threads per block; 0 = default, autotune may change */
+  int perdir;         /* PerDir 1..3: permeability direction (SP3:3560-3570) */
+  int window[6];      /* per_xn,per_xp,per_yn,per_yp,per_zn,per_zp; all -1 = whole box */
+  double fp16_scale;  /* LBM_PREC_F16 storage scale; 0 = derived from nu and |g| */
+  int device;         /* CUDA device ordinal */
+} lbm_params;
+
+/* Diagnostics of one reporting step: Error (SP3:3118-3196) and
+ * Comput_Perm (SP3:3518-3648) at the current state. */
+typedef struct lbm_diag {
+  long long step;        /* time steps completed */
+  double perm[3];        /* Q_d / V * nu / g_d (lattice units) */
+  double perm_rel_change;/* (k - k_prev)/k_prev along perdir */
+  double u_ave;          /* |Q| / (V * porosity) -- the convergence quantity */
+  double u_max;          /* max |u| over nodes 1..count-1 */
+  double u_rel_change;   /* ||u - u_prev|| / ||u|| over nodes 1..count-1 */
+  double u_mean_speed;   /* sum |u| / (V * porosity) over nodes 1..count-1 */
+  double mass;           /* sum rho over all fluid nodes */
+  double porosity;       /* pore fraction of the window */
+  int nan_detected;      /* 1 when u_rel_change is NaN (SP3:733) */
+  int converged;         /* set by lbm_run_to_convergence */
+} lbm_diag;
+
+typedef struct lbm_handle lbm_handle;
+
+/* ---------------------------------------------------------------- basics */
+LBM_API const char* lbm_last_error(void);
+LBM_API const char* lbm_status_string(lbm_status s);
+LBM_API int lbm_abi_version(void);
+LBM_API void lbm_params_default(lbm_params* p);
+
+/* ------------------------------------------------- input formats (SP3 L0/L1) */
+
+/* The INPUT.dat / INPUT_Partition.dat parameter file of the single-phase
+ * solvers, every field in the file's line order (SP3:283-340: one value group
+ * per line followed by a comment; NX..NZ stored as given, not minus one). */
+typedef struct lbm_input {
+  char geometry_file[128];
+  int nx, ny, nz;
+  int n_max;
+  double reso;
+  int in_bc;
+  double gx, gy, gz;
+  int pre_xp; double p_xp; int pre_xn; double p_xn;
+  int pre_yp; double p_yp; int pre_yn; double p_yn;
+  int pre_zp; double p_zp; int pre_zn; double p_zn;
+  int vel_xp; double v_xp; int vel_xn; double v_xn;
+  int vel_yp; double v_yp; int vel_yn; double v_yn;
+  int vel_zp; double v_zp; int vel_zn; double v_zn;
+  double in_vis;
+  double inivx, inivy, inivz;
+  int wr_per, perdir, fre_re, out_mode, fre_ve, fre_de;
+  int lattice_v; double dx_input, dt_input;
+  char output_path[128];
+  int sub_bc, loc_perm;
+  int par_per_x, par_per_y, par_per_z;
+  int per_xp, per_xn, per_yp, per_yn, per_zp, per_zn;
+  int fre_backup, mode_backup_ini, vel_sol;
+  int gperm, n_gperm[4], size_gperm[4], c_gperm[4][3];
+  int decbin;
+  int nnf_module; double nnf_m, nnf_n;
+} lbm_input;
+
+/* Parses a single-phase INPUT file (replaces the rank-0 reader SP3:283-340). */
+LBM_API lbm_status lbm_read_input(const char* path, lbm_input* out);
+
+/* Reads a geometry file into a uint8 [nz][ny][nx] mask (0 pore, 1 solid).
+ * decbin 0: ASCII tokens in x-fastest order, non-zero = solid (SP3:929-943);
+ * decbin 1: int32 C-order [i][j][k] (SP3:947-961). */
+LBM_API lbm_status lbm_read_mask(const char* path, int nx, int ny, int nz, int decbin, uint8_t* mask_out);
+
+/* ------------------------------------------------ single-phase solver (SP3) */
+
+/* Builds the fluid-node compaction (SP3:1018-1071), the pull neighbour table
+ * with halfway bounce-back resolved (equivalent of nei_loc, SP3:1099-1151),
+ * the MRT constants (Comput_MI SP3:838, init SP3:1278) and the device state.
+ * The mask is copied; the caller keeps ownership. */
+LBM_API lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, int nz,
+                      lbm_handle** out);
+
+/* Reads INPUT.dat and its geometry file and creates the solver (main SP3:258-555
+ * at one rank).  Unsupported INPUT features (pressure/velocity boundaries,
+ * non-Newtonian module) return LBM_ERR_ARG. */
+LBM_API lbm_status lbm_create_from_input(const char* input_path, int precision, int ordering,
+                                 lbm_handle** out, lbm_input* parsed_out);
+
+LBM_API void lbm_destroy(lbm_handle* h);
+
+/* Advances nsteps time steps: each is collision (SP3:1398-1819) + streaming +
+ * comput_macro_variables (SP3:2401-2446), fused into one kernel per step. */
+LBM_API lbm_status lbm_step(lbm_handle* h, int nsteps);
+
+/* Diagnostics at the current state (Error + Comput_Perm, SP3:712-713).  The
+ * velocity change is measured against the velocity one step earlier, exactly
+ * like the reference's u0 (comput_macro_variables saves u0 every step). */
+LBM_API lbm_status lbm_reduce(lbm_handle* h, lbm_diag* out);
+
+/* Runs until |(u_ave_prev - u_ave)/u_ave_prev| < tol at a check every
+ * check_every steps (the SP stop test SP:812-816, u_ave from Comput_Perm),
+ * or max_steps.  Returns LBM_OK when converged, LBM_ERR_NOT_CONVERGED at the
+ * cap, LBM_ERR_NAN / LBM_ERR_OVERSPEED on the reference's stop conditions. */
+LBM_API lbm_status lbm_run_to_convergence(lbm_handle* h, double tol, int check_every, int max_steps,
+                                  lbm_diag* out);
+
+/* Number of fluid nodes (the reference's Count) and geometry facts. */
+LBM_API lbm_status lbm_info(lbm_handle* h, int* count, double* porosity, long long* step);
+
+/* rho[(count+1)] and u[(count+1)*3] in reference id order (row 0 zero);
+ * either pointer may be NULL.  Same values comput_macro_variables leaves in
+ * the reference's rho/u arrays. */
+LBM_API lbm_status lbm_get_fields(lbm_handle* h, double* rho, double* u);
+
+/* Post-streaming populations f[(count+1)*19], reference id order -- the
+ * reference's f array after comput_macro_variables. */
+LBM_API lbm_status lbm_get_populations(lbm_handle* h, double* f);
+
+/* Replaces the state (the reference's Backup_init, SP3:3652-3767): rho, u and
+ * f in reference layout.  The next step uses rho and u as given, like the
+ * reference's first collision after init or a restart. */
+LBM_API lbm_status lbm_set_state(lbm_handle* h, const double* rho, const double* u, const double* f);
+
+/* coor[(count+1)] = i*ny*nz + j*nz + k per fluid id (SP3:1065-1071). */
+LBM_API lbm_status lbm_export_compaction(lbm_handle* h, int32_t* coor);
+
+/* The neighbour table in the reference's push form nei_loc[(count+1)*19]
+ * (SP3:1099-1151: destination id, 0 = bounce-back), reconstructed from the
+ * device pull table -- for the bit-exact table test. */
+LBM_API lbm_status lbm_export_table(lbm_handle* h, int32_t* nei_loc);
+
+/* Chooses ordering x block size by timing `trial_steps` steps of each
+ * candidate on this geometry; the state is restored afterwards.  Writes the
+ * chosen ordering / block size and their measured MLUPS. */
+LBM_API lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* block_out,
+                        double* mlups_out);
+
+/* Kernel timing of the last lbm_step call (CUDA events on the handle's stream). */
+LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
+
+/* Memory facts: bytes of device memory the handle holds and the algorithmic
+ * bytes one fluid-node update moves (2*19*s + 18*4). */
+LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

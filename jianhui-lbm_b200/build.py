@@ -1,0 +1,110 @@
+"""Builds liblbm.so in-tree for sm_100a (B200).
+
+    python jianhui-lbm_b200/build.py [--verbose] [--ptxas-info]
+
+CUDA sources are compiled by nvcc with ``-gencode arch=compute_100a,code=sm_100a``,
+host sources by the system g++ (shared libstdc++), and everything is linked
+against the static CUDA runtime into ``lbm_b200/liblbm.so``.  Objects are
+cached under ``_build/`` and rebuilt when a source or header is newer.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+OUT = os.path.join(HERE, "lbm_b200", "liblbm.so")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA, "bin", "nvcc")
+CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+INCLUDES = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+# (source, extra nvcc flags).  sp_faithful.cu must not contract a*b+c into FMA:
+# it reproduces the reference's FP64 arithmetic bit for bit.
+CUDA_SOURCES = [
+    ("sp_kernels.cu", []),
+    ("sp_faithful.cu", ["-fmad=false"]),
+]
+CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp"]
+
+
+def _headers():
+    hs = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
+    hs += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    return hs
+
+
+def _stale(obj, src, headers):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(p) > t for p in [src] + headers)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build step failed ({r.returncode}):\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return r.stdout + r.stderr
+
+
+def build(verbose=False, ptxas_info=False, force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    headers = _headers()
+    sources = [os.path.join(CSRC, s) for s, _ in CUDA_SOURCES] + [os.path.join(CSRC, s) for s in CXX_SOURCES]
+    if not (force or ptxas_info) and os.path.exists(OUT):
+        newest = max(os.path.getmtime(p) for p in sources + headers + [os.path.abspath(__file__)])
+        if os.path.getmtime(OUT) >= newest:
+            return OUT, ""
+    objs = []
+    logs = []
+    for src, extra in CUDA_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+        if force or ptxas_info or _stale(o, s, headers):
+            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-ccbin", CXX, "-Xcompiler", "-fPIC,-fvisibility=hidden",
+                   "--expt-relaxed-constexpr", *INCLUDES, *extra, "-c", s, "-o", o]
+            if ptxas_info:
+                cmd.insert(1, "-Xptxas=-v")
+            logs.append(_run(cmd, verbose))
+    for src in CXX_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+        if force or _stale(o, s, headers):
+            cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wno-unused-function",
+                   "-I", os.path.join(CUDA, "include"), *INCLUDES, "-c", s, "-o", o]
+            logs.append(_run(cmd, verbose))
+    if force or not os.path.exists(OUT) or any(os.path.getmtime(o) > os.path.getmtime(OUT) for o in objs):
+        tmp = OUT + ".tmp"
+        cmd = [NVCC, *ARCH, "-ccbin", CXX, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs,
+               "-cudart", "static", "-Xlinker", "--exclude-libs,ALL"]
+        logs.append(_run(cmd, verbose))
+        shutil.move(tmp, OUT)
+    return OUT, "".join(logs)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-info", action="store_true", help="print -Xptxas -v register/spill report")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    out, log = build(a.verbose, a.ptxas_info, a.force)
+    if a.ptxas_info:
+        print(log)
+    print(out)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,677 @@
+// C ABI of the single-phase solver (include/lbm.h).
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lbm_internal.h"
+
+namespace lbm {
+
+lbm_status read_input_file(const char* path, lbm_input* o);
+lbm_status read_mask_file(const char* path, int nx, int ny, int nz, int decbin, uint8_t* mask);
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+lbm_status fail(lbm_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+static Store store_of(int precision) {
+  switch (precision) {
+    case LBM_PREC_F64: return Store::F64;
+    case LBM_PREC_F32: return Store::F32;
+    case LBM_PREC_F16: return Store::F16;
+    default: return Store::F64D;
+  }
+}
+
+// feq of `feq` (SP3:1382-1394), lattice units.
+static double feq_ref(int q, double rho, const double* u) {
+  const double c2 = 1.0 * 1.0, c4 = c2 * c2;
+  const double eu = (double)cx(q) * u[0] + (double)cy(q) * u[1] + (double)cz(q) * u[2];
+  const double uv = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  return weight(q) * rho * (1.0 + 3.0 * eu / c2 + 4.5 * eu * eu / c4 - 1.5 * uv / c2);
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t b) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = b;
+    return b ? cudaMalloc(&p, b) : cudaSuccess;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+}  // namespace lbm
+
+using namespace lbm;
+
+struct lbm_handle {
+  lbm_params prm{};
+  Store kind = Store::F32;
+  std::vector<uint8_t> mask;
+  Geometry geo;
+  MrtConstants mrt{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf pop[2], table, ref_of, window, rho_given, u_given, rho_prev, u_prev, partials, result;
+  int cur = 0;
+  long long step = 0;
+  bool given_macro = true;  // next step / reduce takes rho, u from rho_given / u_given
+  bool uprev_valid = false;
+  double perm_prev[3] = {0, 0, 0};
+  int overspeed = 0;
+  int block = 256;
+  int ordering = LBM_ORDER_REFERENCE;
+  int last_p = -1;
+  double fp16_scale = 1.0;
+  double last_ms = 0.0;
+  // captured step chains, one per starting buffer
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_steps = 0;
+
+  ~lbm_handle() {
+    for (auto& g : graph)
+      if (g) cudaGraphExecDestroy(g);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  size_t mac_bytes() const { return (kind == Store::F64 || kind == Store::F64D) ? 8 : 4; }
+  void drop_graphs() {
+    for (auto& g : graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+};
+
+namespace {
+
+lbm_status upload_layout(lbm_handle* h) {
+  Geometry& g = h->geo;
+  const size_t npad = (size_t)g.npad;
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->table.p, g.src.data(), sizeof(int32_t) * 18 * npad, cudaMemcpyHostToDevice,
+                               h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->ref_of.p, g.ref_of.data(), sizeof(int32_t) * (size_t)std::max(g.count, 1),
+                               cudaMemcpyHostToDevice, h->stream));
+  if (!g.in_window.empty()) {
+    if (!h->window.p) LBM_CUDA_TRY(h->window.alloc((size_t)g.count));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->window.p, g.in_window.data(), (size_t)g.count, cudaMemcpyHostToDevice, h->stream));
+  }
+  h->last_p = g.count > 0 ? g.int_of[g.count] : -1;
+  h->drop_graphs();
+  return LBM_OK;
+}
+
+lbm_status layout(lbm_handle* h, int ordering) {
+  order_nodes(h->mask.data(), ordering, &h->geo);
+  build_pull_table(h->mask.data(), &h->geo);
+  set_window(h->prm.window, &h->geo);
+  h->ordering = ordering;
+  return upload_layout(h);
+}
+
+lbm_status alloc_device(lbm_handle* h) {
+  const size_t npad = (size_t)h->geo.npad;
+  const size_t s = store_bytes(h->kind);
+  for (auto& b : h->pop) LBM_CUDA_TRY(b.alloc(kQ * npad * s));
+  LBM_CUDA_TRY(h->table.alloc(18 * npad * sizeof(int32_t)));
+  LBM_CUDA_TRY(h->ref_of.alloc(std::max<size_t>(h->geo.count, 1) * sizeof(int32_t)));
+  LBM_CUDA_TRY(h->rho_given.alloc(npad * h->mac_bytes()));
+  LBM_CUDA_TRY(h->u_given.alloc(3 * npad * h->mac_bytes()));
+  LBM_CUDA_TRY(h->rho_prev.alloc(npad * h->mac_bytes()));
+  LBM_CUDA_TRY(h->u_prev.alloc(3 * npad * h->mac_bytes()));
+  LBM_CUDA_TRY(h->partials.alloc((size_t)reduce_blocks(h->geo.count) * 8 * sizeof(double)));
+  LBM_CUDA_TRY(h->result.alloc(8 * sizeof(double)));
+  return LBM_OK;
+}
+
+lbm_status init_state(lbm_handle* h) {
+  double feq[kQ];
+  for (int q = 0; q < kQ; q++) feq[q] = feq_ref(q, 1.0, h->prm.u_init);
+  LBM_CUDA_TRY(launch_init_uniform(h->kind, h->pop[0].p, h->table.as<int32_t>(), h->geo.count, h->geo.npad,
+                                   h->fp16_scale, feq, h->stream));
+  LBM_CUDA_TRY(launch_fill_macro(h->kind, h->rho_given.p, h->u_given.p, h->geo.count, h->geo.npad, 1.0,
+                                 h->prm.u_init, h->stream));
+  h->cur = 0;
+  h->step = 0;
+  h->given_macro = true;
+  h->uprev_valid = false;
+  h->perm_prev[0] = h->perm_prev[1] = h->perm_prev[2] = 0.0;
+  h->overspeed = 0;
+  return LBM_OK;
+}
+
+StepArgs step_args(lbm_handle* h, bool write) {
+  StepArgs a{};
+  a.src_pop = h->pop[h->cur].p;
+  a.dst_pop = h->pop[1 - h->cur].p;
+  a.table = h->table.as<int32_t>();
+  a.n = h->geo.count;
+  a.npad = h->geo.npad;
+  a.rho_in = h->given_macro ? h->rho_given.p : nullptr;
+  a.u_in = h->given_macro ? h->u_given.p : nullptr;
+  a.rho_out = write ? h->rho_prev.p : nullptr;
+  a.u_out = write ? h->u_prev.p : nullptr;
+  a.gx = h->prm.gx;
+  a.gy = h->prm.gy;
+  a.gz = h->prm.gz;
+  a.s_v = h->mrt.s_v;
+  a.s_o = h->mrt.s_o;
+  a.fp16_scale = h->fp16_scale;
+  return a;
+}
+
+lbm_status one_step(lbm_handle* h, bool write) {
+  const StepArgs a = step_args(h, write);
+  LBM_CUDA_TRY(launch_step(h->kind, a, h->block, h->stream));
+  h->cur = 1 - h->cur;
+  h->given_macro = false;
+  h->step++;
+  return LBM_OK;
+}
+
+constexpr int kGraphSteps = 16;  // even: a replay leaves the buffer parity unchanged
+
+lbm_status ensure_graph(lbm_handle* h) {
+  if (h->graph[h->cur]) return LBM_OK;
+  cudaGraph_t g = nullptr;
+  const int cur0 = h->cur;
+  LBM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int c = cur0;
+  cudaError_t err = cudaSuccess;
+  for (int s = 0; s < kGraphSteps && err == cudaSuccess; s++) {
+    StepArgs a = step_args(h, false);
+    a.src_pop = h->pop[c].p;
+    a.dst_pop = h->pop[1 - c].p;
+    a.rho_in = a.u_in = nullptr;
+    err = launch_step(h->kind, a, h->block, h->stream);
+    c = 1 - c;
+  }
+  const cudaError_t end = cudaStreamEndCapture(h->stream, &g);
+  if (err != cudaSuccess || end != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(LBM_ERR_CUDA, std::string("graph capture failed: ") +
+                                  cudaGetErrorString(err != cudaSuccess ? err : end));
+  }
+  const cudaError_t inst = cudaGraphInstantiate(&h->graph[cur0], g, 0);
+  cudaGraphDestroy(g);
+  LBM_CUDA_TRY(inst);
+  h->graph_steps = kGraphSteps;
+  return LBM_OK;
+}
+
+lbm_status run_steps(lbm_handle* h, int nsteps) {
+  if (nsteps <= 0) return LBM_OK;
+  LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  int left = nsteps;
+  lbm_status st;
+  if (h->given_macro) {
+    if ((st = one_step(h, left == 1)) != LBM_OK) return st;
+    left--;
+  }
+  // all but the last step through captured chains, the last one writes the
+  // pre-collision macro fields (the velocity one step before the new state)
+  while (left - 1 >= kGraphSteps) {
+    if ((st = ensure_graph(h)) != LBM_OK) return st;
+    LBM_CUDA_TRY(cudaGraphLaunch(h->graph[h->cur], h->stream));
+    h->step += kGraphSteps;
+    left -= kGraphSteps;
+  }
+  while (left > 0) {
+    if ((st = one_step(h, left == 1)) != LBM_OK) return st;
+    left--;
+  }
+  h->uprev_valid = true;
+  LBM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+  LBM_CUDA_TRY(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  LBM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  return LBM_OK;
+}
+
+// Error + Comput_Perm on the device; optional macro fields (internal order).
+lbm_status reduce_raw(lbm_handle* h, double r[8], double* rho_out_int, double* u_out_int) {
+  ReduceArgs a{};
+  a.pop = h->pop[h->cur].p;
+  a.table = h->table.as<int32_t>();
+  a.n = h->geo.count;
+  a.npad = h->geo.npad;
+  a.rho_in = h->given_macro ? h->rho_given.p : nullptr;
+  a.u_in = h->given_macro ? h->u_given.p : nullptr;
+  a.u_prev = (!h->given_macro && h->uprev_valid) ? h->u_prev.p : nullptr;
+  a.last_p = h->last_p;
+  a.window = h->geo.in_window.empty() ? nullptr : h->window.as<uint8_t>();
+  a.gx = h->prm.gx;
+  a.gy = h->prm.gy;
+  a.gz = h->prm.gz;
+  a.fp16_scale = h->fp16_scale;
+  a.rho_out = rho_out_int;
+  a.u_out = u_out_int;
+  a.partials = h->partials.as<double>();
+  a.result = h->result.as<double>();
+  LBM_CUDA_TRY(launch_reduce(h->kind, a, h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(r, a.result, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+void fill_diag(lbm_handle* h, const double r[8], lbm_diag* d) {
+  const Geometry& g = h->geo;
+  std::memset(d, 0, sizeof(*d));
+  d->step = h->step;
+  const double t1 = std::sqrt(r[0]), t2 = std::sqrt(r[1]);
+  d->u_rel_change = t1 / (t2 + 1e-30);                                   // SP3:3149-3151
+  d->u_max = std::sqrt(r[3]);                                             // SP3:3152
+  d->u_mean_speed = r[2] / ((double)g.nx * g.ny * g.nz * g.porosity);    // SP3:3183
+  const double V = (double)g.window_volume;
+  const double dp = 0.0;
+  const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
+  double perm[3];
+  for (int i = 0; i < 3; i++) perm[i] = r[4 + i] / V * h->prm.nu / (gg[i] + dp);  // SP3:3611-3613
+  const int dir = (h->prm.perdir >= 1 && h->prm.perdir <= 3) ? h->prm.perdir - 1 : 0;
+  d->perm_rel_change = (perm[dir] - h->perm_prev[dir]) / h->perm_prev[dir];  // SP3:3615-3626
+  for (int i = 0; i < 3; i++) {
+    d->perm[i] = perm[i];
+    h->perm_prev[i] = perm[i];
+  }
+  const double ax = r[4] / (V * g.porosity), ay = r[5] / (V * g.porosity), az = r[6] / (V * g.porosity);
+  d->u_ave = std::sqrt(ax * ax + ay * ay + az * az);  // SP3:3634-3638
+  d->mass = r[7];
+  d->porosity = g.porosity;
+  d->nan_detected = (d->u_rel_change != d->u_rel_change) ? 1 : 0;
+}
+
+lbm_status check_handle(lbm_handle* h) {
+  if (!h) return fail(LBM_ERR_ARG, "null handle");
+  if (cudaSetDevice(h->device) != cudaSuccess) return fail(LBM_ERR_CUDA, "cudaSetDevice failed");
+  return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lbm_last_error(void) { return g_last_error.c_str(); }
+
+const char* lbm_status_string(lbm_status s) {
+  switch (s) {
+    case LBM_OK: return "ok";
+    case LBM_ERR_ARG: return "invalid argument";
+    case LBM_ERR_IO: return "i/o error";
+    case LBM_ERR_OOM: return "out of memory";
+    case LBM_ERR_CUDA: return "cuda error";
+    case LBM_ERR_NAN: return "non-finite velocity";
+    case LBM_ERR_NOT_CONVERGED: return "not converged";
+    case LBM_ERR_FORMAT: return "malformed input";
+    case LBM_ERR_STATE: return "invalid state";
+    case LBM_ERR_OVERSPEED: return "velocity above 10 (reference stop rule)";
+    case LBM_ERR_NO_DEVICE: return "no cuda device";
+  }
+  return "unknown status";
+}
+
+int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+void lbm_params_default(lbm_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->nu = 0.1;
+  p->gx = 1e-6;
+  p->precision = LBM_PREC_F32;
+  p->ordering = LBM_ORDER_REFERENCE;
+  p->block_size = 256;
+  p->perdir = 1;
+  for (int i = 0; i < 6; i++) p->window[i] = -1;
+  p->fp16_scale = 0.0;
+  p->device = 0;
+}
+
+lbm_status lbm_read_input(const char* path, lbm_input* out) { return read_input_file(path, out); }
+
+lbm_status lbm_read_mask(const char* path, int nx, int ny, int nz, int decbin, uint8_t* mask_out) {
+  return read_mask_file(path, nx, ny, nz, decbin, mask_out);
+}
+
+lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, int nz, lbm_handle** out) {
+  if (!p || !mask || !out || nx <= 0 || ny <= 0 || nz <= 0) return fail(LBM_ERR_ARG, "lbm_create: bad argument");
+  *out = nullptr;
+  if ((long long)nx * ny * nz > (1LL << 31) - 1) return fail(LBM_ERR_ARG, "lbm_create: grid exceeds 2^31 cells");
+  if (!(p->nu > 0.0)) return fail(LBM_ERR_ARG, "lbm_create: viscosity must be positive");
+  if (p->precision < LBM_PREC_F64 || p->precision > LBM_PREC_F64_FAST)
+    return fail(LBM_ERR_ARG, "lbm_create: unknown precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device");
+  if (p->device < 0 || p->device >= ndev) return fail(LBM_ERR_ARG, "lbm_create: bad device ordinal");
+  auto h = std::make_unique<lbm_handle>();
+  h->prm = *p;
+  h->device = p->device;
+  h->kind = store_of(p->precision);
+  h->block = (p->block_size == 64 || p->block_size == 128 || p->block_size == 256 || p->block_size == 512)
+                 ? p->block_size
+                 : 256;
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  LBM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  LBM_CUDA_TRY(cudaEventCreate(&h->ev0));
+  LBM_CUDA_TRY(cudaEventCreate(&h->ev1));
+  h->mask.assign(mask, mask + (size_t)nx * ny * nz);
+  if (!build_mrt_constants(p->nu, &h->mrt)) return fail(LBM_ERR_ARG, "moment matrix inversion failed");
+  if (h->kind == Store::F64) LBM_CUDA_TRY(set_mi_constant(&h->mrt.MI[0][0], h->stream));
+  if (h->kind == Store::F16) {
+    double sc = p->fp16_scale;
+    if (!(sc > 0)) {
+      const double gmax = std::fmax(std::fabs(p->gx), std::fmax(std::fabs(p->gy), std::fabs(p->gz)));
+      const double target = gmax > 0 ? 10.0 * p->nu / gmax : 1024.0;
+      sc = std::exp2(std::round(std::log2(target)));
+      sc = std::fmin(std::fmax(sc, 1.0), 16777216.0);
+    }
+    h->fp16_scale = sc;
+  }
+  compact_reference(h->mask.data(), nx, ny, nz, &h->geo);
+  if (h->geo.count == 0) return fail(LBM_ERR_ARG, "geometry has no pore cells");
+  if ((long long)h->geo.npad * kQ > (1LL << 31) - 1) return fail(LBM_ERR_ARG, "too many fluid nodes for int32 table");
+  lbm_status st;
+  if ((st = alloc_device(h.get())) != LBM_OK) return st;
+  const int ord = p->ordering == LBM_ORDER_AUTO ? LBM_ORDER_REFERENCE : p->ordering;
+  if ((st = layout(h.get(), ord)) != LBM_OK) return st;
+  if ((st = init_state(h.get())) != LBM_OK) return st;
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = h.release();
+  if (p->ordering == LBM_ORDER_AUTO) {
+    int o, b;
+    double ml;
+    st = lbm_autotune(*out, 20, &o, &b, &ml);
+    if (st != LBM_OK) {
+      lbm_destroy(*out);
+      *out = nullptr;
+      return st;
+    }
+  }
+  return LBM_OK;
+}
+
+lbm_status lbm_create_from_input(const char* input_path, int precision, int ordering, lbm_handle** out,
+                                 lbm_input* parsed_out) {
+  lbm_input in;
+  lbm_status st = read_input_file(input_path, &in);
+  if (st != LBM_OK) return st;
+  if (parsed_out) *parsed_out = in;
+  if (in.in_bc != 0 || in.pre_xp || in.pre_xn || in.pre_yp || in.pre_yn || in.pre_zp || in.pre_zn || in.vel_xp ||
+      in.vel_xn || in.vel_yp || in.vel_yn || in.vel_zp || in.vel_zn)
+    return fail(LBM_ERR_ARG, "pressure/velocity boundaries are not supported (fully periodic solver)");
+  if (in.nnf_module != 0) return fail(LBM_ERR_ARG, "non-Newtonian module is not supported");
+  if (in.lattice_v != 0) return fail(LBM_ERR_ARG, "self-defined lattice velocity is not supported");
+  std::vector<uint8_t> mask((size_t)in.nx * in.ny * in.nz);
+  // the geometry path is relative to the working directory, as in the reference
+  st = read_mask_file(in.geometry_file, in.nx, in.ny, in.nz, in.decbin, mask.data());
+  if (st != LBM_OK) return st;
+  lbm_params p;
+  lbm_params_default(&p);
+  p.nu = in.in_vis;
+  p.gx = in.gx;
+  p.gy = in.gy;
+  p.gz = in.gz;
+  p.u_init[0] = in.inivx;
+  p.u_init[1] = in.inivy;
+  p.u_init[2] = in.inivz;
+  p.precision = precision;
+  p.ordering = ordering;
+  p.perdir = in.perdir;
+  if (in.par_per_x || in.par_per_y || in.par_per_z) {
+    // SP3:1005-1010: an axis without a partial window spans the whole box
+    p.window[0] = in.par_per_x ? in.per_xn : 0;
+    p.window[1] = in.par_per_x ? in.per_xp : in.nx - 1;
+    p.window[2] = in.par_per_y ? in.per_yn : 0;
+    p.window[3] = in.par_per_y ? in.per_yp : in.ny - 1;
+    p.window[4] = in.par_per_z ? in.per_zn : 0;
+    p.window[5] = in.par_per_z ? in.per_zp : in.nz - 1;
+  }
+  return lbm_create(&p, mask.data(), in.nx, in.ny, in.nz, out);
+}
+
+void lbm_destroy(lbm_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  delete h;
+}
+
+lbm_status lbm_step(lbm_handle* h, int nsteps) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (nsteps < 0) return fail(LBM_ERR_ARG, "lbm_step: negative step count");
+  return run_steps(h, nsteps);
+}
+
+lbm_status lbm_reduce(lbm_handle* h, lbm_diag* out) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (!out) return fail(LBM_ERR_ARG, "lbm_reduce: null output");
+  double r[8];
+  if ((st = reduce_raw(h, r, nullptr, nullptr)) != LBM_OK) return st;
+  fill_diag(h, r, out);
+  return LBM_OK;
+}
+
+lbm_status lbm_run_to_convergence(lbm_handle* h, double tol, int check_every, int max_steps, lbm_diag* out) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (check_every <= 0 || max_steps < 0 || !(tol > 0)) return fail(LBM_ERR_ARG, "lbm_run_to_convergence: bad argument");
+  lbm_diag d{};
+  double prev = 0.0;
+  bool have_prev = false;
+  while (h->step < max_steps) {
+    const int k = (int)std::min<long long>(check_every, max_steps - h->step);
+    if ((st = run_steps(h, k)) != LBM_OK) return st;
+    double r[8];
+    if ((st = reduce_raw(h, r, nullptr, nullptr)) != LBM_OK) return st;
+    fill_diag(h, r, &d);
+    if (out) *out = d;
+    if (d.nan_detected) return fail(LBM_ERR_NAN, "non-finite velocity (reference: PROGRAM STOP)");
+    if (d.u_max >= 10.0 && ++h->overspeed >= 5) return fail(LBM_ERR_OVERSPEED, "velocity above 10 five times");
+    if (have_prev && std::fabs((prev - d.u_ave) / prev) < tol) {
+      d.converged = 1;
+      if (out) *out = d;
+      return LBM_OK;
+    }
+    prev = d.u_ave;
+    have_prev = true;
+  }
+  if (out) *out = d;
+  return fail(LBM_ERR_NOT_CONVERGED, "step cap reached before the convergence tolerance");
+}
+
+lbm_status lbm_info(lbm_handle* h, int* count, double* porosity, long long* step) {
+  if (!h) return fail(LBM_ERR_ARG, "null handle");
+  if (count) *count = h->geo.count;
+  if (porosity) *porosity = h->geo.porosity;
+  if (step) *step = h->step;
+  return LBM_OK;
+}
+
+lbm_status lbm_get_fields(lbm_handle* h, double* rho, double* u) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  const int n = h->geo.count, npad = h->geo.npad;
+  DevBuf rint, uint_, rref, uref;
+  LBM_CUDA_TRY(rint.alloc((size_t)npad * sizeof(double)));
+  LBM_CUDA_TRY(uint_.alloc((size_t)3 * npad * sizeof(double)));
+  LBM_CUDA_TRY(rref.alloc((size_t)(n + 1) * sizeof(double)));
+  LBM_CUDA_TRY(uref.alloc((size_t)(n + 1) * 3 * sizeof(double)));
+  double r[8];
+  const double pp[3] = {h->perm_prev[0], h->perm_prev[1], h->perm_prev[2]};
+  if ((st = reduce_raw(h, r, rint.as<double>(), uint_.as<double>())) != LBM_OK) return st;
+  for (int i = 0; i < 3; i++) h->perm_prev[i] = pp[i];
+  LBM_CUDA_TRY(cudaMemsetAsync(rref.p, 0, rref.bytes, h->stream));
+  LBM_CUDA_TRY(cudaMemsetAsync(uref.p, 0, uref.bytes, h->stream));
+  LBM_CUDA_TRY(launch_export_macro(rint.as<double>(), uint_.as<double>(), h->ref_of.as<int32_t>(), n, npad,
+                                   rref.as<double>(), uref.as<double>(), h->stream));
+  if (rho) LBM_CUDA_TRY(cudaMemcpyAsync(rho, rref.p, rref.bytes, cudaMemcpyDeviceToHost, h->stream));
+  if (u) LBM_CUDA_TRY(cudaMemcpyAsync(u, uref.p, uref.bytes, cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+lbm_status lbm_get_populations(lbm_handle* h, double* f) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (!f) return fail(LBM_ERR_ARG, "lbm_get_populations: null output");
+  const int n = h->geo.count;
+  DevBuf out;
+  LBM_CUDA_TRY(out.alloc((size_t)(n + 1) * kQ * sizeof(double)));
+  LBM_CUDA_TRY(cudaMemsetAsync(out.p, 0, out.bytes, h->stream));
+  LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
+                                 h->geo.npad, h->fp16_scale, out.as<double>(), h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(f, out.p, out.bytes, cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+lbm_status lbm_set_state(lbm_handle* h, const double* rho, const double* u, const double* f) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (!rho || !u || !f) return fail(LBM_ERR_ARG, "lbm_set_state: null input");
+  const int n = h->geo.count;
+  DevBuf fin, rin, uin;
+  LBM_CUDA_TRY(fin.alloc((size_t)(n + 1) * kQ * sizeof(double)));
+  LBM_CUDA_TRY(rin.alloc((size_t)(n + 1) * sizeof(double)));
+  LBM_CUDA_TRY(uin.alloc((size_t)(n + 1) * 3 * sizeof(double)));
+  LBM_CUDA_TRY(cudaMemcpyAsync(fin.p, f, fin.bytes, cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(rin.p, rho, rin.bytes, cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(uin.p, u, uin.bytes, cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(launch_import_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
+                                 h->geo.npad, h->fp16_scale, fin.as<double>(), h->stream));
+  LBM_CUDA_TRY(launch_import_macro(h->kind, h->rho_given.p, h->u_given.p, h->ref_of.as<int32_t>(), n, h->geo.npad,
+                                   rin.as<double>(), uin.as<double>(), h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->given_macro = true;
+  h->uprev_valid = false;
+  return LBM_OK;
+}
+
+lbm_status lbm_export_compaction(lbm_handle* h, int32_t* coor) {
+  if (!h || !coor) return fail(LBM_ERR_ARG, "lbm_export_compaction: null argument");
+  std::memcpy(coor, h->geo.coor.data(), sizeof(int32_t) * (size_t)(h->geo.count + 1));
+  return LBM_OK;
+}
+
+lbm_status lbm_export_table(lbm_handle* h, int32_t* nei_loc) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (!nei_loc) return fail(LBM_ERR_ARG, "lbm_export_table: null output");
+  // round-trip through the device copy so the exported table is the one the kernels read
+  Geometry g = h->geo;
+  LBM_CUDA_TRY(cudaMemcpyAsync(g.src.data(), h->table.p, sizeof(int32_t) * 18 * (size_t)g.npad, cudaMemcpyDeviceToHost,
+                               h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  pull_to_push(g, nei_loc);
+  return LBM_OK;
+}
+
+lbm_status lbm_last_step_ms(lbm_handle* h, double* ms) {
+  if (!h || !ms) return fail(LBM_ERR_ARG, "null argument");
+  *ms = h->last_ms;
+  return LBM_OK;
+}
+
+lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu) {
+  if (!h) return fail(LBM_ERR_ARG, "null handle");
+  if (device_bytes) {
+    size_t b = 0;
+    for (const DevBuf* d : {&h->pop[0], &h->pop[1], &h->table, &h->ref_of, &h->window, &h->rho_given, &h->u_given,
+                            &h->rho_prev, &h->u_prev, &h->partials, &h->result})
+      b += d->bytes;
+    *device_bytes = b;
+  }
+  if (bytes_per_lu) *bytes_per_lu = 2.0 * kQ * (double)store_bytes(h->kind) + 18.0 * 4.0;
+  return LBM_OK;
+}
+
+lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* block_out, double* mlups_out) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (trial_steps <= 0) trial_steps = 20;
+  const int n = h->geo.count;
+  // save the state in reference layout (device side)
+  DevBuf fsave, rsave, usave;
+  LBM_CUDA_TRY(fsave.alloc((size_t)(n + 1) * kQ * sizeof(double)));
+  LBM_CUDA_TRY(rsave.alloc((size_t)h->geo.npad * sizeof(double)));
+  LBM_CUDA_TRY(usave.alloc((size_t)3 * h->geo.npad * sizeof(double)));
+  LBM_CUDA_TRY(cudaMemsetAsync(fsave.p, 0, fsave.bytes, h->stream));
+  LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
+                                 h->geo.npad, h->fp16_scale, fsave.as<double>(), h->stream));
+  DevBuf rref, uref;
+  LBM_CUDA_TRY(rref.alloc((size_t)(n + 1) * sizeof(double)));
+  LBM_CUDA_TRY(uref.alloc((size_t)(n + 1) * 3 * sizeof(double)));
+  const bool given = h->given_macro;
+  if (given) {
+    // the given macro fields are part of the state: round-trip them too
+    double r[8];
+    const double pp[3] = {h->perm_prev[0], h->perm_prev[1], h->perm_prev[2]};
+    if ((st = reduce_raw(h, r, rsave.as<double>(), usave.as<double>())) != LBM_OK) return st;
+    for (int i = 0; i < 3; i++) h->perm_prev[i] = pp[i];
+    LBM_CUDA_TRY(launch_export_macro(rsave.as<double>(), usave.as<double>(), h->ref_of.as<int32_t>(), n, h->geo.npad,
+                                     rref.as<double>(), uref.as<double>(), h->stream));
+  }
+  const long long step0 = h->step;
+  const int cur0 = h->cur;
+  const bool uprev0 = h->uprev_valid;
+  const int orders[4] = {LBM_ORDER_REFERENCE, LBM_ORDER_MORTON, LBM_ORDER_HILBERT, LBM_ORDER_BRICK};
+  const int blocks[4] = {128, 256, 512, 64};
+  double best = -1.0;
+  int best_o = h->ordering, best_b = h->block;
+  for (int oi = 0; oi < 4; oi++) {
+    if ((st = layout(h, orders[oi])) != LBM_OK) return st;
+    for (int bi = 0; bi < 4; bi++) {
+      h->block = blocks[bi];
+      h->drop_graphs();
+      h->given_macro = false;  // timing only; the state is restored below
+      h->cur = 0;
+      if ((st = run_steps(h, 2)) != LBM_OK) return st;  // warm-up
+      if ((st = run_steps(h, trial_steps)) != LBM_OK) return st;
+      const double ml = (double)n * trial_steps / (h->last_ms * 1e3);
+      if (ml > best) {
+        best = ml;
+        best_o = orders[oi];
+        best_b = blocks[bi];
+      }
+    }
+  }
+  if ((st = layout(h, best_o)) != LBM_OK) return st;
+  h->block = best_b;
+  h->drop_graphs();
+  h->cur = cur0;
+  LBM_CUDA_TRY(launch_import_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
+                                 h->geo.npad, h->fp16_scale, fsave.as<double>(), h->stream));
+  if (given)
+    LBM_CUDA_TRY(launch_import_macro(h->kind, h->rho_given.p, h->u_given.p, h->ref_of.as<int32_t>(), n, h->geo.npad,
+                                     rref.as<double>(), uref.as<double>(), h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->step = step0;
+  h->given_macro = given;
+  h->uprev_valid = false;
+  (void)uprev0;
+  if (ordering_out) *ordering_out = best_o;
+  if (block_out) *block_out = best_b;
+  if (mlups_out) *mlups_out = best;
+  return LBM_OK;
+}
+
+}  // extern "C"

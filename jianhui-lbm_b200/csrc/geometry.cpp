@@ -1,0 +1,195 @@
+// Host-side sparse indexing: fluid-node compaction, space-filling-curve
+// orderings, pull neighbour table with halfway bounce-back, and the
+// conversion back to the reference's push table.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "lbm_internal.h"
+
+namespace lbm {
+
+// Fluid ids in the reference order: k outer, j, i inner (x fastest), 1-based;
+// coor[id] = i*ny*nz + j*nz + k (SP3:1018-1025, 1065-1071).
+void compact_reference(const uint8_t* mask, int nx, int ny, int nz, Geometry* g) {
+  g->nx = nx;
+  g->ny = ny;
+  g->nz = nz;
+  const long cells = (long)nx * ny * nz;
+  long pores = 0;
+  for (long c = 0; c < cells; c++) pores += (mask[c] == 0);
+  g->count = (int)pores;
+  g->coor.assign((size_t)pores + 1, 0);
+  int id = 0;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++) {
+      const uint8_t* row = mask + (size_t)nx * (j + (size_t)ny * k);
+      for (int i = 0; i < nx; i++)
+        if (row[i] == 0) g->coor[++id] = i * ny * nz + j * nz + k;
+    }
+  g->npad = ((g->count + 255) / 256) * 256;
+  if (g->npad == 0) g->npad = 256;
+  g->porosity = cells ? (double)pores / (double)cells : 0.0;
+  g->window_volume = (int)cells;
+}
+
+static inline void cell_of(const Geometry& g, int id, int* i, int* j, int* k) {
+  const int c = g.coor[id];
+  *i = c / (g.ny * g.nz);
+  *j = (c % (g.ny * g.nz)) / g.nz;
+  *k = c % g.nz;
+}
+
+static inline uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+// 3-D Hilbert index by Skilling's transpose method ("Programming the Hilbert
+// curve", AIP Conf. Proc. 707, 2004): axes -> transposed index -> interleave.
+static uint64_t hilbert3(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t X[3] = {x, y, z};
+  const uint32_t M = 1u << (bits - 1);
+  for (uint32_t Qb = M; Qb > 1; Qb >>= 1) {
+    const uint32_t P = Qb - 1;
+    for (int i = 0; i < 3; i++) {
+      if (X[i] & Qb)
+        X[0] ^= P;
+      else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < 3; i++) X[i] ^= X[i - 1];
+  uint32_t t = 0;
+  for (uint32_t Qb = M; Qb > 1; Qb >>= 1)
+    if (X[2] & Qb) t ^= Qb - 1;
+  for (int i = 0; i < 3; i++) X[i] ^= t;
+  uint64_t h = 0;
+  for (int b = bits - 1; b >= 0; b--)
+    for (int i = 0; i < 3; i++) h = (h << 1) | ((X[i] >> b) & 1u);
+  return h;
+}
+
+void order_nodes(const uint8_t* mask, int ordering, Geometry* g) {
+  (void)mask;
+  const int n = g->count;
+  g->ref_of.resize(n);
+  g->int_of.assign((size_t)n + 1, -1);
+  if (ordering == LBM_ORDER_REFERENCE || n == 0) {
+    for (int p = 0; p < n; p++) g->ref_of[p] = p + 1;
+  } else {
+    std::vector<uint64_t> key(n);
+    int bits = 1;
+    while ((1 << bits) < std::max(g->nx, std::max(g->ny, g->nz))) bits++;
+    const int bx = 16, by = 4, bz = 4;
+    const int nbx = (g->nx + bx - 1) / bx, nby = (g->ny + by - 1) / by;
+    for (int id = 1; id <= n; id++) {
+      int i, j, k;
+      cell_of(*g, id, &i, &j, &k);
+      uint64_t kk;
+      if (ordering == LBM_ORDER_MORTON) {
+        kk = spread3((uint64_t)i) | (spread3((uint64_t)j) << 1) | (spread3((uint64_t)k) << 2);
+      } else if (ordering == LBM_ORDER_HILBERT) {
+        kk = hilbert3((uint32_t)i, (uint32_t)j, (uint32_t)k, bits);
+      } else {  // brick
+        const uint64_t b = ((uint64_t)(k / bz) * nby + (uint64_t)(j / by)) * nbx + (uint64_t)(i / bx);
+        kk = b * (uint64_t)(bx * by * bz) + (uint64_t)((k % bz) * (bx * by) + (j % by) * bx + (i % bx));
+      }
+      key[id - 1] = kk;
+    }
+    std::vector<int32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    for (int p = 0; p < n; p++) g->ref_of[p] = idx[p] + 1;
+  }
+  for (int p = 0; p < n; p++) g->int_of[g->ref_of[p]] = p;
+}
+
+// Pull table: for node p and direction q >= 1 the post-streaming population
+// f_q(p) is the post-collision value f*_q at the fluid cell p - e_q (periodic
+// wrap on every axis, SP3:1128-1130); when that cell is solid it is the
+// node's own f*_{opp q} (halfway bounce-back, SP3:1764-1771 where
+// nei_loc == 0 writes F[ci][LR[mi]]).  Entries are flat indices into the
+// [19][npad] population array.
+void build_pull_table(const uint8_t* mask, Geometry* g) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz, n = g->count, npad = g->npad;
+  std::vector<int32_t> cell_id((size_t)nx * ny * nz, -1);  // x-fastest cell -> internal index
+  for (int p = 0; p < n; p++) {
+    int i, j, k;
+    cell_of(*g, g->ref_of[p], &i, &j, &k);
+    cell_id[i + (size_t)nx * (j + (size_t)ny * k)] = p;
+  }
+  g->src.assign((size_t)18 * npad, 0);
+  for (int p = 0; p < n; p++) {
+    int i, j, k;
+    cell_of(*g, g->ref_of[p], &i, &j, &k);
+    for (int q = 1; q < kQ; q++) {
+      int ip = i - cx(q), jp = j - cy(q), kp = k - cz(q);
+      if (ip < 0) ip = nx - 1;
+      if (ip >= nx) ip = 0;
+      if (jp < 0) jp = ny - 1;
+      if (jp >= ny) jp = 0;
+      if (kp < 0) kp = nz - 1;
+      if (kp >= nz) kp = 0;
+      const size_t c = ip + (size_t)nx * (jp + (size_t)ny * kp);
+      int32_t s;
+      if (mask[c] == 0)
+        s = q * npad + cell_id[c];
+      else
+        s = opp(q) * npad + p;
+      g->src[(size_t)(q - 1) * npad + p] = s;
+    }
+  }
+  // padding lanes point at themselves in direction 0 (never launched)
+  for (int q = 1; q < kQ; q++)
+    for (int p = n; p < npad; p++) g->src[(size_t)(q - 1) * npad + p] = p;
+}
+
+// Inverse of build_pull_table: nei_loc[ref m][q] = ref id of m + e_q, or 0
+// when that cell is solid (the reference's push form, SP3:1135-1140).
+void pull_to_push(const Geometry& g, int32_t* nei) {
+  const int n = g.count, npad = g.npad;
+  std::memset(nei, 0, sizeof(int32_t) * (size_t)(n + 1) * kQ);
+  for (int p = 0; p < n; p++) nei[(size_t)g.ref_of[p] * kQ + 0] = g.ref_of[p];
+  for (int p = 0; p < n; p++)
+    for (int q = 1; q < kQ; q++) {
+      const int32_t s = g.src[(size_t)(q - 1) * npad + p];
+      const int sq = s / npad, sm = s % npad;
+      if (sq == q)  // streamed from node sm along +e_q: sm + e_q = p
+        nei[(size_t)g.ref_of[sm] * kQ + q] = g.ref_of[p];
+      else          // bounced: p + e_{opp q} is solid
+        nei[(size_t)g.ref_of[p] * kQ + opp(q)] = 0;
+    }
+}
+
+// Permeability window (per_xn..per_zp, SP3:1005-1020, 3581-3590).
+void set_window(const int w[6], Geometry* g) {
+  const bool full = (w[0] < 0 && w[1] < 0 && w[2] < 0 && w[3] < 0 && w[4] < 0 && w[5] < 0);
+  if (full) {
+    g->in_window.clear();
+    g->window_volume = g->nx * g->ny * g->nz;
+    return;
+  }
+  const int xn = w[0], xp = w[1], yn = w[2], yp = w[3], zn = w[4], zp = w[5];
+  g->window_volume = (xp - xn + 1) * (yp - yn + 1) * (zp - zn + 1);
+  g->in_window.assign(g->count, 0);
+  long pores = 0;
+  for (int p = 0; p < g->count; p++) {
+    int i, j, k;
+    cell_of(*g, g->ref_of[p], &i, &j, &k);
+    const bool in = i >= xn && i <= xp && j >= yn && j <= yp && k >= zn && k <= zp;
+    g->in_window[p] = in;
+    pores += in;
+  }
+  g->porosity = g->window_volume > 0 ? (double)pores / (double)g->window_volume : 0.0;
+}
+
+}  // namespace lbm

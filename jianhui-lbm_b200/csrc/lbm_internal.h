@@ -1,0 +1,191 @@
+// Internal declarations shared by the host code and the CUDA kernels of
+// liblbm.so.  Not part of the public ABI (include/lbm.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "lbm.h"
+
+namespace lbm {
+
+constexpr int kQ = 19;
+
+// ---------------------------------------------------------------- D3Q19 set
+// Velocity set and opposite directions of the reference (SP3:167-180).
+__host__ __device__ constexpr int cx(int q) {
+  return (q == 1 || q == 7 || q == 9 || q == 15 || q == 17) ? 1
+         : (q == 2 || q == 8 || q == 10 || q == 16 || q == 18) ? -1
+                                                                : 0;
+}
+__host__ __device__ constexpr int cy(int q) {
+  return (q == 3 || q == 7 || q == 8 || q == 11 || q == 13) ? 1
+         : (q == 4 || q == 9 || q == 10 || q == 12 || q == 14) ? -1
+                                                                 : 0;
+}
+__host__ __device__ constexpr int cz(int q) {
+  return (q == 5 || q == 11 || q == 12 || q == 15 || q == 16) ? 1
+         : (q == 6 || q == 13 || q == 14 || q == 17 || q == 18) ? -1
+                                                                  : 0;
+}
+__host__ __device__ constexpr int opp(int q) {
+  return q == 0 ? 0 : (q <= 6 ? (q % 2 ? q + 1 : q - 1) : (q <= 10 ? 17 - q : (q <= 14 ? 25 - q : 33 - q)));
+}
+__host__ __device__ constexpr double weight(int q) {
+  return q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+
+// d'Humieres moment basis of the reference (SP3:64-83) as polynomials of the
+// velocity components; row k, column q.
+__host__ __device__ constexpr int mcoef(int k, int q) {
+  const int x = cx(q), y = cy(q), z = cz(q);
+  const int c2 = x * x + y * y + z * z;
+  switch (k) {
+    case 0: return 1;
+    case 1: return 19 * c2 - 30;
+    case 2: return (21 * c2 * c2 - 53 * c2 + 24) / 2;
+    case 3: return x;
+    case 4: return (5 * c2 - 9) * x;
+    case 5: return y;
+    case 6: return (5 * c2 - 9) * y;
+    case 7: return z;
+    case 8: return (5 * c2 - 9) * z;
+    case 9: return 3 * x * x - c2;
+    case 10: return (3 * c2 - 5) * (3 * x * x - c2);
+    case 11: return y * y - z * z;
+    case 12: return (3 * c2 - 5) * (y * y - z * z);
+    case 13: return x * y;
+    case 14: return y * z;
+    case 15: return x * z;
+    case 16: return (y * y - z * z) * x;
+    case 17: return (z * z - x * x) * y;
+    default: return (x * x - y * y) * z;
+  }
+}
+// Squared norm of row k (rows are mutually orthogonal, so M^-1 = M^T diag(1/norm)).
+__host__ __device__ constexpr int mnorm(int k) {
+  int s = 0;
+  for (int q = 0; q < kQ; q++) s += mcoef(k, q) * mcoef(k, q);
+  return s;
+}
+// Opposite pairs (q, opp q) with q the first of the pair in index order.
+__host__ __device__ constexpr int pair_q(int i) {
+  return i == 0 ? 1 : i == 1 ? 3 : i == 2 ? 5 : i == 3 ? 7 : i == 4 ? 8 : i == 5 ? 11 : i == 6 ? 12 : i == 7 ? 15 : 16;
+}
+// even moments: symmetric under e -> -e; odd: antisymmetric.
+__host__ __device__ constexpr bool even_moment(int k) {
+  return !(k == 3 || k == 4 || k == 5 || k == 6 || k == 7 || k == 8 || k == 16 || k == 17 || k == 18);
+}
+
+// ---------------------------------------------------------------- constants
+struct MrtConstants {
+  double M[kQ][kQ];
+  double MI[kQ][kQ];  // Gauss-Jordan inverse, bit-identical to the reference's
+  double S[kQ];
+  double s_v, s_o;
+};
+bool build_mrt_constants(double nu, MrtConstants* out);
+
+// ---------------------------------------------------------------- geometry
+struct Geometry {
+  int nx = 0, ny = 0, nz = 0;
+  int count = 0;                 // fluid nodes
+  int npad = 0;                  // SoA stride (multiple of 256)
+  double porosity = 0.0;         // over the permeability window
+  std::vector<int32_t> coor;     // [count+1], ref id -> i*ny*nz + j*nz + k
+  std::vector<int32_t> ref_of;   // [count], internal index -> ref id (1-based)
+  std::vector<int32_t> int_of;   // [count+1], ref id -> internal index (row 0 = -1)
+  std::vector<int32_t> src;      // [18][npad], pull sources (flat index q*npad + m)
+  std::vector<uint8_t> in_window;// [count] internal order; empty = whole box
+  int window_volume = 0;
+};
+
+// Fluid-node compaction in the reference order (SP3:1018-1071).
+void compact_reference(const uint8_t* mask, int nx, int ny, int nz, Geometry* g);
+// Internal ordering: fills ref_of / int_of for the requested curve.
+void order_nodes(const uint8_t* mask, int ordering, Geometry* g);
+// Pull table in internal order with halfway bounce-back resolved.
+void build_pull_table(const uint8_t* mask, Geometry* g);
+// Push table nei_loc (reference form) from the pull table.
+void pull_to_push(const Geometry& g, int32_t* nei_loc);
+void set_window(const int window[6], Geometry* g);
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+lbm_status fail(lbm_status s, const std::string& msg);
+
+#define LBM_CUDA_TRY(expr)                                                               \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      return ::lbm::fail(_e == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,   \
+                         std::string(#expr) + ": " + cudaGetErrorString(_e));            \
+  } while (0)
+
+// ---------------------------------------------------------------- kernels
+// Storage kinds of the population arrays.
+enum class Store { F64 = 0, F32 = 1, F16 = 2, F64D = 3 };
+
+struct StepArgs {
+  const void* src_pop;   // [19][npad] post-collision of the previous step
+  void* dst_pop;         // [19][npad] this step's post-collision
+  const int32_t* table;  // [18][npad]
+  int n;                 // fluid nodes
+  int npad;
+  // macro input for a step that must use given rho/u (first step after init
+  // or restart); null otherwise
+  const void* rho_in;
+  const void* u_in;      // [3][npad]
+  // macro output of this step's pre-collision rho/u; null = not written
+  void* rho_out;
+  void* u_out;           // [3][npad]
+  double gx, gy, gz;
+  double s_v, s_o;
+  double fp16_scale;
+};
+cudaError_t launch_step(Store kind, const StepArgs& a, int block, cudaStream_t st);
+
+struct ReduceArgs {
+  const void* pop;        // [19][npad] post-collision of the last step
+  const int32_t* table;
+  int n, npad;
+  const void* rho_in;     // when the state is "given" (no step since set): use these
+  const void* u_in;
+  const void* u_prev;     // [3][npad] velocity one step earlier (null -> zero change)
+  int last_p;             // internal index of the reference's last node (excluded from Error)
+  const uint8_t* window;  // [n] or null
+  double gx, gy, gz;
+  double fp16_scale;
+  double* rho_out;        // optional double[n] (internal order)
+  double* u_out;          // optional double[3][npad]
+  double* partials;       // [blocks][8]
+  double* result;         // [8]
+};
+// result: t1, t2, t3, umax2, Qx, Qy, Qz, mass
+cudaError_t launch_reduce(Store kind, const ReduceArgs& a, cudaStream_t st);
+int reduce_blocks(int n);
+
+// f[(count+1)*19] reference AoS <-> device storage
+cudaError_t launch_export_pop(Store kind, const void* pop, const int32_t* table, const int32_t* ref_of,
+                              int n, int npad, double fp16_scale, double* out, cudaStream_t st);
+cudaError_t launch_import_pop(Store kind, void* pop, const int32_t* table, const int32_t* ref_of, int n,
+                              int npad, double fp16_scale, const double* in, cudaStream_t st);
+// rho/u reference-layout doubles -> device macro arrays of the storage's type
+cudaError_t launch_import_macro(Store kind, void* rho, void* u, const int32_t* ref_of, int n, int npad,
+                                const double* rho_in, const double* u_in, cudaStream_t st);
+cudaError_t launch_export_macro(const double* rho_int, const double* u_int, const int32_t* ref_of, int n,
+                                int npad, double* rho_ref, double* u_ref, cudaStream_t st);
+cudaError_t set_mi_constant(const double* mi361, cudaStream_t st);
+// uniform post-streaming state f_q = feq[q] at every node, written through
+// the inverse pull so the next step pulls exactly feq
+cudaError_t launch_init_uniform(Store kind, void* pop, const int32_t* table, int n, int npad, double fp16_scale,
+                                const double* feq19, cudaStream_t st);
+cudaError_t launch_fill_macro(Store kind, void* rho, void* u, int n, int npad, double rho0, const double* u3,
+                              cudaStream_t st);
+
+size_t store_bytes(Store kind);
+
+}  // namespace lbm

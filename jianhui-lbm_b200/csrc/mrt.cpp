@@ -1,0 +1,80 @@
+// MRT constants: the moment matrix, its inverse and the relaxation rates.
+#include <cmath>
+#include <utility>
+
+#include "lbm_internal.h"
+
+namespace lbm {
+
+namespace {
+
+// Full-pivot Gauss-Jordan inversion in place.  The reference computes M^-1
+// with this algorithm (SP3:797-836) and hard-codes its output as hex literals
+// in the collision (SP3:1745-1779).  The pivot search (first strictly larger
+// |a| in a row-major scan of the trailing block), the row/column swaps and
+// the update order are kept the same because they fix the rounding of every
+// entry, and the FP64 kernel reproduces the reference bit for bit only with
+// the same M^-1.
+template <int N>
+bool gauss_jordan_full_pivot(double (&a)[N][N]) {
+  int piv_r[N], piv_c[N];
+  for (int k = 0; k < N; k++) {
+    double amax = 0.0;
+    for (int i = k; i < N; i++)
+      for (int j = k; j < N; j++)
+        if (std::fabs(a[i][j]) > amax) {
+          amax = std::fabs(a[i][j]);
+          piv_r[k] = i;
+          piv_c[k] = j;
+        }
+    if (std::fabs(amax) < 1e-12) return false;
+    if (piv_r[k] != k)
+      for (int j = 0; j < N; j++) std::swap(a[k][j], a[piv_r[k]][j]);
+    if (piv_c[k] != k)
+      for (int i = 0; i < N; i++) std::swap(a[i][k], a[i][piv_c[k]]);
+    a[k][k] = 1 / a[k][k];
+    const double d = a[k][k];
+    for (int j = 0; j < N; j++)
+      if (j != k) a[k][j] *= d;
+    for (int i = 0; i < N; i++) {
+      if (i == k) continue;
+      for (int j = 0; j < N; j++)
+        if (j != k) a[i][j] -= a[i][k] * a[k][j];
+    }
+    for (int i = 0; i < N; i++)
+      if (i != k) a[i][k] *= -d;
+  }
+  for (int k = N - 1; k >= 0; k--) {
+    if (piv_c[k] != k)
+      for (int j = 0; j < N; j++) std::swap(a[k][j], a[piv_c[k]][j]);
+    if (piv_r[k] != k)
+      for (int i = 0; i < N; i++) std::swap(a[i][k], a[i][piv_r[k]]);
+  }
+  return true;
+}
+
+}  // namespace
+
+// Rates of `init` (SP3:1289-1322): lattice units (dx = dt = 1, c_s^2 = 1/3).
+bool build_mrt_constants(double nu, MrtConstants* out) {
+  for (int k = 0; k < kQ; k++)
+    for (int q = 0; q < kQ; q++) out->M[k][q] = mcoef(k, q);
+  for (int k = 0; k < kQ; k++)
+    for (int q = 0; q < kQ; q++) out->MI[k][q] = out->M[k][q];
+  if (!gauss_jordan_full_pivot<kQ>(out->MI)) return false;
+  const double lat_c = 1.0, dt = 1.0;
+  const double c_s2 = lat_c * lat_c / 3;
+  const double tau = nu / (c_s2 * dt) + 0.5;
+  const double s_v = 1 / tau;
+  const double s_o = 8 * (2 - s_v) / (8 - s_v);
+  const bool viscous[kQ] = {false, true, true, false, false, false, false, false, false, true,
+                            true,  true, true, true,  true,  true,  false, false, false};
+  const bool conserved[kQ] = {true, false, false, true, false, true, false, true, false, false,
+                              false, false, false, false, false, false, false, false, false};
+  for (int k = 0; k < kQ; k++) out->S[k] = conserved[k] ? 0.0 : (viscous[k] ? s_v : s_o);
+  out->s_v = s_v;
+  out->s_o = s_o;
+  return true;
+}
+
+}  // namespace lbm

@@ -1,0 +1,230 @@
+// Single-phase fused collide + pull-stream kernels in deviation storage
+// (FP32, FP16, FP64-fast) and the dispatch of every single-phase kernel.
+//
+// One thread owns one fluid node.  Per node and step it moves, from/to HBM:
+//   18 x int32 table entries (coalesced), 19 pulled populations (gathered
+//   through the table; neighbours are close in the node order), 19
+//   post-collision populations (coalesced stores)
+// = 2*19*s + 18*4 bytes, s = bytes per stored population.
+#include "kernels_common.cuh"
+
+namespace lbm {
+
+cudaError_t launch_step_f64(const StepArgs& a, int block, cudaStream_t st);
+cudaError_t reduce_f64(const ReduceArgs& a, cudaStream_t st);
+cudaError_t export_f64(const void*, const int32_t*, const int32_t*, int, int, double*, cudaStream_t);
+cudaError_t import_f64(void*, const int32_t*, const int32_t*, int, int, const double*, cudaStream_t);
+cudaError_t import_macro_f64(void*, void*, const int32_t*, int, int, const double*, const double*, cudaStream_t);
+
+template <Store K, int BS, bool GIVEN, bool WRITE>
+__global__ void __launch_bounds__(BS) step_dev_kernel(StepArgs a) {
+  using T = typename Traits<K>::T;
+  using A = typename Traits<K>::A;
+  using Mac = typename Traits<K>::Mac;
+  const int p = blockIdx.x * BS + threadIdx.x;
+  if (p >= a.n) return;
+  const T* __restrict__ src = static_cast<const T*>(a.src_pop);
+  T* __restrict__ dst = static_cast<T*>(a.dst_pop);
+  const float scale = (float)a.fp16_scale;
+  const float inv_scale = (float)(1.0 / a.fp16_scale);
+
+  A f[kQ];
+  f[0] = load_pop<K>(src + p, inv_scale);
+#pragma unroll
+  for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(src + __ldg(a.table + (size_t)(q - 1) * a.npad + p), inv_scale);
+
+  PairSplit<A> ps;
+  split_pairs(f, ps);
+  A drho, rho, ux, uy, uz;
+  if (GIVEN) {
+    const Mac* r = static_cast<const Mac*>(a.rho_in);
+    const Mac* u = static_cast<const Mac*>(a.u_in);
+    rho = (A)r[p];
+    drho = rho - A(1);
+    ux = (A)u[p];
+    uy = (A)u[a.npad + p];
+    uz = (A)u[2 * a.npad + p];
+  } else {
+    macro_dev<A>(f, ps, A(0.5 * a.gx), A(0.5 * a.gy), A(0.5 * a.gz), drho, rho, ux, uy, uz);
+  }
+  if (WRITE) {
+    static_cast<Mac*>(a.rho_out)[p] = (Mac)rho;
+    Mac* u = static_cast<Mac*>(a.u_out);
+    u[p] = (Mac)ux;
+    u[a.npad + p] = (Mac)uy;
+    u[2 * a.npad + p] = (Mac)uz;
+  }
+  mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(a.gx), A(a.gy), A(a.gz), A(a.s_v), A(a.s_o));
+#pragma unroll
+  for (int q = 0; q < kQ; q++) store_pop<K>(dst + (size_t)q * a.npad + p, f[q], scale);
+}
+
+template <Store K, int BS>
+static cudaError_t launch_dev_bs(const StepArgs& a, cudaStream_t st) {
+  const int grid = (a.n + BS - 1) / BS;
+  if (grid == 0) return cudaSuccess;
+  const bool given = a.rho_in != nullptr, write = a.rho_out != nullptr;
+  if (given && write)
+    step_dev_kernel<K, BS, true, true><<<grid, BS, 0, st>>>(a);
+  else if (given)
+    step_dev_kernel<K, BS, true, false><<<grid, BS, 0, st>>>(a);
+  else if (write)
+    step_dev_kernel<K, BS, false, true><<<grid, BS, 0, st>>>(a);
+  else
+    step_dev_kernel<K, BS, false, false><<<grid, BS, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <Store K>
+static cudaError_t launch_dev(const StepArgs& a, int block, cudaStream_t st) {
+  switch (block) {
+    case 64: return launch_dev_bs<K, 64>(a, st);
+    case 128: return launch_dev_bs<K, 128>(a, st);
+    case 512: return launch_dev_bs<K, 512>(a, st);
+    default: return launch_dev_bs<K, 256>(a, st);
+  }
+}
+
+cudaError_t launch_step(Store kind, const StepArgs& a, int block, cudaStream_t st) {
+  switch (kind) {
+    case Store::F64: return launch_step_f64(a, block, st);
+    case Store::F64D: return launch_dev<Store::F64D>(a, block, st);
+    case Store::F32: return launch_dev<Store::F32>(a, block, st);
+    case Store::F16: return launch_dev<Store::F16>(a, block, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int reduce_blocks(int n) {
+  const int b = (n + kReduceThreads - 1) / kReduceThreads;
+  return b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b);
+}
+
+cudaError_t launch_reduce(Store kind, const ReduceArgs& a, cudaStream_t st) {
+  switch (kind) {
+    case Store::F64: return reduce_f64(a, st);
+    case Store::F64D: return reduce_dispatch<Store::F64D>(a, st);
+    case Store::F32: return reduce_dispatch<Store::F32>(a, st);
+    case Store::F16: return reduce_dispatch<Store::F16>(a, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_export_pop(Store kind, const void* pop, const int32_t* table, const int32_t* ref_of, int n,
+                              int npad, double fp16_scale, double* out, cudaStream_t st) {
+  switch (kind) {
+    case Store::F64: return export_f64(pop, table, ref_of, n, npad, out, st);
+    case Store::F64D: return export_dispatch<Store::F64D>(pop, table, ref_of, n, npad, fp16_scale, out, st);
+    case Store::F32: return export_dispatch<Store::F32>(pop, table, ref_of, n, npad, fp16_scale, out, st);
+    case Store::F16: return export_dispatch<Store::F16>(pop, table, ref_of, n, npad, fp16_scale, out, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_import_pop(Store kind, void* pop, const int32_t* table, const int32_t* ref_of, int n, int npad,
+                              double fp16_scale, const double* in, cudaStream_t st) {
+  switch (kind) {
+    case Store::F64: return import_f64(pop, table, ref_of, n, npad, in, st);
+    case Store::F64D: return import_dispatch<Store::F64D>(pop, table, ref_of, n, npad, fp16_scale, in, st);
+    case Store::F32: return import_dispatch<Store::F32>(pop, table, ref_of, n, npad, fp16_scale, in, st);
+    case Store::F16: return import_dispatch<Store::F16>(pop, table, ref_of, n, npad, fp16_scale, in, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_import_macro(Store kind, void* rho, void* u, const int32_t* ref_of, int n, int npad,
+                                const double* rho_in, const double* u_in, cudaStream_t st) {
+  switch (kind) {
+    case Store::F64: return import_macro_f64(rho, u, ref_of, n, npad, rho_in, u_in, st);
+    case Store::F64D: return import_macro_dispatch<Store::F64D>(rho, u, ref_of, n, npad, rho_in, u_in, st);
+    case Store::F32: return import_macro_dispatch<Store::F32>(rho, u, ref_of, n, npad, rho_in, u_in, st);
+    case Store::F16: return import_macro_dispatch<Store::F16>(rho, u, ref_of, n, npad, rho_in, u_in, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+__global__ void export_macro_kernel(const double* __restrict__ rho_int, const double* __restrict__ u_int,
+                                    const int32_t* __restrict__ ref_of, int n, int npad, double* __restrict__ rho_ref,
+                                    double* __restrict__ u_ref) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int r = ref_of[p];
+  if (rho_ref) rho_ref[r] = rho_int[p];
+  if (u_ref) {
+    u_ref[(size_t)r * 3 + 0] = u_int[p];
+    u_ref[(size_t)r * 3 + 1] = u_int[npad + p];
+    u_ref[(size_t)r * 3 + 2] = u_int[2 * npad + p];
+  }
+}
+
+cudaError_t launch_export_macro(const double* rho_int, const double* u_int, const int32_t* ref_of, int n, int npad,
+                                double* rho_ref, double* u_ref, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  export_macro_kernel<<<(n + 255) / 256, 256, 0, st>>>(rho_int, u_int, ref_of, n, npad, rho_ref, u_ref);
+  return cudaGetLastError();
+}
+
+struct Feq19 {
+  double v[kQ];
+};
+
+template <Store K>
+__global__ void init_uniform_kernel(typename Traits<K>::T* __restrict__ pop, const int32_t* __restrict__ table, int n,
+                                    int npad, float scale, Feq19 feq) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  store_pop<K>(pop + p, from_full<K>(feq.v[0], 0), scale);
+#pragma unroll
+  for (int q = 1; q < kQ; q++)
+    store_pop<K>(pop + table[(size_t)(q - 1) * npad + p], from_full<K>(feq.v[q], q), scale);
+}
+
+template <typename Mac>
+__global__ void fill_macro_kernel(Mac* __restrict__ rho, Mac* __restrict__ u, int n, int npad, double rho0,
+                                  double ux, double uy, double uz) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  rho[p] = (Mac)rho0;
+  u[p] = (Mac)ux;
+  u[npad + p] = (Mac)uy;
+  u[2 * npad + p] = (Mac)uz;
+}
+
+cudaError_t launch_init_uniform(Store kind, void* pop, const int32_t* table, int n, int npad, double fp16_scale,
+                                const double* feq19, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  Feq19 f;
+  for (int q = 0; q < kQ; q++) f.v[q] = feq19[q];
+  const int g = (n + 255) / 256;
+  const float sc = (float)fp16_scale;
+  switch (kind) {
+    case Store::F64: init_uniform_kernel<Store::F64><<<g, 256, 0, st>>>((double*)pop, table, n, npad, sc, f); break;
+    case Store::F64D: init_uniform_kernel<Store::F64D><<<g, 256, 0, st>>>((double*)pop, table, n, npad, sc, f); break;
+    case Store::F32: init_uniform_kernel<Store::F32><<<g, 256, 0, st>>>((float*)pop, table, n, npad, sc, f); break;
+    case Store::F16: init_uniform_kernel<Store::F16><<<g, 256, 0, st>>>((__half*)pop, table, n, npad, sc, f); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_macro(Store kind, void* rho, void* u, int n, int npad, double rho0, const double* u3,
+                              cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int g = (n + 255) / 256;
+  if (kind == Store::F64 || kind == Store::F64D)
+    fill_macro_kernel<double><<<g, 256, 0, st>>>((double*)rho, (double*)u, n, npad, rho0, u3[0], u3[1], u3[2]);
+  else
+    fill_macro_kernel<float><<<g, 256, 0, st>>>((float*)rho, (float*)u, n, npad, rho0, u3[0], u3[1], u3[2]);
+  return cudaGetLastError();
+}
+
+size_t store_bytes(Store kind) {
+  switch (kind) {
+    case Store::F64:
+    case Store::F64D: return 8;
+    case Store::F32: return 4;
+    case Store::F16: return 2;
+  }
+  return 8;
+}
+
+}  // namespace lbm

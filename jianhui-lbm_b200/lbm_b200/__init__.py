@@ -1,0 +1,318 @@
+"""Python front-end of liblbm.so (the B200 sparse D3Q19 lattice Boltzmann library).
+
+This module only binds the C ABI declared in include/lbm.h with ctypes; all
+compute runs in the native library.  There is no fallback: if liblbm.so is
+missing or has no kernel image for the GPU, the import or the first call
+fails with an error.
+
+The names mirror the reference's solver surface (Single_Phase_3D/
+SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp): ``step`` is its time loop
+body (collision + comput_macro_variables), ``reduce`` is Error +
+Comput_Perm, ``fields``/``populations`` return the reference's rho/u/f arrays
+in its own id order and layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbm.so")
+
+PREC_F64, PREC_F32, PREC_F16, PREC_F64_FAST = 0, 1, 2, 3
+ORDER_REFERENCE, ORDER_MORTON, ORDER_HILBERT, ORDER_BRICK, ORDER_AUTO = 0, 1, 2, 3, -1
+
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16, "f64fast": PREC_F64_FAST}
+ORDERINGS = {"reference": ORDER_REFERENCE, "morton": ORDER_MORTON, "hilbert": ORDER_HILBERT,
+             "brick": ORDER_BRICK, "auto": ORDER_AUTO}
+
+STATUS = {
+    0: "LBM_OK", -1: "LBM_ERR_ARG", -2: "LBM_ERR_IO", -3: "LBM_ERR_OOM", -4: "LBM_ERR_CUDA",
+    -5: "LBM_ERR_NAN", -6: "LBM_ERR_NOT_CONVERGED", -7: "LBM_ERR_FORMAT", -8: "LBM_ERR_STATE",
+    -9: "LBM_ERR_OVERSPEED", -10: "LBM_ERR_NO_DEVICE",
+}
+
+
+class LbmError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nu", C.c_double), ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+        ("u_init", C.c_double * 3), ("precision", C.c_int), ("ordering", C.c_int),
+        ("block_size", C.c_int), ("perdir", C.c_int), ("window", C.c_int * 6),
+        ("fp16_scale", C.c_double), ("device", C.c_int),
+    ]
+
+
+class Diag(C.Structure):
+    _fields_ = [
+        ("step", C.c_longlong), ("perm", C.c_double * 3), ("perm_rel_change", C.c_double),
+        ("u_ave", C.c_double), ("u_max", C.c_double), ("u_rel_change", C.c_double),
+        ("u_mean_speed", C.c_double), ("mass", C.c_double), ("porosity", C.c_double),
+        ("nan_detected", C.c_int), ("converged", C.c_int),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["perm"] = list(self.perm)
+        return d
+
+
+class Input(C.Structure):
+    _fields_ = [
+        ("geometry_file", C.c_char * 128), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("n_max", C.c_int), ("reso", C.c_double), ("in_bc", C.c_int),
+        ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+        ("pre_xp", C.c_int), ("p_xp", C.c_double), ("pre_xn", C.c_int), ("p_xn", C.c_double),
+        ("pre_yp", C.c_int), ("p_yp", C.c_double), ("pre_yn", C.c_int), ("p_yn", C.c_double),
+        ("pre_zp", C.c_int), ("p_zp", C.c_double), ("pre_zn", C.c_int), ("p_zn", C.c_double),
+        ("vel_xp", C.c_int), ("v_xp", C.c_double), ("vel_xn", C.c_int), ("v_xn", C.c_double),
+        ("vel_yp", C.c_int), ("v_yp", C.c_double), ("vel_yn", C.c_int), ("v_yn", C.c_double),
+        ("vel_zp", C.c_int), ("v_zp", C.c_double), ("vel_zn", C.c_int), ("v_zn", C.c_double),
+        ("in_vis", C.c_double), ("inivx", C.c_double), ("inivy", C.c_double), ("inivz", C.c_double),
+        ("wr_per", C.c_int), ("perdir", C.c_int), ("fre_re", C.c_int), ("out_mode", C.c_int),
+        ("fre_ve", C.c_int), ("fre_de", C.c_int),
+        ("lattice_v", C.c_int), ("dx_input", C.c_double), ("dt_input", C.c_double),
+        ("output_path", C.c_char * 128), ("sub_bc", C.c_int), ("loc_perm", C.c_int),
+        ("par_per_x", C.c_int), ("par_per_y", C.c_int), ("par_per_z", C.c_int),
+        ("per_xp", C.c_int), ("per_xn", C.c_int), ("per_yp", C.c_int), ("per_yn", C.c_int),
+        ("per_zp", C.c_int), ("per_zn", C.c_int),
+        ("fre_backup", C.c_int), ("mode_backup_ini", C.c_int), ("vel_sol", C.c_int),
+        ("gperm", C.c_int), ("n_gperm", C.c_int * 4), ("size_gperm", C.c_int * 4),
+        ("c_gperm", (C.c_int * 3) * 4), ("decbin", C.c_int),
+        ("nnf_module", C.c_int), ("nnf_m", C.c_double), ("nnf_n", C.c_double),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for k, t in self._fields_:
+            v = getattr(self, k)
+            if isinstance(v, bytes):
+                v = v.decode()
+            elif hasattr(v, "__len__"):
+                v = [list(x) if hasattr(x, "__len__") else x for x in v]
+            out[k] = v
+        return out
+
+
+_lib = None
+_F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_U8P = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+# name -> (argtypes, restype)
+_SIGNATURES = {
+    "lbm_last_error": ([], C.c_char_p),
+    "lbm_status_string": ([C.c_int], C.c_char_p),
+    "lbm_abi_version": ([], C.c_int),
+    "lbm_params_default": ([C.POINTER(Params)], None),
+    "lbm_read_input": ([C.c_char_p, C.POINTER(Input)], C.c_int),
+    "lbm_read_mask": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, _U8P], C.c_int),
+    "lbm_create": ([C.POINTER(Params), _U8P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_create_from_input": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(Input)], C.c_int),
+    "lbm_destroy": ([C.c_void_p], None),
+    "lbm_step": ([C.c_void_p, C.c_int], C.c_int),
+    "lbm_reduce": ([C.c_void_p, C.POINTER(Diag)], C.c_int),
+    "lbm_run_to_convergence": ([C.c_void_p, C.c_double, C.c_int, C.c_int, C.POINTER(Diag)], C.c_int),
+    "lbm_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong)], C.c_int),
+    "lbm_get_fields": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "lbm_get_populations": ([C.c_void_p, _F64P], C.c_int),
+    "lbm_set_state": ([C.c_void_p, _F64P, _F64P, _F64P], C.c_int),
+    "lbm_export_compaction": ([C.c_void_p, _I32P], C.c_int),
+    "lbm_export_table": ([C.c_void_p, _I32P], C.c_int),
+    "lbm_autotune": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+    "lbm_last_step_ms": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "lbm_memory": ([C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_double)], C.c_int),
+}
+
+
+def lib():
+    """Loads liblbm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python jianhui-lbm_b200/build.py`")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGNATURES)
+
+
+def _check(status):
+    if status != 0:
+        raise LbmError(status, lib().lbm_last_error().decode(errors="replace"))
+
+
+def read_input(path):
+    """INPUT.dat of the single-phase solvers as a dict (field order SP3:283-340)."""
+    out = Input()
+    _check(lib().lbm_read_input(os.fsencode(path), C.byref(out)))
+    return out.as_dict()
+
+
+def read_mask(path, shape, decbin):
+    nx, ny, nz = shape
+    m = np.zeros(nx * ny * nz, dtype=np.uint8)
+    _check(lib().lbm_read_mask(os.fsencode(path), nx, ny, nz, int(decbin), m))
+    return m.reshape(nz, ny, nx)
+
+
+def default_params():
+    p = Params()
+    lib().lbm_params_default(C.byref(p))
+    return p
+
+
+class SinglePhase:
+    """One single-phase periodic solve resident on a GPU.
+
+    ``mask`` is a (nz, ny, nx) uint8 array, 0 = pore.  ``g`` is the body
+    force (acceleration), ``nu`` the kinematic viscosity (tau = 3 nu + 1/2).
+    """
+
+    def __init__(self, mask, nu, g=(1e-6, 0.0, 0.0), precision="f32", ordering="reference",
+                 block_size=256, u_init=(0.0, 0.0, 0.0), perdir=1, window=None, fp16_scale=0.0, device=0,
+                 _handle=None):
+        self._h = None
+        if _handle is not None:
+            self._h = _handle
+            self._load_info()
+            return
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        nz, ny, nx = mask.shape
+        p = default_params()
+        p.nu = float(nu)
+        p.gx, p.gy, p.gz = (float(x) for x in g)
+        p.u_init = (C.c_double * 3)(*[float(x) for x in u_init])
+        p.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p.ordering = ORDERINGS[ordering] if isinstance(ordering, str) else int(ordering)
+        p.block_size = int(block_size)
+        p.perdir = int(perdir)
+        if window is not None:
+            p.window = (C.c_int * 6)(*[int(x) for x in window])
+        p.fp16_scale = float(fp16_scale)
+        p.device = int(device)
+        h = C.c_void_p()
+        _check(lib().lbm_create(C.byref(p), mask.reshape(-1), nx, ny, nz, C.byref(h)))
+        self._h = h
+        self.shape = (nx, ny, nz)
+        self._load_info()
+
+    @classmethod
+    def from_input(cls, input_path, precision="f32", ordering="reference"):
+        h = C.c_void_p()
+        parsed = Input()
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        order = ORDERINGS[ordering] if isinstance(ordering, str) else int(ordering)
+        _check(lib().lbm_create_from_input(os.fsencode(input_path), prec, order, C.byref(h), C.byref(parsed)))
+        obj = cls(None, 0, _handle=h)
+        obj.input = parsed.as_dict()
+        obj.shape = (parsed.nx, parsed.ny, parsed.nz)
+        return obj
+
+    def _load_info(self):
+        c = C.c_int()
+        ph = C.c_double()
+        st = C.c_longlong()
+        _check(lib().lbm_info(self._h, C.byref(c), C.byref(ph), C.byref(st)))
+        self.count = c.value
+        self.porosity = ph.value
+
+    @property
+    def steps_done(self):
+        c = C.c_int()
+        ph = C.c_double()
+        st = C.c_longlong()
+        _check(lib().lbm_info(self._h, C.byref(c), C.byref(ph), C.byref(st)))
+        return st.value
+
+    def close(self):
+        if self._h:
+            lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, n=1):
+        _check(lib().lbm_step(self._h, int(n)))
+
+    def reduce(self):
+        d = Diag()
+        _check(lib().lbm_reduce(self._h, C.byref(d)))
+        return d.as_dict()
+
+    def run_to_convergence(self, tol=1e-6, check_every=100, max_steps=100000, raise_on_cap=False):
+        d = Diag()
+        st = lib().lbm_run_to_convergence(self._h, float(tol), int(check_every), int(max_steps), C.byref(d))
+        if st != 0 and (raise_on_cap or st != -6):
+            _check(st)
+        out = d.as_dict()
+        out["status"] = st
+        return out
+
+    def fields(self):
+        rho = np.zeros(self.count + 1)
+        u = np.zeros((self.count + 1) * 3)
+        _check(lib().lbm_get_fields(self._h, rho.ctypes.data, u.ctypes.data))
+        return rho, u.reshape(-1, 3)
+
+    def populations(self):
+        f = np.zeros((self.count + 1) * 19)
+        _check(lib().lbm_get_populations(self._h, f))
+        return f.reshape(-1, 19)
+
+    def set_state(self, rho, u, f):
+        _check(lib().lbm_set_state(self._h, np.ascontiguousarray(rho, dtype=np.float64).reshape(-1),
+                                   np.ascontiguousarray(u, dtype=np.float64).reshape(-1),
+                                   np.ascontiguousarray(f, dtype=np.float64).reshape(-1)))
+
+    def compaction(self):
+        c = np.zeros(self.count + 1, dtype=np.int32)
+        _check(lib().lbm_export_compaction(self._h, c))
+        return c
+
+    def table(self):
+        t = np.zeros((self.count + 1) * 19, dtype=np.int32)
+        _check(lib().lbm_export_table(self._h, t))
+        return t.reshape(-1, 19)
+
+    def autotune(self, trial_steps=20):
+        o = C.c_int()
+        b = C.c_int()
+        m = C.c_double()
+        _check(lib().lbm_autotune(self._h, int(trial_steps), C.byref(o), C.byref(b), C.byref(m)))
+        return {"ordering": o.value, "block": b.value, "mlups": m.value}
+
+    def last_step_ms(self):
+        v = C.c_double()
+        _check(lib().lbm_last_step_ms(self._h, C.byref(v)))
+        return v.value
+
+    def memory(self):
+        b = C.c_size_t()
+        bl = C.c_double()
+        _check(lib().lbm_memory(self._h, C.byref(b), C.byref(bl)))
+        return {"device_bytes": b.value, "bytes_per_lu": bl.value}

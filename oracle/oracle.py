@@ -1,0 +1,251 @@
+"""ctypes front-end of the oracle (TEST INFRASTRUCTURE ONLY).
+
+Two checkers live behind this module:
+
+* ``Restatement`` -- liboracle.so, the CPU restatement of the reference's
+  single-phase sparse update (lbm_oracle.c), plus the colour-gradient and
+  solute restatements.
+* ``ReferenceSP3`` -- _ref/libref_sp3.so, the reference solver
+  Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp compiled from
+  its own source with single-rank MPI/ParMETIS stand-ins (built by the
+  Makefile here when the reference sources are present; the prebuilt .so
+  travels with the repository snapshot otherwise).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+legs may import this module.  The product library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_U8P = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def build(quiet=True):
+    """Build liboracle.so (and _ref/ when the reference sources exist)."""
+    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def _load(name):
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        build()
+    return C.CDLL(path)
+
+
+def reference_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_sp3.so"))
+
+
+class Restatement:
+    """CPU restatement of the reference algorithm (lbm_oracle.c)."""
+
+    def __init__(self):
+        L = _load("liboracle.so")
+        self.L = L
+        L.orc_mrt_matrices.argtypes = [_F64P, _F64P]
+        L.orc_mrt_matrices.restype = C.c_int
+        L.orc_rates.argtypes = [C.c_double, _F64P]
+        L.orc_compact.argtypes = [_U8P, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.orc_compact.restype = C.c_int
+        L.orc_nei_loc.argtypes = [_U8P, C.c_int, C.c_int, C.c_int, _I32P, C.c_int, _I32P]
+        L.orc_sp_init.argtypes = [C.c_int, _F64P, _F64P, _F64P, _F64P]
+        L.orc_sp_step.argtypes = [C.c_int, _I32P, _F64P, _F64P, _F64P, C.c_double, C.c_double,
+                                  C.c_double, _F64P, _F64P, _F64P, _F64P, _F64P]
+        L.orc_sp_error.argtypes = [C.c_int, _F64P, _F64P, C.c_int, C.c_int, C.c_int, C.c_double,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_sp_error.restype = C.c_double
+        L.orc_sp_perm.argtypes = [C.c_int, _F64P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                  C.c_double, C.c_double, C.c_double, C.c_int, _F64P,
+                                  C.POINTER(C.c_double)]
+        L.orc_sp_perm.restype = C.c_double
+        L.orc_porosity.argtypes = [_U8P, C.c_int, C.c_int, C.c_int]
+        L.orc_porosity.restype = C.c_double
+
+    def matrices(self):
+        M = np.zeros((19, 19))
+        MI = np.zeros((19, 19))
+        ok = self.L.orc_mrt_matrices(M, MI)
+        assert ok == 1
+        return M, MI
+
+    def rates(self, nu):
+        S = np.zeros(19)
+        self.L.orc_rates(nu, S)
+        return S
+
+    def compact(self, mask):
+        nz, ny, nx = mask.shape
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        count = self.L.orc_compact(m, nx, ny, nz, None)
+        coor = np.zeros(count + 1, dtype=np.int32)
+        self.L.orc_compact(m, nx, ny, nz, coor.ctypes.data)
+        return coor
+
+    def nei_loc(self, mask, coor):
+        nz, ny, nx = mask.shape
+        count = coor.size - 1
+        nei = np.zeros((count + 1) * 19, dtype=np.int32)
+        self.L.orc_nei_loc(np.ascontiguousarray(mask, dtype=np.uint8), nx, ny, nz, coor, count, nei)
+        return nei.reshape(count + 1, 19)
+
+    def porosity(self, mask):
+        nz, ny, nx = mask.shape
+        return self.L.orc_porosity(np.ascontiguousarray(mask, dtype=np.uint8), nx, ny, nz)
+
+
+class SinglePhaseRun:
+    """A single-phase solve driven step by step through the restatement."""
+
+    def __init__(self, mask, nu, g=(1e-6, 0.0, 0.0), u_init=(0.0, 0.0, 0.0)):
+        self.R = Restatement()
+        self.mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        self.nz, self.ny, self.nx = mask.shape
+        self.coor = self.R.compact(self.mask)
+        self.count = self.coor.size - 1
+        self.nei = np.ascontiguousarray(self.R.nei_loc(self.mask, self.coor).reshape(-1))
+        self.M, self.MI = self.R.matrices()
+        self.M = np.ascontiguousarray(self.M.reshape(-1))
+        self.MI = np.ascontiguousarray(self.MI.reshape(-1))
+        self.S = self.R.rates(nu)
+        self.nu = nu
+        self.g = tuple(float(x) for x in g)
+        self.porosity = self.R.porosity(self.mask)
+        n = self.count + 1
+        self.rho = np.zeros(n)
+        self.u = np.zeros(n * 3)
+        self.u0 = np.zeros(n * 3)
+        self.f = np.zeros(n * 19)
+        self.F = np.zeros(n * 19)
+        self.perm_prev = np.zeros(3)
+        self.R.L.orc_sp_init(self.count, np.array(u_init, dtype=np.float64), self.rho, self.u, self.f)
+
+    def step(self, n=1):
+        for _ in range(n):
+            self.R.L.orc_sp_step(self.count, self.nei, self.M, self.MI, self.S, *self.g,
+                                 self.rho, self.u, self.u0, self.f, self.F)
+
+    def error(self):
+        um = C.c_double()
+        ua = C.c_double()
+        e = self.R.L.orc_sp_error(self.count, self.u, self.u0, self.nx, self.ny, self.nz,
+                                  self.porosity, C.byref(um), C.byref(ua))
+        return e, um.value, ua.value
+
+    def perm(self, perdir=1):
+        ua = C.c_double()
+        e = self.R.L.orc_sp_perm(self.count, self.u, self.nx, self.ny, self.nz, self.porosity, self.nu,
+                                 *self.g, perdir, self.perm_prev, C.byref(ua))
+        return e, self.perm_prev.copy(), ua.value
+
+    def fields(self):
+        return (self.f.reshape(-1, 19).copy(), self.u.reshape(-1, 3).copy(), self.rho.copy())
+
+
+class ReferenceSP3:
+    """The reference solver itself (compiled from its source), one rank.
+
+    The reference keeps its state in globals, so one instance per process is
+    meaningful at a time; ``create`` re-initialises it."""
+
+    _lib = None
+
+    def __init__(self, fast=False):
+        name = os.path.join("_ref", "libref_sp3_fast.so" if fast else "libref_sp3.so")
+        if not os.path.exists(os.path.join(HERE, name)):
+            build()
+        if not os.path.exists(os.path.join(HERE, name)):
+            raise FileNotFoundError(f"{name} not built (reference sources absent and no prebuilt library)")
+        L = C.CDLL(os.path.join(HERE, name))
+        self.L = L
+        L.ref_sp3_create.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                     C.c_double, C.c_double, C.c_double]
+        L.ref_sp3_create.restype = C.c_int
+        L.ref_sp3_step.argtypes = [C.c_int]
+        L.ref_sp3_error.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_sp3_error.restype = C.c_double
+        L.ref_sp3_perm.argtypes = [_F64P, C.POINTER(C.c_double)]
+        L.ref_sp3_perm.restype = C.c_double
+        L.ref_sp3_porosity.restype = C.c_double
+        L.ref_sp3_s_v.restype = C.c_double
+        for nm in ("get_f", "get_u", "get_rho", "get_M", "get_MI", "set_f", "set_u", "set_rho"):
+            getattr(L, "ref_sp3_" + nm).argtypes = [_F64P]
+        L.ref_sp3_get_coor.argtypes = [_I32P]
+        L.ref_sp3_get_nei_loc.argtypes = [_I32P]
+        self.count = 0
+
+    def create(self, mask, nu, g=(1e-6, 0.0, 0.0), binary=True, workdir=None):
+        from_path = None
+        nz, ny, nx = mask.shape
+        self.shape = (nx, ny, nz)
+        tmpdir = workdir or tempfile.mkdtemp(prefix="refsp3_")
+        from_path = os.path.join(tmpdir, "mask.bin" if binary else "mask.dat")
+        if binary:
+            arr = np.ascontiguousarray(np.transpose(mask, (2, 1, 0)).astype(np.int32))
+            arr.tofile(from_path)
+        else:
+            flat = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+            out = np.empty(flat.size * 2, dtype=np.uint8)
+            out[0::2] = flat + ord("0")
+            out[1::2] = ord("\n")
+            open(from_path, "wb").write(out.tobytes())
+        self.count = self.L.ref_sp3_create(from_path.encode(), nx, ny, nz, 1 if binary else 0, nu,
+                                           *[float(x) for x in g])
+        return self.count
+
+    def step(self, n=1):
+        self.L.ref_sp3_step(int(n))
+
+    def error(self):
+        um = C.c_double()
+        ua = C.c_double()
+        e = self.L.ref_sp3_error(C.byref(um), C.byref(ua))
+        return e, um.value, ua.value
+
+    def perm(self):
+        p = np.zeros(3)
+        ua = C.c_double()
+        e = self.L.ref_sp3_perm(p, C.byref(ua))
+        return e, p, ua.value
+
+    def coor(self):
+        out = np.zeros(self.count + 1, dtype=np.int32)
+        self.L.ref_sp3_get_coor(out)
+        return out
+
+    def nei_loc(self):
+        out = np.zeros((self.count + 1) * 19, dtype=np.int32)
+        self.L.ref_sp3_get_nei_loc(out)
+        return out.reshape(-1, 19)
+
+    def fields(self):
+        n = self.count + 1
+        f = np.zeros(n * 19)
+        u = np.zeros(n * 3)
+        r = np.zeros(n)
+        self.L.ref_sp3_get_f(f)
+        self.L.ref_sp3_get_u(u)
+        self.L.ref_sp3_get_rho(r)
+        return f.reshape(-1, 19), u.reshape(-1, 3), r
+
+    def matrices(self):
+        M = np.zeros(361)
+        MI = np.zeros(361)
+        self.L.ref_sp3_get_M(M)
+        self.L.ref_sp3_get_MI(MI)
+        return M.reshape(19, 19), MI.reshape(19, 19)
+
+    def porosity(self):
+        return self.L.ref_sp3_porosity()

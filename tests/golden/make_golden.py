@@ -1,0 +1,111 @@
+"""Generates the golden fixtures of this directory by running the reference
+solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
+compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
+
+    python tests/golden/make_golden.py [--cfg1]
+
+Fixtures (all inputs are stored with the outputs, so nothing depends on a
+random generator at test time):
+  sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
+                M^-1, f/u/rho after 20 steps, Error and Comput_Perm outputs
+  sp_24.npz     24^3 spheres, 200 steps: compaction digest, u, rho, f digest,
+                diagnostics
+  sp_cfg1.npz   64^3 spheres r=6, porosity 0.40, nu=1/6 (tau=1), gx=1e-6,
+                5000 steps (the reference's n_max=4999): diagnostics every 500
+                steps, digests of f and u, u of every 97th node  (--cfg1; ~8 min)
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "jianhui-lbm_b200"))
+
+import oracle  # noqa: E402
+from lbm_b200 import geometry as G  # noqa: E402
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def pack(mask):
+    return np.packbits(mask.reshape(-1).astype(np.uint8))
+
+
+def diag(ref):
+    e, umax, umean = ref.error()
+    pe, perm, uave = ref.perm()
+    return np.array([e, umax, umean, pe, perm[0], perm[1], perm[2], uave])
+
+
+def small(ref):
+    mask = G.overlapping_spheres((12, 10, 8), 0.6, 2.5, seed=11)
+    nu, g, steps = 0.1, (1e-5, 2e-6, -1e-6), 20
+    ref.create(mask, nu, g, binary=True)
+    coor, nei = ref.coor(), ref.nei_loc()
+    _, MI = ref.matrices()
+    ref.step(steps)
+    d = diag(ref)
+    f, u, rho = ref.fields()
+    np.savez_compressed(os.path.join(HERE, "sp_small.npz"), mask=pack(mask), shape=np.array(mask.shape), nu=nu,
+                        g=np.array(g), steps=steps, coor=coor, nei_loc=nei, MI=MI, f=f, u=u, rho=rho, diag=d)
+    print("sp_small", mask.shape, ref.count)
+
+
+def mid(ref):
+    mask = G.overlapping_spheres((24, 24, 24), 0.55, 4.0, seed=5)
+    nu, g, steps = 0.05, (1e-5, 0.0, 0.0), 200
+    ref.create(mask, nu, g, binary=False)  # exercises the ASCII reader too
+    coor = ref.coor()
+    nei = ref.nei_loc()
+    ref.step(steps - 1)
+    ref.step(1)
+    d = diag(ref)
+    f, u, rho = ref.fields()
+    np.savez_compressed(os.path.join(HERE, "sp_24.npz"), mask=pack(mask), shape=np.array(mask.shape), nu=nu,
+                        g=np.array(g), steps=steps, coor_digest=digest(coor), nei_digest=digest(nei), u=u, rho=rho,
+                        f_digest=digest(f), u_digest=digest(u), f_sample=f[1::53].copy(), diag=d)
+    print("sp_24", mask.shape, ref.count)
+
+
+def cfg1(ref):
+    mask = G.overlapping_spheres((64, 64, 64), 0.40, 6.0, seed=2024)
+    nu, g, steps, every = 0.16666666666666667, (1e-6, 0.0, 0.0), 5000, 500
+    ref.create(mask, nu, g, binary=True)
+    hist = []
+    done = 0
+    while done < steps:
+        ref.step(every)
+        done += every
+        hist.append([done] + list(diag(ref)))
+        print("cfg1", done, hist[-1][1:], flush=True)
+    f, u, rho = ref.fields()
+    np.savez_compressed(os.path.join(HERE, "sp_cfg1.npz"), mask=pack(mask), shape=np.array(mask.shape), nu=nu,
+                        g=np.array(g), steps=steps, every=every, history=np.array(hist), f_digest=digest(f),
+                        u_digest=digest(u), rho_digest=digest(rho), u_sample=u[1::97].copy(),
+                        f_sample=f[1::997].copy(), count=ref.count, porosity=ref.porosity())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cfg1", action="store_true")
+    a = ap.parse_args()
+    oracle.build()
+    ref = oracle.ReferenceSP3()
+    if a.cfg1:
+        cfg1(ref)
+    else:
+        small(ref)
+        mid(ref)
+
+
+if __name__ == "__main__":
+    main()
