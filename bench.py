@@ -90,7 +90,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -162,6 +162,9 @@ def barrier(pg):
 # ------------------------------------------------------------ reference arm
 def _ref_worker(args):
     sub, steps, warm = args
+    # the reference prints progress on stdout; keep the bench's stdout to its JSON line
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
     import oracle
 
     ref = oracle.ReferenceSP3(fast=True)
@@ -231,10 +234,12 @@ def run_ours(a):
 
     mask = workload_mask()
     # pick ordering / block size once (not timed), then build the timed solver with them
-    tune = {}
-    with lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering="reference", device=local) as s0:
-        tune = s0.autotune(trial_steps=10)
-    order, block = tune["ordering"], tune["block"]
+    if a.ordering == "auto":
+        with lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering="reference", device=local) as s0:
+            tune = s0.autotune(trial_steps=10)
+        order, block = tune["ordering"], tune["block"]
+    else:
+        order, block = lbm_b200.ORDERINGS[a.ordering], a.block
 
     s = lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering=order, block_size=block, device=local)
     count = s.count
@@ -251,9 +256,11 @@ def run_ours(a):
 
     # end to end through the C ABI from host buffers
     barrier(pg)
+    if a.skip_e2e:
+        t_e2e, count_e2e = None, count
     t0 = time.perf_counter()
     e = lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering=order, block_size=block, device=local)
-    left, reads = a.steps, 0
+    left, reads = (0 if a.skip_e2e else a.steps), 0
     while left > 0:
         k = min(100, left)
         e.step(k)
@@ -303,11 +310,14 @@ def run_ours(a):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ordering", default="auto", choices=["auto", "reference", "morton", "hilbert", "brick"])
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: no end-to-end pass")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

