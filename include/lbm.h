@@ -225,6 +225,32 @@ LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
  * bytes one fluid-node update moves (2*19*s + 18*4). */
 LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
 
+/* No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory (a host framework that owns every allocation and
+ * hands libraries its own arena, code in a region where cudaMalloc is not
+ * allowed or would synchronise the device).  It computes the same eight
+ * diagnostic sums as lbm_reduce -- sum |u - u_prev|^2, sum |u|^2, sum |u|,
+ * max |u|^2 (all without node skip_node, the reference's last node), Q_x,
+ * Q_y, Q_z, sum rho -- from caller-owned device arrays and writes them to
+ * result_dev[8], allocating nothing:
+ *   f_dev       post-streaming populations, FP64, f_q of node p at
+ *               f_dev[q*stride + p] (19 rows)
+ *   u_prev_dev  velocity one step earlier, [3][stride], or NULL (zero change)
+ *   n, stride   nodes and row stride (stride >= n)
+ *   stream      a cudaStream_t, or NULL for the default stream; the call is
+ *               asynchronous on it
+ * Its scratch (one row of partial sums per 2048-node tile) is a static
+ * device array of 512 KiB that every GPU loading the library holds until the
+ * process exits, so n is limited to 16,777,216 nodes; larger n is rejected
+ * with LBM_ERR_ARG.  The first call on a device looks up the array's device
+ * address (and loads the library's kernels there); make that first call
+ * before any stream capture.  All calls share the one array and every call
+ * overwrites it: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+LBM_API lbm_status lbm_reduce_noalloc(const double* f_dev, const double* u_prev_dev, int n, int stride,
+                                      int skip_node, double gx, double gy, double gz, double* result_dev,
+                                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

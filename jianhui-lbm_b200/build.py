@@ -31,6 +31,7 @@ INCLUDES = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
 CUDA_SOURCES = [
     ("sp_kernels.cu", []),
     ("sp_faithful.cu", ["-fmad=false"]),
+    ("reduce_noalloc.cu", ["-fmad=false"]),
 ]
 CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp"]
 

@@ -129,6 +129,8 @@ _SIGNATURES = {
     "lbm_autotune": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "lbm_last_step_ms": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
     "lbm_memory": ([C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_double)], C.c_int),
+    "lbm_reduce_noalloc": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                            C.c_void_p, C.c_void_p], C.c_int),
 }
 
 
