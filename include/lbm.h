@@ -225,6 +225,96 @@ LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
  * bytes one fluid-node update moves (2*19*s + 18*4). */
 LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
 
+/* ------------------------------------------ many independent solves (pool) */
+
+/* One single-phase permeability solve: geometry and physics (fully periodic,
+ * rest initial state, whole-box permeability window). */
+typedef struct lbm_instance {
+  const uint8_t* mask;  /* [nz][ny][nx], 0 = pore; copied by the library */
+  int nx, ny, nz;
+  double nu;            /* viscosity; tau = 3 nu + 1/2 */
+  double gx, gy, gz;    /* body force (acceleration) */
+} lbm_instance;
+
+/* Outcome of one solve run to the reference's stop test
+ * |(u_ave_prev - u_ave)/u_ave_prev| < tol checked every check_every steps
+ * (SP:812-816), u_ave and permeability from Comput_Perm (SP3:3611-3638). */
+typedef struct lbm_solve_result {
+  long long steps;   /* steps run */
+  int status;        /* LBM_OK converged, LBM_ERR_NOT_CONVERGED cap, LBM_ERR_NAN */
+  int count;         /* fluid nodes */
+  double perm[3];    /* Q_d / V * nu / g_d */
+  double u_ave;      /* |Q| / (V * porosity) */
+  double porosity;
+  double mass;       /* sum rho */
+} lbm_solve_result;
+
+typedef struct lbm_batch lbm_batch;
+
+/* Packs n solves of arbitrary sizes into one node pool (each instance a
+ * contiguous tile-aligned node range, its pull table pointing only into its
+ * own range) stepped by one persistent kernel per step inside CUDA graphs.
+ * precision: LBM_PREC_F32 or LBM_PREC_F16; ordering: node order inside each
+ * instance; block: 128/256/512 (0 = 256).  Replaces running the reference
+ * binary once per subsample. */
+LBM_API lbm_status lbm_batch_create(int n, const lbm_instance* inst, int precision, int ordering, int block,
+                                    int device, lbm_batch** out);
+/* Runs every instance to convergence (or max_steps); instances that converge
+ * stop stepping while the others continue.  results[n] may be NULL. */
+LBM_API lbm_status lbm_batch_run(lbm_batch* b, double tol, int check_every, long long max_steps,
+                                 lbm_solve_result* results);
+/* Puts every instance back to its initial state (rest, rho = 1). */
+LBM_API lbm_status lbm_batch_reset(lbm_batch* b);
+/* rho[(count_i+1)], u[(count_i+1)*3] of instance i in its reference id order. */
+LBM_API lbm_status lbm_batch_get_fields(lbm_batch* b, int i, double* rho, double* u);
+/* Picks the step block size and the node ordering by timing trial_steps
+ * steps of the whole batch for each candidate; resets the batch. */
+LBM_API lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* ordering_out, int* block_out,
+                                      double* mlups_out);
+/* total fluid nodes, device time of the last lbm_batch_run (ms), steps summed
+ * over instances in that run. */
+LBM_API lbm_status lbm_batch_info(lbm_batch* b, long long* total_nodes, double* last_run_ms,
+                                  long long* node_steps);
+LBM_API void lbm_batch_destroy(lbm_batch* b);
+
+/* ---------------------------------------- continuous-batching solve server */
+
+typedef struct lbm_server_config {
+  long long capacity_nodes;  /* HBM budget of the node pool, in fluid nodes */
+  int max_active;            /* slots: solves resident at once */
+  int precision;             /* LBM_PREC_F32 or LBM_PREC_F16 */
+  int ordering;              /* node order inside each solve */
+  int block;                 /* step block size (0 = 256) */
+  double tol;                /* stop test tolerance */
+  int check_every;           /* steps per device chain between admissions */
+  long long max_steps;       /* per-solve step cap */
+  int device;
+} lbm_server_config;
+
+typedef struct lbm_server_result {
+  long long request_id;
+  lbm_solve_result result;
+  double t_submit, t_admit, t_done;  /* seconds on the server's steady clock */
+} lbm_server_result;
+
+typedef struct lbm_server lbm_server;
+
+LBM_API void lbm_server_config_default(lbm_server_config* c);
+LBM_API lbm_status lbm_server_create(const lbm_server_config* c, lbm_server** out);
+/* Queues a solve (the mask is copied).  Requests larger than the whole pool
+ * are rejected with LBM_ERR_ARG. */
+LBM_API lbm_status lbm_server_submit(lbm_server* s, const lbm_instance* req, long long* request_id);
+/* One round: the resident solves advance check_every steps on the device
+ * while the host prepares queued requests; finished solves are retired and
+ * their nodes freed; queued requests are admitted (first fit, in arrival
+ * order with skip-ahead) as slots and pool memory allow. */
+LBM_API lbm_status lbm_server_pump(lbm_server* s, int* n_active, int* n_queued);
+/* Moves up to max finished results into out; *n_out = number written. */
+LBM_API lbm_status lbm_server_poll(lbm_server* s, lbm_server_result* out, int max, int* n_out);
+/* Seconds on the server's clock (the same clock as the result stamps). */
+LBM_API double lbm_server_now(lbm_server* s);
+LBM_API void lbm_server_destroy(lbm_server* s);
+
 /* No counterpart in the reference: an addition for callers that cannot
  * allocate device memory (a host framework that owns every allocation and
  * hands libraries its own arena, code in a region where cudaMalloc is not

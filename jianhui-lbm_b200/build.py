@@ -32,8 +32,9 @@ CUDA_SOURCES = [
     ("sp_kernels.cu", []),
     ("sp_faithful.cu", ["-fmad=false"]),
     ("reduce_noalloc.cu", ["-fmad=false"]),
+    ("batch_kernels.cu", []),
 ]
-CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp"]
+CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp"]
 
 
 def _headers():

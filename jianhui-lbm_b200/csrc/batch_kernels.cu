@@ -1,0 +1,257 @@
+// Many independent single-phase solves in one node pool.
+//
+// Layout: every instance owns a contiguous, tile-aligned node range
+// [begin, end) of one population pool pop[19][cap] and one pull table
+// [18][cap] whose entries are flat indices q*cap + m into the same pool (an
+// instance only ever pulls from its own range).  The pool is cut into tiles
+// of kTile nodes; tile_inst[t] names the instance slot owning tile t (-1 =
+// free).  One persistent kernel walks the tiles of all instances each step
+// and skips tiles of free or finished slots, so the launch shape -- and the
+// captured CUDA graph -- never changes while instances come and go.
+//
+// Convergence is decided on the device: every chain of check_every steps ends
+// with a per-tile sum of u, a per-instance sum of its tiles in fixed order
+// (results do not depend on what else is in the pool), and an update that
+// applies the reference's stop test |(u_ave_prev - u_ave)/u_ave_prev| < tol
+// (SP:812-816, u_ave from Comput_Perm SP3:3634-3638) per instance.
+#include "batch.h"
+#include "kernels_common.cuh"
+
+namespace lbm {
+
+template <Store K, int BS>
+__global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
+  using T = typename Traits<K>::T;
+  using A = typename Traits<K>::A;
+  const T* __restrict__ src = static_cast<const T*>(a.src_pop);
+  T* __restrict__ dst = static_cast<T*>(a.dst_pop);
+  const size_t cap = (size_t)a.cap;
+  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const int slot = a.tile_inst[t];
+    if (slot < 0) continue;
+    const InstParams ip = a.inst[slot];
+    if (!a.state[slot].active) continue;
+    const bool given = (chain_step == 0) && a.state[slot].fresh;
+    const float scale = ip.fp16_scale, inv_scale = 1.0f / ip.fp16_scale;
+#pragma unroll 1
+    for (int k = threadIdx.x; k < kTile; k += BS) {
+      const int p = t * kTile + k;
+      if (p >= ip.end) break;
+      A f[kQ];
+      f[0] = load_pop<K>(src + p, inv_scale);
+#pragma unroll
+      for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(src + __ldg(a.table + (size_t)(q - 1) * cap + p), inv_scale);
+      PairSplit<A> ps;
+      split_pairs(f, ps);
+      A drho, rho, ux, uy, uz;
+      if (given) {
+        rho = A(1);
+        drho = A(0);
+        ux = A(ip.u0[0]);
+        uy = A(ip.u0[1]);
+        uz = A(ip.u0[2]);
+      } else {
+        macro_dev<A>(f, ps, A(0.5f * ip.g[0]), A(0.5f * ip.g[1]), A(0.5f * ip.g[2]), drho, rho, ux, uy, uz);
+      }
+      mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(ip.g[0]), A(ip.g[1]), A(ip.g[2]), A(ip.s_v), A(ip.s_o));
+#pragma unroll
+      for (int q = 0; q < kQ; q++) store_pop<K>(dst + (size_t)q * cap + p, f[q], scale);
+    }
+  }
+}
+
+// Per-tile sum of u (and rho) over the post-streaming state, active slots only.
+template <Store K>
+__global__ void __launch_bounds__(kTile) batch_tile_sums_kernel(BatchReduceArgs a) {
+  using T = typename Traits<K>::T;
+  using A = typename Traits<K>::A;
+  __shared__ double smem[8 * 32];
+  const int t = blockIdx.x;
+  const int slot = a.tile_inst[t];
+  if (slot < 0 || !a.state[slot].active) return;  // whole block leaves together
+  const InstParams ip = a.inst[slot];
+  const T* __restrict__ pop = static_cast<const T*>(a.pop);
+  const size_t cap = (size_t)a.cap;
+  const float inv_scale = 1.0f / ip.fp16_scale;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int p = t * kTile + threadIdx.x;
+  if (p < ip.end) {
+    A f[kQ];
+    f[0] = load_pop<K>(pop + p, inv_scale);
+#pragma unroll
+    for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(pop + __ldg(a.table + (size_t)(q - 1) * cap + p), inv_scale);
+    PairSplit<A> ps;
+    split_pairs(f, ps);
+    A drho, rho, ux, uy, uz;
+    macro_dev<A>(f, ps, A(0.5f * ip.g[0]), A(0.5f * ip.g[1]), A(0.5f * ip.g[2]), drho, rho, ux, uy, uz);
+    acc[4] = ux;
+    acc[5] = uy;
+    acc[6] = uz;
+    acc[7] = rho;
+  }
+  block_reduce8(acc, a.tile_partials + (size_t)t * 8, smem);
+}
+
+// One block per active slot: its tiles' partials in index order, then the
+// stop test.  Deterministic: the sum order depends only on the instance.
+__global__ void __launch_bounds__(256) batch_update_kernel(BatchReduceArgs a, int chain_len, double tol,
+                                                           long long max_steps) {
+  __shared__ double smem[8 * 32];
+  __shared__ double tot[8];
+  const int slot = blockIdx.x;
+  if (slot >= a.nslots) return;
+  InstState& st = a.state[slot];
+  if (!st.active) return;
+  const InstParams ip = a.inst[slot];
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int t = ip.tile_begin + threadIdx.x; t < ip.tile_end; t += blockDim.x)
+#pragma unroll
+    for (int i = 4; i < 8; i++) acc[i] += a.tile_partials[(size_t)t * 8 + i];
+  block_reduce8(acc, tot, smem);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  st.steps += chain_len;
+  st.fresh = 0;
+  const double V = ip.volume, phi = ip.porosity;
+  double uave2 = 0.0;
+  for (int d = 0; d < 3; d++) {
+    st.q[d] = tot[4 + d];
+    const double c = tot[4 + d] / (V * phi);
+    uave2 += c * c;
+  }
+  st.mass = tot[7];
+  const double uave = sqrt(uave2);
+  const bool have_prev = st.checks > 0;
+  const bool conv = have_prev && fabs((st.uave - uave) / st.uave) < tol;
+  st.uave_prev = st.uave;
+  st.uave = uave;
+  st.checks += 1;
+  if (!(uave == uave)) {
+    st.active = 0;
+    st.done = 3;  // non-finite
+  } else if (conv) {
+    st.active = 0;
+    st.done = 1;
+  } else if (st.steps >= max_steps) {
+    st.active = 0;
+    st.done = 2;
+  }
+}
+
+// Post-streaming macro fields of one instance (reference layout, double).
+template <Store K>
+__global__ void batch_export_macro_kernel(const typename Traits<K>::T* __restrict__ pop, const int32_t* __restrict__ table,
+                                          int cap, int begin, int n, const int32_t* __restrict__ ref_of,
+                                          InstParams ip, double* __restrict__ rho_ref, double* __restrict__ u_ref) {
+  using A = typename Traits<K>::A;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = begin + i;
+  const float inv_scale = 1.0f / ip.fp16_scale;
+  A f[kQ];
+  f[0] = load_pop<K>(pop + p, inv_scale);
+#pragma unroll
+  for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(pop + table[(size_t)(q - 1) * cap + p], inv_scale);
+  PairSplit<A> ps;
+  split_pairs(f, ps);
+  A drho, rho, ux, uy, uz;
+  macro_dev<A>(f, ps, A(0.5f * ip.g[0]), A(0.5f * ip.g[1]), A(0.5f * ip.g[2]), drho, rho, ux, uy, uz);
+  const int r = ref_of[i];
+  if (rho_ref) rho_ref[r] = rho;
+  if (u_ref) {
+    u_ref[(size_t)r * 3 + 0] = ux;
+    u_ref[(size_t)r * 3 + 1] = uy;
+    u_ref[(size_t)r * 3 + 2] = uz;
+  }
+}
+
+// Uniform initial state feq(1, u0) of one instance's nodes, through the
+// inverse pull (the table is a permutation of the instance's slots).
+template <Store K>
+__global__ void batch_init_kernel(typename Traits<K>::T* __restrict__ pop, const int32_t* __restrict__ table, int cap,
+                                  int begin, int n, InstParams ip) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = begin + i;
+  const double u[3] = {ip.u0[0], ip.u0[1], ip.u0[2]};
+#pragma unroll
+  for (int q = 0; q < kQ; q++) {
+    const double eu = cx(q) * u[0] + cy(q) * u[1] + cz(q) * u[2];
+    const double uv = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const double feq = weight(q) * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv);
+    const size_t dst = q == 0 ? (size_t)p : (size_t)table[(size_t)(q - 1) * cap + p];
+    store_pop<K>(pop + dst, from_full<K>(feq, q), ip.fp16_scale);
+  }
+}
+
+template <Store K>
+static cudaError_t step_k(const BatchStepArgs& a, int block, int grid, int chain_step, cudaStream_t st) {
+  switch (block) {
+    case 128: batch_step_kernel<K, 128><<<grid, 128, 0, st>>>(a, chain_step); break;
+    case 512: batch_step_kernel<K, 512><<<grid, 512, 0, st>>>(a, chain_step); break;
+    default: batch_step_kernel<K, 256><<<grid, 256, 0, st>>>(a, chain_step); break;
+  }
+  return cudaGetLastError();
+}
+
+// Persistent launch shape: as many resident blocks as the SMs hold.
+int batch_step_grid(Store kind, int block) {
+  int dev = 0, sms = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaErrorInvalidValue;
+  if (kind == Store::F16) {
+    if (block == 128) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F16, 128>, 128, 0);
+    else if (block == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F16, 512>, 512, 0);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F16, 256>, 256, 0);
+  } else {
+    if (block == 128) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 128>, 128, 0);
+    else if (block == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 512>, 512, 0);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 256>, 256, 0);
+  }
+  if (e != cudaSuccess || per < 1) per = 1;
+  return sms * per;
+}
+
+cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int grid, int chain_step,
+                              cudaStream_t st) {
+  if (kind == Store::F16) return step_k<Store::F16>(a, block, grid, chain_step, st);
+  return step_k<Store::F32>(a, block, grid, chain_step, st);
+}
+
+cudaError_t launch_batch_check(Store kind, const BatchReduceArgs& a, int chain_len, double tol, long long max_steps,
+                               cudaStream_t st) {
+  if (a.ntiles > 0) {
+    if (kind == Store::F16)
+      batch_tile_sums_kernel<Store::F16><<<a.ntiles, kTile, 0, st>>>(a);
+    else
+      batch_tile_sums_kernel<Store::F32><<<a.ntiles, kTile, 0, st>>>(a);
+  }
+  if (a.nslots > 0) batch_update_kernel<<<a.nslots, 256, 0, st>>>(a, chain_len, tol, max_steps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_export_macro(Store kind, const void* pop, const int32_t* table, int cap, int begin, int n,
+                                      const int32_t* ref_of, const InstParams& ip, double* rho, double* u,
+                                      cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int g = (n + 255) / 256;
+  if (kind == Store::F16)
+    batch_export_macro_kernel<Store::F16><<<g, 256, 0, st>>>((const __half*)pop, table, cap, begin, n, ref_of, ip, rho, u);
+  else
+    batch_export_macro_kernel<Store::F32><<<g, 256, 0, st>>>((const float*)pop, table, cap, begin, n, ref_of, ip, rho, u);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_init(Store kind, void* pop, const int32_t* table, int cap, int begin, int n,
+                              const InstParams& ip, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int g = (n + 255) / 256;
+  if (kind == Store::F16)
+    batch_init_kernel<Store::F16><<<g, 256, 0, st>>>((__half*)pop, table, cap, begin, n, ip);
+  else
+    batch_init_kernel<Store::F32><<<g, 256, 0, st>>>((float*)pop, table, cap, begin, n, ip);
+  return cudaGetLastError();
+}
+
+}  // namespace lbm

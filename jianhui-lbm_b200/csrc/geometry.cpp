@@ -170,6 +170,32 @@ void pull_to_push(const Geometry& g, int32_t* nei) {
     }
 }
 
+// Table rows of one pool instance: row q-1 holds, for each of its nodes p
+// (internal order), the flat pool index of f_q's source: q*cap + begin + m for
+// the fluid cell m = p - e_q, or opp(q)*cap + begin + p (bounce-back).
+void fill_pool_rows(const uint8_t* mask, const Geometry& g, int64_t cap, int begin, int32_t* rows) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz, n = g.count;
+  std::vector<int32_t> cell_id((size_t)nx * ny * nz, -1);
+  for (int p = 0; p < n; p++) {
+    int i, j, k;
+    cell_of(g, g.ref_of[p], &i, &j, &k);
+    cell_id[i + (size_t)nx * (j + (size_t)ny * k)] = p;
+  }
+  for (int p = 0; p < n; p++) {
+    int i, j, k;
+    cell_of(g, g.ref_of[p], &i, &j, &k);
+    for (int q = 1; q < kQ; q++) {
+      int ip = i - cx(q), jp = j - cy(q), kp = k - cz(q);
+      ip = ip < 0 ? nx - 1 : (ip >= nx ? 0 : ip);
+      jp = jp < 0 ? ny - 1 : (jp >= ny ? 0 : jp);
+      kp = kp < 0 ? nz - 1 : (kp >= nz ? 0 : kp);
+      const size_t c = ip + (size_t)nx * (jp + (size_t)ny * kp);
+      const int64_t s = mask[c] == 0 ? (int64_t)q * cap + begin + cell_id[c] : (int64_t)opp(q) * cap + begin + p;
+      rows[(size_t)(q - 1) * n + p] = (int32_t)s;
+    }
+  }
+}
+
 // Permeability window (per_xn..per_zp, SP3:1005-1020, 3581-3590).
 void set_window(const int w[6], Geometry* g) {
   const bool full = (w[0] < 0 && w[1] < 0 && w[2] < 0 && w[3] < 0 && w[4] < 0 && w[5] < 0);

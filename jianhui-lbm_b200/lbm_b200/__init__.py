@@ -101,6 +101,31 @@ class Input(C.Structure):
         return out
 
 
+class Instance(C.Structure):
+    _fields_ = [("mask", C.c_void_p), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nu", C.c_double),
+                ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double)]
+
+
+class SolveResult(C.Structure):
+    _fields_ = [("steps", C.c_longlong), ("status", C.c_int), ("count", C.c_int), ("perm", C.c_double * 3),
+                ("u_ave", C.c_double), ("porosity", C.c_double), ("mass", C.c_double)]
+
+    def as_dict(self):
+        return {"steps": self.steps, "status": self.status, "count": self.count, "perm": list(self.perm),
+                "u_ave": self.u_ave, "porosity": self.porosity, "mass": self.mass}
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("capacity_nodes", C.c_longlong), ("max_active", C.c_int), ("precision", C.c_int),
+                ("ordering", C.c_int), ("block", C.c_int), ("tol", C.c_double), ("check_every", C.c_int),
+                ("max_steps", C.c_longlong), ("device", C.c_int)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("request_id", C.c_longlong), ("result", SolveResult), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
 _lib = None
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -131,7 +156,159 @@ _SIGNATURES = {
     "lbm_memory": ([C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_double)], C.c_int),
     "lbm_reduce_noalloc": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                             C.c_void_p, C.c_void_p], C.c_int),
+    "lbm_batch_create": ([C.c_int, C.POINTER(Instance), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+                         C.c_int),
+    "lbm_batch_run": ([C.c_void_p, C.c_double, C.c_int, C.c_longlong, C.POINTER(SolveResult)], C.c_int),
+    "lbm_batch_reset": ([C.c_void_p], C.c_int),
+    "lbm_batch_get_fields": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "lbm_batch_autotune": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
+                           C.c_int),
+    "lbm_batch_info": ([C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_longlong)], C.c_int),
+    "lbm_batch_destroy": ([C.c_void_p], None),
+    "lbm_server_config_default": ([C.POINTER(ServerConfig)], None),
+    "lbm_server_create": ([C.POINTER(ServerConfig), C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_server_submit": ([C.c_void_p, C.POINTER(Instance), C.POINTER(C.c_longlong)], C.c_int),
+    "lbm_server_pump": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "lbm_server_poll": ([C.c_void_p, C.POINTER(ServerResult), C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "lbm_server_now": ([C.c_void_p], C.c_double),
+    "lbm_server_destroy": ([C.c_void_p], None),
 }
+
+
+def _instance(mask, nu, g):
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    nz, ny, nx = m.shape
+    inst = Instance(m.ctypes.data, nx, ny, nz, float(nu), float(g[0]), float(g[1]), float(g[2]))
+    return inst, m
+
+
+class Batch:
+    """Many independent single-phase solves in one node pool on one GPU.
+
+    ``solves`` is a list of (mask, nu, g) tuples."""
+
+    def __init__(self, solves, precision="f32", ordering="reference", block=256, device=0):
+        keep = []
+        arr = (Instance * len(solves))()
+        for i, (mask, nu, g) in enumerate(solves):
+            arr[i], m = _instance(mask, nu, g)
+            keep.append(m)
+        h = C.c_void_p()
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        order = ORDERINGS[ordering] if isinstance(ordering, str) else int(ordering)
+        _check(lib().lbm_batch_create(len(solves), arr, prec, order, int(block), int(device), C.byref(h)))
+        self._h = h
+        self.n = len(solves)
+        self.counts = None
+
+    def run(self, tol=1e-6, check_every=100, max_steps=1_000_000):
+        res = (SolveResult * self.n)()
+        _check(lib().lbm_batch_run(self._h, float(tol), int(check_every), int(max_steps), res))
+        out = [r.as_dict() for r in res]
+        self.counts = [r["count"] for r in out]
+        return out
+
+    def reset(self):
+        _check(lib().lbm_batch_reset(self._h))
+
+    def fields(self, i):
+        if self.counts is None:
+            raise LbmError(-8, "run the batch before reading fields")
+        n = self.counts[i]
+        rho = np.zeros(n + 1)
+        u = np.zeros((n + 1) * 3)
+        _check(lib().lbm_batch_get_fields(self._h, int(i), rho.ctypes.data, u.ctypes.data))
+        return rho, u.reshape(-1, 3)
+
+    def autotune(self, trial_steps=20):
+        o, b, m = C.c_int(), C.c_int(), C.c_double()
+        _check(lib().lbm_batch_autotune(self._h, int(trial_steps), C.byref(o), C.byref(b), C.byref(m)))
+        return {"ordering": o.value, "block": b.value, "mlups": m.value}
+
+    def info(self):
+        t, ms, ns = C.c_longlong(), C.c_double(), C.c_longlong()
+        _check(lib().lbm_batch_info(self._h, C.byref(t), C.byref(ms), C.byref(ns)))
+        return {"total_nodes": t.value, "last_run_ms": ms.value, "node_steps": ns.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Server:
+    """Continuous-batching permeability solve server on one GPU."""
+
+    def __init__(self, capacity_nodes=64 * 1024 * 1024, max_active=256, precision="f32", ordering="reference",
+                 block=256, tol=1e-6, check_every=100, max_steps=1_000_000, device=0):
+        c = ServerConfig()
+        lib().lbm_server_config_default(C.byref(c))
+        c.capacity_nodes = int(capacity_nodes)
+        c.max_active = int(max_active)
+        c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        c.ordering = ORDERINGS[ordering] if isinstance(ordering, str) else int(ordering)
+        c.block = int(block)
+        c.tol = float(tol)
+        c.check_every = int(check_every)
+        c.max_steps = int(max_steps)
+        c.device = int(device)
+        h = C.c_void_p()
+        _check(lib().lbm_server_create(C.byref(c), C.byref(h)))
+        self._h = h
+
+    def submit(self, mask, nu, g):
+        inst, m = _instance(mask, nu, g)
+        rid = C.c_longlong()
+        _check(lib().lbm_server_submit(self._h, C.byref(inst), C.byref(rid)))
+        return rid.value
+
+    def pump(self):
+        a, q = C.c_int(), C.c_int()
+        _check(lib().lbm_server_pump(self._h, C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def poll(self, max_results=1024):
+        buf = (ServerResult * max_results)()
+        n = C.c_int()
+        _check(lib().lbm_server_poll(self._h, buf, max_results, C.byref(n)))
+        out = []
+        for r in buf[:n.value]:
+            d = r.result.as_dict()
+            d.update(request_id=r.request_id, t_submit=r.t_submit, t_admit=r.t_admit, t_done=r.t_done)
+            out.append(d)
+        return out
+
+    def now(self):
+        return lib().lbm_server_now(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def lib():
