@@ -307,8 +307,151 @@ def run_ours(a):
     return 0
 
 
+# ------------------------------------------------------------ batch / serve
+def shard(items, world, rank, weight):
+    """Greedy longest-first assignment of independent solves to ranks (no
+    collective needed: each rank runs its own share)."""
+    order = sorted(range(len(items)), key=lambda i: -weight(items[i]))
+    load = [0.0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda k: load[k])
+        load[r] += weight(items[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def run_batch(a):
+    """64 independent sphere packs to the 1e-6 stop test: one batched pool vs
+    the plain one-at-a-time GPU path, same tolerance."""
+    world, rank, local, pg = dist_setup()
+    import lbm_b200
+    from lbm_b200 import workloads as W
+
+    inst_all = W.config4_instances(64)
+    mine = shard(inst_all, world, rank, lambda x: float((x[0] == 0).sum()))
+    inst = [inst_all[i] for i in mine]
+    tol, every, cap = 1e-6, 100, 400000
+    with lbm_b200.Batch(inst, precision="f32", ordering="auto", block=0, device=local) as b:
+        tune = b.autotune(trial_steps=10)
+        b.reset()
+        barrier(pg)
+        t0 = time.perf_counter()
+        res = b.run(tol=tol, check_every=every, max_steps=cap)
+        t_batch = time.perf_counter() - t0
+        info = b.info()
+    singles, t_single = [], 0.0
+    for (mask, nu, g) in inst:
+        with lbm_b200.SinglePhase(mask, nu, g, precision="f32", device=local) as s:
+            t0 = time.perf_counter()
+            d = s.run_to_convergence(tol=tol, check_every=every, max_steps=cap)
+            t_single += time.perf_counter() - t0
+            singles.append(d)
+    t_batch = allmax(pg, t_batch)
+    t_single = allmax(pg, t_single)
+    if rank != 0:
+        return 0
+    dk = max(abs(r["perm"][0] - s["perm"][0]) / abs(s["perm"][0]) for r, s in zip(res, singles))
+    line = {"metric": "perm solves/s (batched)", "value": len(inst_all) / t_batch, "unit": "solves/s",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64 sphere packs, edge log-U[48,160], porosity U[0.25,0.5], r=5, tau=0.8, "
+                                   "gx=1e-6, stop test 1e-6 per 100 steps", "seed": 404,
+                       "ordering": tune["ordering"], "block": tune["block"]},
+            "one_at_a_time": {"value": len(inst_all) / t_single, "unit": "solves/s", "wall_s": t_single},
+            "batched_wall_s": t_batch, "speedup_vs_one_at_a_time": t_single / t_batch,
+            "fluid_nodes": info["total_nodes"], "node_steps": info["node_steps"],
+            "mlups_batched": info["node_steps"] / t_batch / 1e6,
+            "converged": sum(r["status"] == 0 for r in res), "max_rel_perm_diff_vs_one_at_a_time": dk}
+    print(json.dumps(line))
+    return 0
+
+
+def run_serve(a):
+    """Poisson request stream served by continuous batching; p50/p99 latency,
+    solves/s and the permeability error of a sample against FP64."""
+    world, rank, local, pg = dist_setup()
+    import lbm_b200
+    from lbm_b200 import workloads as W
+
+    reqs_all = W.config5_requests(n=a.requests, rate_per_s=a.rate)
+    mine = [i for i in range(len(reqs_all)) if i % world == rank]
+    reqs = [reqs_all[i] for i in mine]
+    tol, every = 1e-6, 100
+    lat, results, ids = [], {}, {}
+    with lbm_b200.Server(capacity_nodes=a.pool_nodes, max_active=64, precision="f32", tol=tol, check_every=every,
+                         max_steps=400000, device=local, target_active_nodes=a.target_nodes) as srv:
+        barrier(pg)
+        t0 = srv.now()
+        nxt = 0
+        while len(results) < len(reqs):
+            now = srv.now() - t0
+            while nxt < len(reqs) and reqs[nxt][0] <= now:
+                _, mask, nu, g = reqs[nxt]
+                ids[srv.submit(mask, nu, g)] = nxt
+                nxt += 1
+            active, queued = srv.pump()
+            for r in srv.poll():
+                results[ids[r["request_id"]]] = r
+            if active == 0 and queued == 0 and nxt < len(reqs):
+                time.sleep(max(0.0, reqs[nxt][0] - (srv.now() - t0)))
+        t_end = srv.now() - t0
+    for i, r in results.items():
+        lat.append(r["t_done"] - (t0 + reqs[i][0]))
+    # the plain one-at-a-time GPU path on the same stream: each request's solo
+    # solve time (single-domain FP32 solver, same stop test), served FIFO
+    solo = []
+    for (_, mask, nu, g) in reqs:
+        with lbm_b200.SinglePhase(mask, nu, g, precision="f32", device=local) as s:
+            ts = time.perf_counter()
+            s.run_to_convergence(tol=tol, check_every=every, max_steps=400000)
+            solo.append(time.perf_counter() - ts)
+    free_at, fifo_lat = 0.0, []
+    for (arr, _, _, _), d in zip(reqs, solo):
+        start = max(arr, free_at)
+        free_at = start + d
+        fifo_lat.append(free_at - arr)
+    fifo_lat = np.array(fifo_lat)
+    fifo_span = free_at - reqs[0][0] if reqs else 0.0
+    # FP64 check of a seeded sample of the requests
+    rng = np.random.default_rng(7)
+    sample = sorted(rng.choice(len(reqs), size=min(a.fp64_sample, len(reqs)), replace=False).tolist())
+    errs = []
+    for i in sample:
+        _, mask, nu, g = reqs[i]
+        with lbm_b200.SinglePhase(mask, nu, g, precision="f64", device=local) as s:
+            d = s.run_to_convergence(tol=tol, check_every=every, max_steps=400000)
+        errs.append(abs(results[i]["perm"][0] - d["perm"][0]) / abs(d["perm"][0]))
+    if rank != 0:
+        return 0
+    lat = np.array(lat)
+    line = {"metric": "perm solves/s (served), p50/p99 latency", "value": len(reqs) / t_end, "unit": "solves/s",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{a.requests} Poisson requests at {a.rate}/s, edge log-U[32,192], porosity "
+                                   "U[0.2,0.5], r U[3,8], gx=1e-6, tau=0.8, stop test 1e-6 per 100 steps",
+                       "seed": 505, "pool_nodes": a.pool_nodes, "target_active_nodes": a.target_nodes},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "makespan_s": t_end, "converged": sum(r["status"] == 0 for r in results.values()),
+            "one_at_a_time_fifo": {"solves_per_s": len(reqs) / (fifo_span + reqs[0][0]) if reqs else None,
+                                   "p50": float(np.percentile(fifo_lat, 50)),
+                                   "p99": float(np.percentile(fifo_lat, 99)),
+                                   "gpu_busy_s": float(sum(solo))},
+            "fp64_check": {"sample": len(sample), "max_rel_perm_err": max(errs) if errs else None}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve"],
+                    help="cfg2 = the headline single-domain bench; batch / serve = configs 4 / 5")
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=8.0)
+    ap.add_argument("--pool-nodes", type=int, default=96 * 1024 * 1024)
+    ap.add_argument("--fp64-sample", type=int, default=6)
+    ap.add_argument("--target-nodes", type=int, default=8 * 1024 * 1024,
+                    help="serve: resident-node target (0 = admit while memory allows)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
@@ -323,6 +466,10 @@ def main():
         a.warmup = 3
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "batch":
+        return run_batch(a)
+    if a.workload == "serve":
+        return run_serve(a)
     return run_ours(a)
 
 

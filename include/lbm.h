@@ -289,6 +289,10 @@ typedef struct lbm_server_config {
   int check_every;           /* steps per device chain between admissions */
   long long max_steps;       /* per-solve step cap */
   int device;
+  long long target_active_nodes; /* admit while resident nodes are below this
+                                    (0 = no limit but memory): enough nodes to
+                                    keep HBM busy, no more, so each resident
+                                    solve gets a large share of the device */
 } lbm_server_config;
 
 typedef struct lbm_server_result {

@@ -33,6 +33,7 @@ CUDA_SOURCES = [
     ("sp_faithful.cu", ["-fmad=false"]),
     ("reduce_noalloc.cu", ["-fmad=false"]),
     ("batch_kernels.cu", []),
+    ("setup_kernels.cu", []),
 ]
 CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp"]
 

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "lbm_internal.h"
+#include "setup.h"
 
 namespace lbm {
 
@@ -83,6 +84,10 @@ struct lbm_handle {
   // captured step chains, one per starting buffer
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_steps = 0;
+  // false when the layout was built on the device and the host copies of the
+  // compaction / node order (needed only for exports and re-layouts) are not
+  // built yet
+  bool host_geo = true;
 
   ~lbm_handle() {
     for (auto& g : graph)
@@ -119,7 +124,21 @@ lbm_status upload_layout(lbm_handle* h) {
   return LBM_OK;
 }
 
+// Host copies of the compaction and node order, built on first need.
+void ensure_host_geometry(lbm_handle* h) {
+  if (h->host_geo) return;
+  const int nx = h->geo.nx, ny = h->geo.ny, nz = h->geo.nz;
+  Geometry g;
+  compact_reference(h->mask.data(), nx, ny, nz, &g);
+  order_nodes(h->mask.data(), h->ordering, &g);
+  h->geo.coor = std::move(g.coor);
+  h->geo.ref_of = std::move(g.ref_of);
+  h->geo.int_of = std::move(g.int_of);
+  h->host_geo = true;
+}
+
 lbm_status layout(lbm_handle* h, int ordering) {
+  ensure_host_geometry(h);
   order_nodes(h->mask.data(), ordering, &h->geo);
   build_pull_table(h->mask.data(), &h->geo);
   set_window(h->prm.window, &h->geo);
@@ -397,13 +416,42 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
     }
     h->fp16_scale = sc;
   }
-  compact_reference(h->mask.data(), nx, ny, nz, &h->geo);
+  const int ord = p->ordering == LBM_ORDER_AUTO ? LBM_ORDER_REFERENCE : p->ordering;
+  const bool full_window = p->window[0] < 0 && p->window[1] < 0 && p->window[2] < 0 && p->window[3] < 0 &&
+                           p->window[4] < 0 && p->window[5] < 0;
+  const bool on_device = ord == LBM_ORDER_REFERENCE && full_window;
+  if (on_device) {
+    // count only; numbering and table are built on the device
+    const size_t cells = (size_t)nx * ny * nz;
+    long long pores = 0;
+    for (size_t c = 0; c < cells; c++) pores += (h->mask[c] == 0);
+    Geometry& g = h->geo;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.count = (int)pores;
+    g.npad = std::max(256, (int)(((pores + 255) / 256) * 256));
+    g.porosity = (double)pores / (double)cells;
+    g.window_volume = (int)cells;
+    h->host_geo = false;
+  } else {
+    compact_reference(h->mask.data(), nx, ny, nz, &h->geo);
+  }
   if (h->geo.count == 0) return fail(LBM_ERR_ARG, "geometry has no pore cells");
   if ((long long)h->geo.npad * kQ > (1LL << 31) - 1) return fail(LBM_ERR_ARG, "too many fluid nodes for int32 table");
   lbm_status st;
   if ((st = alloc_device(h.get())) != LBM_OK) return st;
-  const int ord = p->ordering == LBM_ORDER_AUTO ? LBM_ORDER_REFERENCE : p->ordering;
-  if ((st = layout(h.get(), ord)) != LBM_OK) return st;
+  if (on_device) {
+    SetupScratch scratch;
+    if ((st = device_index_reference(h->mask.data(), nx, ny, nz, h->geo.count, h->table.as<int32_t>(), h->geo.npad,
+                                     0, h->ref_of.as<int32_t>(), scratch, h->stream)) != LBM_OK)
+      return st;
+    h->ordering = LBM_ORDER_REFERENCE;
+    h->last_p = h->geo.count - 1;
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));  // before the scratch is freed
+  } else if ((st = layout(h.get(), ord)) != LBM_OK) {
+    return st;
+  }
   if ((st = init_state(h.get())) != LBM_OK) return st;
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   *out = h.release();
@@ -581,6 +629,7 @@ lbm_status lbm_set_state(lbm_handle* h, const double* rho, const double* u, cons
 
 lbm_status lbm_export_compaction(lbm_handle* h, int32_t* coor) {
   if (!h || !coor) return fail(LBM_ERR_ARG, "lbm_export_compaction: null argument");
+  ensure_host_geometry(h);
   std::memcpy(coor, h->geo.coor.data(), sizeof(int32_t) * (size_t)(h->geo.count + 1));
   return LBM_OK;
 }
@@ -590,7 +639,9 @@ lbm_status lbm_export_table(lbm_handle* h, int32_t* nei_loc) {
   if (st != LBM_OK) return st;
   if (!nei_loc) return fail(LBM_ERR_ARG, "lbm_export_table: null output");
   // round-trip through the device copy so the exported table is the one the kernels read
+  ensure_host_geometry(h);
   Geometry g = h->geo;
+  g.src.assign((size_t)18 * g.npad, 0);
   LBM_CUDA_TRY(cudaMemcpyAsync(g.src.data(), h->table.p, sizeof(int32_t) * 18 * (size_t)g.npad, cudaMemcpyDeviceToHost,
                                h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));

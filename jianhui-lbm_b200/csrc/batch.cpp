@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "batch.h"
+#include "setup.h"
 
 namespace lbm {
 
@@ -52,9 +53,25 @@ struct Job {
   double t_submit = 0, t_admit = 0;
 };
 
+// Host part of a solve's layout.  In the reference node order the numbering
+// and the table are built on the device at admission, so the host only
+// counts pores; other orders are built here.
 void build_job(Job* j, int ordering) {
-  compact_reference(j->mask.data(), j->nx, j->ny, j->nz, &j->geo);
-  order_nodes(j->mask.data(), ordering, &j->geo);
+  if (ordering == LBM_ORDER_REFERENCE) {
+    const size_t cells = (size_t)j->nx * j->ny * j->nz;
+    long long pores = 0;
+    const uint8_t* m = j->mask.data();
+    for (size_t c = 0; c < cells; c++) pores += (m[c] == 0);
+    j->geo = Geometry{};
+    j->geo.nx = j->nx;
+    j->geo.ny = j->ny;
+    j->geo.nz = j->nz;
+    j->geo.count = (int)pores;
+    j->geo.porosity = (double)pores / (double)cells;
+  } else {
+    compact_reference(j->mask.data(), j->nx, j->ny, j->nz, &j->geo);
+    order_nodes(j->mask.data(), ordering, &j->geo);
+  }
   j->built = true;
 }
 
@@ -83,7 +100,8 @@ struct Pool {
   int block = 256, grid = 0;
   int ordering = LBM_ORDER_REFERENCE;
   double fp16_scale = 1.0;
-  Buf pop[2], table, tile_inst, inst, state, partials;
+  Buf pop[2], table, tile_inst, inst, state, partials, active_tiles, n_active;
+  SetupScratch setup;
   std::vector<InstParams> h_inst;
   InstState* h_state = nullptr;  // pinned
   std::vector<int> h_tile_inst;
@@ -135,6 +153,9 @@ struct Pool {
     LBM_CUDA_TRY(inst.alloc((size_t)nslots * sizeof(InstParams)));
     LBM_CUDA_TRY(state.alloc((size_t)nslots * sizeof(InstState)));
     LBM_CUDA_TRY(partials.alloc((size_t)ntiles * 8 * sizeof(double)));
+    LBM_CUDA_TRY(active_tiles.alloc((size_t)ntiles * sizeof(int)));
+    LBM_CUDA_TRY(n_active.alloc(sizeof(int)));
+    LBM_CUDA_TRY(cudaMemsetAsync(n_active.p, 0, sizeof(int), stream));
     LBM_CUDA_TRY(cudaMallocHost((void**)&h_state, (size_t)nslots * sizeof(InstState)));
     std::memset(h_state, 0, (size_t)nslots * sizeof(InstState));
     h_inst.assign(nslots, InstParams{});
@@ -208,12 +229,19 @@ struct Pool {
     Job& j = *slot_job[slot];
     const InstParams ip = params_of(j, tile0);
     h_inst[slot] = ip;
-    std::vector<int32_t> rows((size_t)18 * j.geo.count);
-    fill_pool_rows(j.mask.data(), j.geo, cap, ip.begin, rows.data());
-    for (int q = 1; q < kQ; q++)
-      LBM_CUDA_TRY(cudaMemcpyAsync(table.as<int32_t>() + (size_t)(q - 1) * cap + ip.begin,
-                                   rows.data() + (size_t)(q - 1) * j.geo.count, sizeof(int32_t) * j.geo.count,
-                                   cudaMemcpyHostToDevice, stream));
+    if (ordering == LBM_ORDER_REFERENCE) {
+      lbm_status st = device_index_reference(j.mask.data(), j.nx, j.ny, j.nz, j.geo.count, table.as<int32_t>(), cap,
+                                             ip.begin, nullptr, setup, stream);
+      if (st != LBM_OK) return st;
+    } else {
+      std::vector<int32_t> rows((size_t)18 * j.geo.count);
+      fill_pool_rows(j.mask.data(), j.geo, cap, ip.begin, rows.data());
+      for (int q = 1; q < kQ; q++)
+        LBM_CUDA_TRY(cudaMemcpyAsync(table.as<int32_t>() + (size_t)(q - 1) * cap + ip.begin,
+                                     rows.data() + (size_t)(q - 1) * j.geo.count, sizeof(int32_t) * j.geo.count,
+                                     cudaMemcpyHostToDevice, stream));
+      LBM_CUDA_TRY(cudaStreamSynchronize(stream));  // rows is a host temporary
+    }
     for (int t = ip.tile_begin; t < ip.tile_end; t++) h_tile_inst[t] = slot;
     LBM_CUDA_TRY(cudaMemcpyAsync(tile_inst.as<int>() + ip.tile_begin, h_tile_inst.data() + ip.tile_begin,
                                  sizeof(int) * (ip.tile_end - ip.tile_begin), cudaMemcpyHostToDevice, stream));
@@ -255,6 +283,8 @@ struct Pool {
     a.tile_inst = tile_inst.as<int>();
     a.inst = inst.as<InstParams>();
     a.state = state.as<InstState>();
+    a.active_tiles = active_tiles.as<int>();
+    a.n_active = n_active.as<int>();
     return a;
   }
   BatchReduceArgs reduce_args(int c) const {
@@ -268,13 +298,17 @@ struct Pool {
     r.state = state.as<InstState>();
     r.nslots = nslots;
     r.tile_partials = partials.as<double>();
+    r.active_tiles = active_tiles.as<int>();
+    r.n_active = n_active.as<int>();
     return r;
   }
 
   lbm_status capture(int c0, int chain, double tol, long long max_steps) {
     cudaGraph_t g = nullptr;
     LBM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t err = cudaSuccess;
+    // the chain starts from the current set of stepping slots (admissions and
+    // retirements happen between chains)
+    cudaError_t err = launch_batch_list(reduce_args(c0), stream);
     int c = c0;
     for (int s = 0; s < chain && err == cudaSuccess; s++) {
       err = launch_batch_step(kind, step_args(c), block, grid, s, stream);
@@ -341,7 +375,14 @@ struct Pool {
     LBM_CUDA_TRY(ref.alloc(sizeof(int32_t) * n));
     LBM_CUDA_TRY(r.alloc(sizeof(double) * (n + 1)));
     LBM_CUDA_TRY(v.alloc(sizeof(double) * 3 * (n + 1)));
-    LBM_CUDA_TRY(cudaMemcpyAsync(ref.p, j.geo.ref_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
+    std::vector<int32_t> iota;
+    const int32_t* ref_src = j.geo.ref_of.data();
+    if (j.geo.ref_of.empty()) {  // reference order: internal index p is reference id p + 1
+      iota.resize(n);
+      for (int p = 0; p < n; p++) iota[p] = p + 1;
+      ref_src = iota.data();
+    }
+    LBM_CUDA_TRY(cudaMemcpyAsync(ref.p, ref_src, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
     LBM_CUDA_TRY(cudaMemsetAsync(r.p, 0, r.bytes, stream));
     LBM_CUDA_TRY(cudaMemsetAsync(v.p, 0, v.bytes, stream));
     LBM_CUDA_TRY(launch_batch_export_macro(kind, pop[slot_parity[slot]].p, table.as<int32_t>(), cap, ip.begin, n,
@@ -562,6 +603,7 @@ lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* ordering_out, 
       P.block = bl;
       P.grid = batch_step_grid(P.kind, bl);
       if ((st = batch_reset(b)) != LBM_OK) return st;
+      LBM_CUDA_TRY(launch_batch_list(P.reduce_args(P.cur), P.stream));
       for (int s = 0; s < 2; s++) {  // warm-up
         LBM_CUDA_TRY(launch_batch_step(P.kind, P.step_args(P.cur), P.block, P.grid, s, P.stream));
         P.cur = 1 - P.cur;
@@ -703,10 +745,16 @@ lbm_status lbm_server_pump(lbm_server* s, int* n_active, int* n_queued) {
       if ((st = P.unplace(i)) != LBM_OK) return st;
     }
   }
-  // 4. admit waiting requests while slots and contiguous nodes allow
+  // 4. admit waiting requests while slots, contiguous nodes and the
+  //    saturation target allow
+  long long resident = 0;
+  for (int i = 0; i < P.nslots; i++)
+    if (P.slot_job[i]) resident += P.slot_job[i]->geo.count;
   for (auto it = s->queue.begin(); it != s->queue.end();) {
     Job& j = **it;
     if (!j.built) build_job(&j, P.ordering);
+    if (s->cfg.target_active_nodes > 0 && resident > 0 && resident + j.geo.count > s->cfg.target_active_nodes)
+      break;  // in arrival order: later requests wait too
     const int slot = P.free_slot();
     if (slot < 0) break;
     const int t0 = P.alloc_tiles((j.geo.count + kTile - 1) / kTile);
@@ -715,6 +763,7 @@ lbm_status lbm_server_pump(lbm_server* s, int* n_active, int* n_queued) {
       continue;
     }
     j.t_admit = s->now();
+    resident += j.geo.count;
     P.slot_job[slot] = std::move(*it);
     it = s->queue.erase(it);
     if ((st = P.place(slot, t0)) != LBM_OK) return st;

@@ -40,6 +40,8 @@ struct BatchStepArgs {
   const int* tile_inst;
   const InstParams* inst;
   const InstState* state;
+  const int* active_tiles;  // tiles of stepping slots, ascending
+  const int* n_active;      // its length (device scalar)
 };
 
 struct BatchReduceArgs {
@@ -52,7 +54,12 @@ struct BatchReduceArgs {
   InstState* state;
   int nslots;
   double* tile_partials;  // [ntiles][8]
+  int* active_tiles;
+  int* n_active;
 };
+
+// Rebuilds the active tile list from tile ownership and slot states.
+cudaError_t launch_batch_list(const BatchReduceArgs& a, cudaStream_t st);
 
 cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int grid, int chain_step,
                               cudaStream_t st);

@@ -26,11 +26,11 @@ __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int cha
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
   const size_t cap = (size_t)a.cap;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+  const int na = *a.n_active;
+  for (int i = blockIdx.x; i < na; i += gridDim.x) {
+    const int t = a.active_tiles[i];
     const int slot = a.tile_inst[t];
-    if (slot < 0) continue;
     const InstParams ip = a.inst[slot];
-    if (!a.state[slot].active) continue;
     const bool given = (chain_step == 0) && a.state[slot].fresh;
     const float scale = ip.fp16_scale, inv_scale = 1.0f / ip.fp16_scale;
 #pragma unroll 1
@@ -60,16 +60,43 @@ __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int cha
   }
 }
 
-// Per-tile sum of u (and rho) over the post-streaming state, active slots only.
+// Active tile list: one block scans tile ownership in index order.
+__global__ void __launch_bounds__(1024) batch_list_kernel(BatchReduceArgs a) {
+  __shared__ int counts[1024];
+  const int chunk = (a.ntiles + 1023) / 1024;
+  const int lo = threadIdx.x * chunk, hi = min(lo + chunk, a.ntiles);
+  int c = 0;
+  for (int t = lo; t < hi; t++) {
+    const int s = a.tile_inst[t];
+    c += (s >= 0 && a.state[s].active);
+  }
+  counts[threadIdx.x] = c;
+  __syncthreads();
+  // inclusive scan (Hillis-Steele)
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int v = threadIdx.x >= off ? counts[threadIdx.x - off] : 0;
+    __syncthreads();
+    counts[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int w = counts[threadIdx.x] - c;
+  for (int t = lo; t < hi; t++) {
+    const int s = a.tile_inst[t];
+    if (s >= 0 && a.state[s].active) a.active_tiles[w++] = t;
+  }
+  if (threadIdx.x == 1023) *a.n_active = counts[1023];
+}
+
+cudaError_t launch_batch_list(const BatchReduceArgs& a, cudaStream_t st) {
+  batch_list_kernel<<<1, 1024, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Sum of u (and rho) over one tile's post-streaming state.
 template <Store K>
-__global__ void __launch_bounds__(kTile) batch_tile_sums_kernel(BatchReduceArgs a) {
+__device__ __forceinline__ void batch_tile_sum(const BatchReduceArgs& a, int t, const InstParams& ip, double* smem) {
   using T = typename Traits<K>::T;
   using A = typename Traits<K>::A;
-  __shared__ double smem[8 * 32];
-  const int t = blockIdx.x;
-  const int slot = a.tile_inst[t];
-  if (slot < 0 || !a.state[slot].active) return;  // whole block leaves together
-  const InstParams ip = a.inst[slot];
   const T* __restrict__ pop = static_cast<const T*>(a.pop);
   const size_t cap = (size_t)a.cap;
   const float inv_scale = 1.0f / ip.fp16_scale;
@@ -90,6 +117,19 @@ __global__ void __launch_bounds__(kTile) batch_tile_sums_kernel(BatchReduceArgs 
     acc[7] = rho;
   }
   block_reduce8(acc, a.tile_partials + (size_t)t * 8, smem);
+}
+
+// Persistent over the active tile list.
+template <Store K>
+__global__ void __launch_bounds__(kTile) batch_tile_sums_kernel(BatchReduceArgs a) {
+  __shared__ double smem[8 * 32];
+  const int na = *a.n_active;
+  for (int i = blockIdx.x; i < na; i += gridDim.x) {
+    const int t = a.active_tiles[i];
+    const InstParams ip = a.inst[a.tile_inst[t]];
+    batch_tile_sum<K>(a, t, ip, smem);
+    __syncthreads();  // smem is reused by the next tile
+  }
 }
 
 // One block per active slot: its tiles' partials in index order, then the
@@ -222,10 +262,14 @@ cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int
 cudaError_t launch_batch_check(Store kind, const BatchReduceArgs& a, int chain_len, double tol, long long max_steps,
                                cudaStream_t st) {
   if (a.ntiles > 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::min(a.ntiles, 2 * sms);
     if (kind == Store::F16)
-      batch_tile_sums_kernel<Store::F16><<<a.ntiles, kTile, 0, st>>>(a);
+      batch_tile_sums_kernel<Store::F16><<<grid, kTile, 0, st>>>(a);
     else
-      batch_tile_sums_kernel<Store::F32><<<a.ntiles, kTile, 0, st>>>(a);
+      batch_tile_sums_kernel<Store::F32><<<grid, kTile, 0, st>>>(a);
   }
   if (a.nslots > 0) batch_update_kernel<<<a.nslots, 256, 0, st>>>(a, chain_len, tol, max_steps);
   return cudaGetLastError();

@@ -118,7 +118,7 @@ class SolveResult(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("capacity_nodes", C.c_longlong), ("max_active", C.c_int), ("precision", C.c_int),
                 ("ordering", C.c_int), ("block", C.c_int), ("tol", C.c_double), ("check_every", C.c_int),
-                ("max_steps", C.c_longlong), ("device", C.c_int)]
+                ("max_steps", C.c_longlong), ("device", C.c_int), ("target_active_nodes", C.c_longlong)]
 
 
 class ServerResult(C.Structure):
@@ -252,9 +252,10 @@ class Server:
     """Continuous-batching permeability solve server on one GPU."""
 
     def __init__(self, capacity_nodes=64 * 1024 * 1024, max_active=256, precision="f32", ordering="reference",
-                 block=256, tol=1e-6, check_every=100, max_steps=1_000_000, device=0):
+                 block=256, tol=1e-6, check_every=100, max_steps=1_000_000, device=0, target_active_nodes=0):
         c = ServerConfig()
         lib().lbm_server_config_default(C.byref(c))
+        c.target_active_nodes = int(target_active_nodes)
         c.capacity_nodes = int(capacity_nodes)
         c.max_active = int(max_active)
         c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)

@@ -53,12 +53,10 @@ def _stamp_ball(mask, cz, cy, cx, r):
     iz = (zz % nz)[:, None, None]
     iy = (yy % ny)[None, :, None]
     ix = (xx % nx)[None, None, :]
-    sel = np.broadcast_to(inside, d2.shape)
-    tz = np.broadcast_to(iz, d2.shape)[sel]
-    ty = np.broadcast_to(iy, d2.shape)[sel]
-    tx = np.broadcast_to(ix, d2.shape)[sel]
-    # a wrapped ball larger than the box can hit a cell twice; count unique cells
-    flat = np.unique((tz * ny + ty) * nx + tx)
+    flat = ((iz * ny + iy) * nx + ix)[inside]
+    if len(zz) > nz or len(yy) > ny or len(xx) > nx:
+        # a wrapped ball wider than the box can hit a cell twice; count unique cells
+        flat = np.unique(flat)
     view = mask.reshape(-1)
     newly = int(np.count_nonzero(view[flat] == 0))
     view[flat] = 1

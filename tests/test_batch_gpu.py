@@ -100,14 +100,15 @@ def test_batch_fp16_close_to_fp32(L, masks):
             np.testing.assert_allclose(c["perm"][0], a["perm"][0], rtol=1e-2)
 
 
-def test_server_continuous_batching_matches_batch(L, masks):
+@pytest.mark.parametrize("target", [0, 30000])
+def test_server_continuous_batching_matches_batch(L, masks, target):
     tol, every = 1e-4, 50
     with L.Batch([(m, NU, G) for m in masks], precision="f32") as b:
         want = b.run(tol=tol, check_every=every, max_steps=20000)
     # a pool that holds the biggest request but not all of them at once
     big = max(int((m == 0).sum()) for m in masks)
     with L.Server(capacity_nodes=big + 2048, max_active=3, precision="f32", tol=tol, check_every=every,
-                  max_steps=20000) as srv:
+                  max_steps=20000, target_active_nodes=target) as srv:
         ids = [srv.submit(m, NU, G) for m in masks]
         got, rounds, saw_queue = {}, 0, False
         while len(got) < len(masks):
