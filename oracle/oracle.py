@@ -154,6 +154,159 @@ class SinglePhaseRun:
         return (self.f.reshape(-1, 19).copy(), self.u.reshape(-1, 3).copy(), self.rho.copy())
 
 
+class CGParams(C.Structure):
+    _fields_ = [("nu_l", C.c_double), ("nu_g", C.c_double), ("psi_solid", C.c_double), ("cap_a", C.c_double),
+                ("g", C.c_double * 3), ("body_force_phase", C.c_int), ("flux_psi", C.c_double),
+                ("flux_umax", C.c_double)]
+
+
+class ColourGradientRun:
+    """The colour-gradient restatement (lbm_oracle_cg.c), one periodic solve."""
+
+    def __init__(self, mask, psi, nu_l, nu_g, psi_solid, cap_a, g, body_force_phase=-1, flux_psi=0.99,
+                 flux_umax=0.01):
+        L = _load("liboracle.so")
+        self.L = L
+        L.orc_cg_matrices.argtypes = [_F64P, _F64P]
+        L.orc_cg_matrices.restype = C.c_int
+        L.orc_cg_nei_loc.argtypes = [_U8P, C.c_int, C.c_int, C.c_int, _I32P, C.c_int, _I32P]
+        L.orc_cg_init.argtypes = [C.c_int, _F64P, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS"),
+                                  _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
+        L.orc_cg_step.argtypes = [C.c_int, _I32P, _F64P, _F64P, C.POINTER(CGParams)] + [_F64P] * 10
+        L.orc_cg_perm.argtypes = [C.c_int, _F64P, _F64P, C.c_int, C.c_int, C.c_int, C.c_double,
+                                  C.POINTER(CGParams), _F64P, _F64P, C.POINTER(C.c_double)]
+        L.orc_cg_perm.restype = C.c_double
+        L.orc_cg_saturation.argtypes = [C.c_int, _F64P, C.c_int, C.c_int, C.c_int, C.c_double]
+        L.orc_cg_saturation.restype = C.c_double
+        R = Restatement()
+        self.mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        self.nz, self.ny, self.nx = mask.shape
+        self.coor = R.compact(self.mask)
+        self.count = n = self.coor.size - 1
+        self.porosity = R.porosity(self.mask)
+        self.nei = np.zeros((n + 1) * 19, dtype=np.int32)
+        L.orc_cg_nei_loc(self.mask, self.nx, self.ny, self.nz, self.coor, n, self.nei)
+        self.M, self.MI = np.zeros(361), np.zeros(361)
+        assert L.orc_cg_matrices(self.M, self.MI) == 1
+        self.p = CGParams(nu_l, nu_g, psi_solid, cap_a, (C.c_double * 3)(*g), body_force_phase, flux_psi, flux_umax)
+        # phase values per node in compaction order (x fastest over pore cells), as float
+        flat = np.ascontiguousarray(psi, dtype=np.float64).reshape(-1)
+        psi_nodes = np.zeros(n + 1, dtype=np.float32)
+        psi_nodes[1:] = flat[self.mask.reshape(-1) == 0].astype(np.float32)
+        z = lambda k: np.zeros(k)
+        self.rho, self.psi, self.rho_r, self.rho_b = z(n + 1), z(n + 1), z(n + 1), z(n + 1)
+        self.rhor, self.rhob = z(n + 1), z(n + 1)
+        self.u, self.u0 = z((n + 1) * 3), z((n + 1) * 3)
+        self.f, self.F = z((n + 1) * 19), z((n + 1) * 19)
+        self.per_l, self.per_g = z(3), z(3)
+        L.orc_cg_init(n, self.MI, psi_nodes, self.rho, self.u, self.f, self.psi, self.rho_r, self.rho_b)
+
+    def step(self, k=1):
+        for _ in range(k):
+            self.L.orc_cg_step(self.count, self.nei, self.M, self.MI, C.byref(self.p), self.rho, self.u, self.u0,
+                               self.f, self.F, self.psi, self.rho_r, self.rho_b, self.rhor, self.rhob)
+
+    def perm(self):
+        ua = C.c_double()
+        e = self.L.orc_cg_perm(self.count, self.u, self.psi, self.nx, self.ny, self.nz, self.porosity,
+                               C.byref(self.p), self.per_l, self.per_g, C.byref(ua))
+        return e, self.per_l.copy(), self.per_g.copy(), ua.value
+
+    def saturation(self):
+        return self.L.orc_cg_saturation(self.count, self.psi, self.nx, self.ny, self.nz, self.porosity)
+
+    def fields(self):
+        return {"f": self.f.reshape(-1, 19).copy(), "u": self.u.reshape(-1, 3).copy(), "rho": self.rho.copy(),
+                "psi": self.psi.copy(), "rho_r": self.rho_r.copy(), "rho_b": self.rho_b.copy()}
+
+
+def write_phase_file(path, psi):
+    """Phase file of the colour-gradient solver: one value per cell, ASCII,
+    x fastest (read with `fin >> pore2` into a float, CG3:2144-2150)."""
+    flat = np.ascontiguousarray(psi, dtype=np.float64).reshape(-1)
+    with open(path, "w") as fh:
+        fh.write("\n".join(repr(float(v)) for v in flat))
+        fh.write("\n")
+
+
+class ReferenceCG3:
+    """The reference colour-gradient solver (compiled from its source), one rank."""
+
+    def __init__(self):
+        name = os.path.join(HERE, "_ref", "libref_cg3.so")
+        if not os.path.exists(name):
+            build()
+        if not os.path.exists(name):
+            raise FileNotFoundError("libref_cg3.so not built (reference sources absent and no prebuilt library)")
+        L = C.CDLL(name)
+        self.L = L
+        L.ref_cg3_create.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                     C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     C.c_int, C.c_double, C.c_double]
+        L.ref_cg3_create.restype = C.c_int
+        L.ref_cg3_step.argtypes = [C.c_int]
+        L.ref_cg3_perm.argtypes = [_F64P, _F64P, C.POINTER(C.c_double)]
+        L.ref_cg3_perm.restype = C.c_double
+        L.ref_cg3_saturation.restype = C.c_double
+        L.ref_cg3_porosity.restype = C.c_double
+        L.ref_cg3_get_coor.argtypes = [_I32P]
+        L.ref_cg3_get_nei_loc.argtypes = [_I32P]
+        L.ref_cg3_get_f.argtypes = [_F64P]
+        L.ref_cg3_get_u.argtypes = [_F64P]
+        L.ref_cg3_get_scalars.argtypes = [_F64P, _F64P, _F64P, _F64P]
+        L.ref_cg3_get_M.argtypes = [_F64P]
+        L.ref_cg3_get_MI.argtypes = [_F64P]
+        self.count = 0
+
+    def create(self, mask, psi, nu_l, nu_g, psi_solid, cap_a, g, body_force_phase=-1, flux_psi=0.99,
+               flux_umax=0.01, workdir=None):
+        nz, ny, nx = mask.shape
+        d = workdir or tempfile.mkdtemp(prefix="refcg3_")
+        mpath = os.path.join(d, "mask.bin")
+        np.ascontiguousarray(np.transpose(mask, (2, 1, 0)).astype(np.int32)).tofile(mpath)
+        ppath = os.path.join(d, "phase.dat")
+        write_phase_file(ppath, psi)
+        self.count = self.L.ref_cg3_create(mpath.encode(), ppath.encode(), nx, ny, nz, 1, nu_l, nu_g, psi_solid,
+                                           cap_a, *[float(x) for x in g], int(body_force_phase), flux_psi, flux_umax)
+        return self.count
+
+    def step(self, n=1):
+        self.L.ref_cg3_step(int(n))
+
+    def perm(self):
+        pl, pg, ua = np.zeros(3), np.zeros(3), C.c_double()
+        e = self.L.ref_cg3_perm(pl, pg, C.byref(ua))
+        return e, pl, pg, ua.value
+
+    def saturation(self):
+        return self.L.ref_cg3_saturation()
+
+    def coor(self):
+        out = np.zeros(self.count + 1, dtype=np.int32)
+        self.L.ref_cg3_get_coor(out)
+        return out
+
+    def nei_loc(self):
+        out = np.zeros((self.count + 1) * 19, dtype=np.int32)
+        self.L.ref_cg3_get_nei_loc(out)
+        return out.reshape(-1, 19)
+
+    def fields(self):
+        n = self.count + 1
+        f, u = np.zeros(n * 19), np.zeros(n * 3)
+        rho, psi, rr, rb = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+        self.L.ref_cg3_get_f(f)
+        self.L.ref_cg3_get_u(u)
+        self.L.ref_cg3_get_scalars(rho, psi, rr, rb)
+        return {"f": f.reshape(-1, 19), "u": u.reshape(-1, 3), "rho": rho, "psi": psi, "rho_r": rr, "rho_b": rb}
+
+    def matrices(self):
+        M, MI = np.zeros(361), np.zeros(361)
+        self.L.ref_cg3_get_M(M)
+        self.L.ref_cg3_get_MI(MI)
+        return M.reshape(19, 19), MI.reshape(19, 19)
+
+
 class ReferenceSP3:
     """The reference solver itself (compiled from its source), one rank.
 

@@ -94,11 +94,40 @@ def cfg1(ref):
                         f_sample=f[1::997].copy(), count=ref.count, porosity=ref.porosity())
 
 
+CG_ARGS = dict(nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0), body_force_phase=-1,
+               flux_psi=0.99, flux_umax=0.01)
+
+
+def cg_small():
+    """Colour-gradient reference (CG3) on 18x16x14 random cylinders with a
+    blob phase field (saturation 0.5), 60 steps."""
+    mask = G.random_cylinders((18, 16, 14), 0.6, 2.0, seed=31)
+    psi = G.blob_phase_field(mask, seed=32, saturation=0.5)
+    ref = oracle.ReferenceCG3()
+    ref.create(mask, psi, **CG_ARGS)
+    coor, nei = ref.coor(), ref.nei_loc()
+    ref.step(60)
+    d = ref.fields()
+    e, pl, pg, ua = ref.perm()
+    sat = ref.saturation()
+    np.savez_compressed(os.path.join(HERE, "cg_small.npz"), mask=pack(mask), shape=np.array(mask.shape), psi0=psi,
+                        steps=60, coor=coor, nei_loc=nei, f=d["f"], u=d["u"], rho=d["rho"], psi=d["psi"],
+                        rho_r=d["rho_r"], rho_b=d["rho_b"], perm_l=pl, perm_g=pg, u_ave=ua, saturation=sat,
+                        args=np.array([CG_ARGS["nu_l"], CG_ARGS["nu_g"], CG_ARGS["psi_solid"], CG_ARGS["cap_a"],
+                                       *CG_ARGS["g"], CG_ARGS["body_force_phase"], CG_ARGS["flux_psi"],
+                                       CG_ARGS["flux_umax"]]))
+    print("cg_small", mask.shape, ref.count)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg1", action="store_true")
+    ap.add_argument("--cg", action="store_true")
     a = ap.parse_args()
     oracle.build()
+    if a.cg:
+        cg_small()
+        return
     ref = oracle.ReferenceSP3()
     if a.cfg1:
         cfg1(ref)
