@@ -225,6 +225,52 @@ LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
  * bytes one fluid-node update moves (2*19*s + 18*4). */
 LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
 
+/* --------------------------------------- colour-gradient two-phase solver */
+
+/* Physics of the colour-gradient model (the INPUT_CG_SPARSE fields of
+ * CG3:386-470 that a fully periodic run uses). */
+typedef struct lbm_cg_params {
+  double nu_l, nu_g;       /* viscosity of component r (psi = 1) and b (psi = -1) */
+  double psi_solid;        /* wall colour = cos(contact angle) (ContactAngle_parameter) */
+  double cap_a;            /* surface-tension parameter CapA */
+  double gx, gy, gz;       /* body force */
+  int body_force_phase;    /* 1: only psi >= flux_psi driven, -1: only psi <= -flux_psi, 0: both */
+  double flux_psi;         /* rel_perm_psi: phase threshold of forcing and fluxes */
+  double flux_umax;        /* rel_perm_psi2: fluxes count nodes with |u| below this */
+  int precision;           /* LBM_PREC_F64 (bit-exact) or LBM_PREC_F32 */
+  int device;
+} lbm_cg_params;
+
+/* Comput_Perm (CG3:5116-5284) and Comput_Saturation (CG3:5286-5370). */
+typedef struct lbm_cg_diag {
+  long long step;
+  double saturation;       /* share of pore nodes with psi >= 0 */
+  double q_l[3], q_g[3];   /* phase fluxes (sum of u per phase) */
+  double perm_l[3], perm_g[3];
+  double perm_rel_change;  /* liquid permeability along x, relative change */
+  double u_ave;            /* |Q_l + Q_g| / (V * porosity) */
+  double capillary;        /* u_ave * nu_l / cap_a */
+  double mass;             /* sum rho */
+} lbm_cg_diag;
+
+typedef struct lbm_cg_handle lbm_cg_handle;
+
+/* mask [nz][ny][nx] (0 = pore), psi [nz][ny][nx] initial phase per cell (the
+ * reference's phase file; read as float, CG3:2144-2150). */
+LBM_API lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const double* psi, int nx, int ny,
+                                 int nz, lbm_cg_handle** out);
+/* collision (CG3:2546-3290) + comput_macro_variables (CG3:3316-3370), n times */
+LBM_API lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps);
+LBM_API lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out);
+/* reference id order, row 0 unused; any pointer may be NULL */
+LBM_API lbm_status lbm_cg_get_fields(lbm_cg_handle* h, double* rho, double* u, double* psi, double* rho_r,
+                                     double* rho_b);
+/* post-streaming f in the CG velocity order, [(count+1)*19] */
+LBM_API lbm_status lbm_cg_get_populations(lbm_cg_handle* h, double* f);
+LBM_API lbm_status lbm_cg_info(lbm_cg_handle* h, int* count, double* porosity, long long* step,
+                               double* last_step_ms);
+LBM_API void lbm_cg_destroy(lbm_cg_handle* h);
+
 /* ------------------------------------------ many independent solves (pool) */
 
 /* One single-phase permeability solve: geometry and physics (fully periodic,

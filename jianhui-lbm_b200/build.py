@@ -34,8 +34,10 @@ CUDA_SOURCES = [
     ("reduce_noalloc.cu", ["-fmad=false"]),
     ("batch_kernels.cu", []),
     ("setup_kernels.cu", []),
+    ("cg_faithful.cu", ["-fmad=false"]),
+    ("cg_fast.cu", []),
 ]
-CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp"]
+CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp"]
 
 
 def _headers():

@@ -1,0 +1,429 @@
+// C ABI of the colour-gradient two-phase solver (lbm_cg_*).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cg_api.h"
+#include "cg_basis.h"
+
+namespace lbm {
+namespace {
+
+struct Dev {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~Dev() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t b) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = b;
+    return b ? cudaMalloc(&p, b) : cudaSuccess;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+constexpr int kCgGraphSteps = 16;
+
+}  // namespace
+}  // namespace lbm
+
+using namespace lbm;
+
+struct lbm_cg_handle {
+  lbm_cg_params prm{};
+  bool f64 = true;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<uint8_t> mask;
+  Geometry geo;
+  double MI[kQ][kQ];
+  CgParams cp{};
+  Dev f[2], gr, gb, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
+  int cur = 0;
+  int given = 1;
+  long long step = 0;
+  double perm_prev = 0.0;
+  double last_ms = 0.0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  ~lbm_cg_handle() {
+    for (auto& g : graph)
+      if (g) cudaGraphExecDestroy(g);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  size_t s() const { return f64 ? 8 : 4; }
+};
+
+namespace {
+
+CgArgs cg_args(lbm_cg_handle* h, int c, int given) {
+  CgArgs a{};
+  a.f_src = h->f[c].p;
+  a.f_dst = h->f[1 - c].p;
+  a.gr = h->gr.p;
+  a.gb = h->gb.p;
+  a.table = h->table.as<int32_t>();
+  a.corder = h->f64 ? h->corder.as<uint8_t>() : nullptr;
+  a.n = h->geo.count;
+  a.npad = h->geo.npad;
+  a.psi = h->psi.p;
+  a.rho_r = h->rho_r.p;
+  a.rho_b = h->rho_b.p;
+  a.given = given;
+  a.p = h->cp;
+  return a;
+}
+
+cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given) {
+  const CgArgs a = cg_args(h, c, given);
+  cudaError_t e = cudaSuccess;
+  if (!given) e = h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream);
+  if (e != cudaSuccess) return e;
+  return h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
+}
+
+lbm_status cg_graph(lbm_cg_handle* h, int c0) {
+  if (h->graph[c0]) return LBM_OK;
+  cudaGraph_t g = nullptr;
+  LBM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  int c = c0;
+  for (int s = 0; s < kCgGraphSteps && err == cudaSuccess; s++) {
+    err = one_cg_step(h, c, 0);
+    c = 1 - c;
+  }
+  const cudaError_t end = cudaStreamEndCapture(h->stream, &g);
+  if (err != cudaSuccess || end != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(LBM_ERR_CUDA, std::string("cg graph capture: ") + cudaGetErrorString(err ? err : end));
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&h->graph[c0], g, 0);
+  cudaGraphDestroy(g);
+  LBM_CUDA_TRY(ie);
+  return LBM_OK;
+}
+
+// Colour summation order of the reference's scatter (CG3:3507-3570): the
+// contributions to rho_r(x) arrive in ascending source-node id, and for one
+// source in ascending push direction (CG order).
+void build_colour_order(const Geometry& g, std::vector<uint8_t>& order) {
+  const int n = g.count, npad = g.npad;
+  order.assign((size_t)kQ * npad, 0);
+  for (int x = 0; x < n; x++) {
+    long long key[kQ];
+    int qs[kQ];
+    for (int q = 0; q < kQ; q++) {
+      int src_node, mi;
+      if (q == 0) {
+        src_node = x;
+        mi = 0;
+      } else {
+        const int32_t s = g.src[(size_t)(q - 1) * npad + x];
+        const int sq = s / npad, m = s % npad;
+        if (sq == q) {
+          src_node = m;
+          mi = cg::of_row(q);
+        } else {
+          src_node = x;
+          mi = cg::of_row(opp(q));
+        }
+      }
+      key[q] = (long long)g.ref_of[src_node] * kQ + mi;
+      qs[q] = q;
+    }
+    std::sort(qs, qs + kQ, [&](int a, int b) { return key[a] < key[b]; });
+    for (int k = 0; k < kQ; k++) order[(size_t)k * npad + x] = (uint8_t)qs[k];
+  }
+}
+
+lbm_status cg_check(lbm_cg_handle* h) {
+  if (!h) return fail(LBM_ERR_ARG, "null cg handle");
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  return LBM_OK;
+}
+
+// Runs the colour pass (when the state is not the initial one) and the
+// diagnostics reduction; optional macro fields in internal order.
+lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double* u_out) {
+  if (!h->given) {
+    const CgArgs a = cg_args(h, h->cur, 0);
+    LBM_CUDA_TRY(h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream));
+  }
+  CgReduceArgs ra{};
+  ra.f = h->f[h->cur].p;
+  ra.table = h->table.as<int32_t>();
+  ra.psi = h->psi.p;
+  ra.n = h->geo.count;
+  ra.npad = h->geo.npad;
+  ra.given = h->given;
+  ra.g[0] = h->prm.gx;
+  ra.g[1] = h->prm.gy;
+  ra.g[2] = h->prm.gz;
+  ra.flux_psi = h->prm.flux_psi;
+  ra.flux_umax = h->prm.flux_umax;
+  ra.rho_out = rho_out;
+  ra.u_out = u_out;
+  ra.partials = h->partials.as<double>();
+  ra.result = h->result.as<double>();
+  const int nb = reduce_blocks(h->geo.count);
+  LBM_CUDA_TRY(h->f64 ? cg_reduce_f64(ra, nb, h->stream) : cg_reduce_f32(ra, nb, h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(r, ra.result, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const double* psi_cells, int nx, int ny,
+                         int nz, lbm_cg_handle** out) {
+  if (!p || !mask || !psi_cells || !out || nx <= 0 || ny <= 0 || nz <= 0)
+    return fail(LBM_ERR_ARG, "lbm_cg_create: bad argument");
+  *out = nullptr;
+  if (!(p->nu_l > 0) || !(p->nu_g > 0)) return fail(LBM_ERR_ARG, "lbm_cg_create: viscosities must be positive");
+  if (p->precision != LBM_PREC_F64 && p->precision != LBM_PREC_F32)
+    return fail(LBM_ERR_ARG, "lbm_cg_create: precision must be F64 or F32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device");
+  auto h = std::make_unique<lbm_cg_handle>();
+  h->prm = *p;
+  h->f64 = p->precision == LBM_PREC_F64;
+  h->device = p->device;
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  LBM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  LBM_CUDA_TRY(cudaEventCreate(&h->ev0));
+  LBM_CUDA_TRY(cudaEventCreate(&h->ev1));
+  const size_t cells = (size_t)nx * ny * nz;
+  h->mask.assign(mask, mask + cells);
+  Geometry& g = h->geo;
+  compact_reference(mask, nx, ny, nz, &g);
+  if (g.count == 0) return fail(LBM_ERR_ARG, "geometry has no pore cells");
+  order_nodes(mask, LBM_ORDER_REFERENCE, &g);
+  build_pull_table(mask, &g);
+  if (!build_cg_inverse(h->MI)) return fail(LBM_ERR_ARG, "colour-gradient basis inversion failed");
+
+  // constants of init (CG3:2226-2260)
+  CgParams& cp = h->cp;
+  cp.psi_solid = p->psi_solid;
+  cp.cap_a = p->cap_a;
+  cp.g[0] = p->gx;
+  cp.g[1] = p->gy;
+  cp.g[2] = p->gz;
+  cp.body_force_phase = p->body_force_phase;
+  cp.flux_psi = p->flux_psi;
+  const double c_s2 = 1.0 * 1.0 / 3, dt = 1.0;
+  cp.delta = 0.1;
+  cp.wl = 1.0 / (p->nu_l / (c_s2 * dt) + 0.5);
+  cp.wg = 1.0 / (p->nu_g / (c_s2 * dt) + 0.5);
+  cp.lg0 = 2 * cp.wl * cp.wg / (cp.wl + cp.wg);
+  cp.l1 = 2 * (cp.wl - cp.lg0) / cp.delta;
+  cp.l2 = -cp.l1 / (2 * cp.delta);
+  cp.g1 = 2 * (cp.lg0 - cp.wg) / cp.delta;
+  cp.g2 = cp.g1 / (2 * cp.delta);
+
+  const int n = g.count, npad = g.npad;
+  const size_t s = h->s();
+  for (auto& b : h->f) LBM_CUDA_TRY(b.alloc((size_t)kQ * npad * s));
+  LBM_CUDA_TRY(h->gr.alloc((size_t)kQ * npad * s));
+  LBM_CUDA_TRY(h->gb.alloc((size_t)kQ * npad * s));
+  LBM_CUDA_TRY(h->table.alloc((size_t)18 * npad * sizeof(int32_t)));
+  LBM_CUDA_TRY(h->psi.alloc((size_t)npad * s));
+  LBM_CUDA_TRY(h->rho_r.alloc((size_t)npad * s));
+  LBM_CUDA_TRY(h->rho_b.alloc((size_t)npad * s));
+  LBM_CUDA_TRY(h->ref_of.alloc((size_t)n * sizeof(int32_t)));
+  LBM_CUDA_TRY(h->partials.alloc((size_t)reduce_blocks(n) * 8 * sizeof(double)));
+  LBM_CUDA_TRY(h->result.alloc(8 * sizeof(double)));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->table.p, g.src.data(), sizeof(int32_t) * 18 * (size_t)npad,
+                               cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->ref_of.p, g.ref_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                               h->stream));
+  std::vector<uint8_t> order;
+  if (h->f64) {
+    build_colour_order(g, order);
+    LBM_CUDA_TRY(h->corder.alloc(order.size()));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->corder.p, order.data(), order.size(), cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cg_set_mi_f64(&h->MI[0][0], h->stream));
+  } else {
+    LBM_CUDA_TRY(cg_set_mi_f32(&h->MI[0][0], h->stream));
+  }
+  // init (CG3:2360-2380): f = feq(1, 0) = first column of M^-1 in CG order,
+  // psi from the phase file as float, rho_r = (psi + 1)/2, rho_b = 1 - rho_r
+  double f0[kQ];
+  for (int q = 0; q < kQ; q++) f0[q] = h->MI[cg::of_row(q)][0];
+  LBM_CUDA_TRY(launch_init_uniform(h->f64 ? Store::F64 : Store::F32, h->f[0].p, h->table.as<int32_t>(), n, npad, 1.0,
+                                   f0, h->stream));
+  std::vector<double> ps(npad, 0.0), rr(npad, 0.0), rb(npad, 0.0);
+  for (int x = 0; x < n; x++) {
+    const int c = g.coor[g.ref_of[x]];  // i*ny*nz + j*nz + k
+    const int i = c / (ny * nz), j = (c % (ny * nz)) / nz, k = c % nz;
+    const double v = (double)(float)psi_cells[i + (size_t)nx * (j + (size_t)ny * k)];
+    const double rho = 1.0;
+    ps[x] = v;
+    rr[x] = (v * rho + rho) / 2;
+    rb[x] = rho - rr[x];
+  }
+  if (h->f64) {
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->psi.p, ps.data(), sizeof(double) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->rho_r.p, rr.data(), sizeof(double) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->rho_b.p, rb.data(), sizeof(double) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<float> a(ps.begin(), ps.end()), b(rr.begin(), rr.end()), c(rb.begin(), rb.end());
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->psi.p, a.data(), sizeof(float) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->rho_r.p, b.data(), sizeof(float) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->rho_b.p, c.data(), sizeof(float) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  LBM_CUDA_TRY(cudaMemsetAsync(h->gr.p, 0, h->gr.bytes, h->stream));
+  LBM_CUDA_TRY(cudaMemsetAsync(h->gb.p, 0, h->gb.bytes, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = h.release();
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (nsteps < 0) return fail(LBM_ERR_ARG, "lbm_cg_step: negative step count");
+  if (nsteps == 0) return LBM_OK;
+  int left = nsteps;
+  if (left - (h->given ? 1 : 0) >= kCgGraphSteps) {
+    const int c0 = h->cur;
+    for (int c = 0; c < 2; c++)
+      if ((st = cg_graph(h, c)) != LBM_OK) return st;
+    h->cur = c0;
+  }
+  LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  if (h->given) {
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, 1));
+    h->cur = 1 - h->cur;
+    h->given = 0;
+    left--;
+  }
+  while (left >= kCgGraphSteps) {
+    LBM_CUDA_TRY(cudaGraphLaunch(h->graph[h->cur], h->stream));
+    left -= kCgGraphSteps;  // even chain: parity unchanged
+  }
+  while (left > 0) {
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, 0));
+    h->cur = 1 - h->cur;
+    left--;
+  }
+  LBM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+  LBM_CUDA_TRY(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  LBM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  h->step += nsteps;
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!out) return fail(LBM_ERR_ARG, "lbm_cg_reduce: null output");
+  double r[8];
+  if ((st = cg_reduce_raw(h, r, nullptr, nullptr)) != LBM_OK) return st;
+  const Geometry& g = h->geo;
+  const double V = (double)g.nx * g.ny * g.nz, phi = g.porosity, dp = 0.0;
+  const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
+  std::memset(out, 0, sizeof(*out));
+  out->step = h->step;
+  for (int d = 0; d < 3; d++) {
+    out->q_l[d] = r[d];
+    out->q_g[d] = r[4 + d];
+    out->perm_l[d] = r[d] / V * h->prm.nu_l / (gg[d] + dp);      // CG3:5217-5222
+    out->perm_g[d] = r[4 + d] / V * h->prm.nu_g / (gg[d] + dp);
+  }
+  const double vx = (r[0] + r[4]) / V, vy = (r[1] + r[5]) / V, vz = (r[2] + r[6]) / V;
+  out->u_ave = std::sqrt((vx / phi) * (vx / phi) + (vy / phi) * (vy / phi) + (vz / phi) * (vz / phi));
+  out->capillary = std::sqrt(vx * vx + vy * vy + vz * vz) / phi * h->prm.nu_l / h->prm.cap_a;
+  out->saturation = r[3] / (V * phi);  // CG3:5361
+  out->mass = r[7];
+  out->perm_rel_change = (out->perm_l[0] - h->perm_prev) / h->perm_prev;
+  h->perm_prev = out->perm_l[0];
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_get_fields(lbm_cg_handle* h, double* rho, double* u, double* psi, double* rho_r, double* rho_b) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  const int n = h->geo.count, npad = h->geo.npad;
+  Dev rint, uint_, rref, uref;
+  LBM_CUDA_TRY(rint.alloc((size_t)npad * sizeof(double)));
+  LBM_CUDA_TRY(uint_.alloc((size_t)3 * npad * sizeof(double)));
+  LBM_CUDA_TRY(rref.alloc((size_t)(n + 1) * sizeof(double)));
+  LBM_CUDA_TRY(uref.alloc((size_t)(n + 1) * 3 * sizeof(double)));
+  double r[8];
+  if ((st = cg_reduce_raw(h, r, rint.as<double>(), uint_.as<double>())) != LBM_OK) return st;
+  LBM_CUDA_TRY(cudaMemsetAsync(rref.p, 0, rref.bytes, h->stream));
+  LBM_CUDA_TRY(cudaMemsetAsync(uref.p, 0, uref.bytes, h->stream));
+  LBM_CUDA_TRY(launch_export_macro(rint.as<double>(), uint_.as<double>(), h->ref_of.as<int32_t>(), n, npad,
+                                   rref.as<double>(), uref.as<double>(), h->stream));
+  if (rho) LBM_CUDA_TRY(cudaMemcpyAsync(rho, rref.p, rref.bytes, cudaMemcpyDeviceToHost, h->stream));
+  if (u) LBM_CUDA_TRY(cudaMemcpyAsync(u, uref.p, uref.bytes, cudaMemcpyDeviceToHost, h->stream));
+  // scalar fields: internal order equals reference order - 1 for this solver
+  std::vector<double> tmp(npad);
+  std::vector<float> tmpf(npad);
+  double* outs[3] = {psi, rho_r, rho_b};
+  Dev* srcs[3] = {&h->psi, &h->rho_r, &h->rho_b};
+  for (int i = 0; i < 3; i++) {
+    if (!outs[i]) continue;
+    if (h->f64) {
+      LBM_CUDA_TRY(cudaMemcpyAsync(tmp.data(), srcs[i]->p, sizeof(double) * npad, cudaMemcpyDeviceToHost, h->stream));
+      LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    } else {
+      LBM_CUDA_TRY(cudaMemcpyAsync(tmpf.data(), srcs[i]->p, sizeof(float) * npad, cudaMemcpyDeviceToHost, h->stream));
+      LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+      for (int x = 0; x < npad; x++) tmp[x] = tmpf[x];
+    }
+    outs[i][0] = 0.0;
+    for (int x = 0; x < n; x++) outs[i][h->geo.ref_of[x]] = tmp[x];
+  }
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_get_populations(lbm_cg_handle* h, double* f) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!f) return fail(LBM_ERR_ARG, "lbm_cg_get_populations: null output");
+  const int n = h->geo.count;
+  Dev o;
+  LBM_CUDA_TRY(o.alloc((size_t)(n + 1) * kQ * sizeof(double)));
+  LBM_CUDA_TRY(cudaMemsetAsync(o.p, 0, o.bytes, h->stream));
+  LBM_CUDA_TRY(cg_export_f(h->f64, h->f[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n, h->geo.npad,
+                           o.as<double>(), h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(f, o.p, o.bytes, cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_info(lbm_cg_handle* h, int* count, double* porosity, long long* step, double* last_step_ms) {
+  if (!h) return fail(LBM_ERR_ARG, "null cg handle");
+  if (count) *count = h->geo.count;
+  if (porosity) *porosity = h->geo.porosity;
+  if (step) *step = h->step;
+  if (last_step_ms) *last_step_ms = h->last_ms;
+  return LBM_OK;
+}
+
+void lbm_cg_destroy(lbm_cg_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// Host-visible structures and launchers of the colour-gradient kernels.
+#pragma once
+
+#include "lbm_internal.h"
+
+namespace lbm {
+
+struct CgParams {
+  double psi_solid, cap_a;
+  double g[3];
+  int body_force_phase;
+  double flux_psi;
+  // viscosity interpolation (CG3 init, delta = 0.1)
+  double wl, wg, lg0, l1, l2, g1, g2, delta;
+};
+
+struct CgArgs {
+  const void* f_src;  // [19][npad] post-collision f of the previous step
+  void* f_dst;
+  void* gr;           // [19][npad] recoloured red distributions (at their source node)
+  void* gb;
+  const int32_t* table;
+  const uint8_t* corder;  // [19][npad] colour summation order (FP64), or null
+  int n, npad;
+  void* psi;          // [npad] current phase field
+  void* rho_r;
+  void* rho_b;
+  int given;          // first step after init: rho = 1, u = 0
+  CgParams p;
+};
+
+struct CgReduceArgs {
+  const void* f;  // current post-collision f
+  const int32_t* table;
+  const void* psi;
+  int n, npad;
+  int given;
+  double g[3];
+  double flux_psi, flux_umax;
+  double* rho_out;  // optional [npad] internal order
+  double* u_out;    // optional [3][npad]
+  double* partials;
+  double* result;   // Ql(3), count(psi >= 0), Qg(3), mass
+};
+
+cudaError_t cg_set_mi_f64(const double* mi, cudaStream_t st);
+cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st);
+cudaError_t cg_colour_f64(const CgArgs& a, cudaStream_t st);
+cudaError_t cg_colour_f32(const CgArgs& a, cudaStream_t st);
+cudaError_t cg_collide_f64(const CgArgs& a, cudaStream_t st);
+cudaError_t cg_collide_f32(const CgArgs& a, cudaStream_t st);
+cudaError_t cg_reduce_f64(const CgReduceArgs& a, int nblocks, cudaStream_t st);
+cudaError_t cg_reduce_f32(const CgReduceArgs& a, int nblocks, cudaStream_t st);
+bool build_cg_inverse(double MI[kQ][kQ]);
+// f in the CG direction order, reference layout [(count+1)*19]
+cudaError_t cg_export_f(bool f64, const void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,
+                        double* out, cudaStream_t st);
+
+}  // namespace lbm

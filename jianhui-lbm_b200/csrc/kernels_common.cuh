@@ -257,16 +257,17 @@ __device__ __forceinline__ void mrt_collide_dev(A (&f)[kQ], const PairSplit<A>& 
 }
 
 // ----------------------------------------------------------------------------
-// Block-level reduction of the 8 diagnostic accumulators
-// (t1, t2, t3, umax^2, Qx, Qy, Qz, mass): slot 3 is a max, the rest sums.
-// Deterministic for a fixed launch shape.
+// Block-level reduction of 8 accumulators: slot MAXSLOT (if any) is a max,
+// the others sums; for the single-phase diagnostics the slots are
+// (t1, t2, t3, umax^2, Qx, Qy, Qz, mass).  Deterministic for a fixed launch shape.
+template <int MAXSLOT = 3>
 __device__ __forceinline__ void block_reduce8(double (&v)[8], double* out, double* smem /*[8*32]*/) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1)
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const double o = __shfl_down_sync(0xffffffffu, v[i], off);
-      v[i] = (i == 3) ? fmax(v[i], o) : v[i] + o;
+      v[i] = (i == MAXSLOT) ? fmax(v[i], o) : v[i] + o;
     }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0)
@@ -282,7 +283,7 @@ __device__ __forceinline__ void block_reduce8(double (&v)[8], double* out, doubl
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const double o = __shfl_down_sync(0xffffffffu, v[i], off);
-        v[i] = (i == 3) ? fmax(v[i], o) : v[i] + o;
+        v[i] = (i == MAXSLOT) ? fmax(v[i], o) : v[i] + o;
       }
     if (lane == 0)
 #pragma unroll

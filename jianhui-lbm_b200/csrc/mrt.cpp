@@ -2,6 +2,7 @@
 #include <cmath>
 #include <utility>
 
+#include "cg_basis.h"
 #include "lbm_internal.h"
 
 namespace lbm {
@@ -54,6 +55,18 @@ bool gauss_jordan_full_pivot(double (&a)[N][N]) {
 }
 
 }  // namespace
+
+// Inverse of the colour-gradient basis; the reference hard-codes this
+// algorithm's output in its collision too (CG3:3081-3117).
+bool build_cg_inverse(double MI[kQ][kQ]) {
+  double a[kQ][kQ];
+  for (int k = 0; k < kQ; k++)
+    for (int q = 0; q < kQ; q++) a[k][q] = cg::mcoef(k, q);
+  if (!gauss_jordan_full_pivot<kQ>(a)) return false;
+  for (int k = 0; k < kQ; k++)
+    for (int q = 0; q < kQ; q++) MI[k][q] = a[k][q];
+  return true;
+}
 
 // Rates of `init` (SP3:1289-1322): lattice units (dx = dt = 1, c_s^2 = 1/3).
 bool build_mrt_constants(double nu, MrtConstants* out) {

@@ -126,6 +126,25 @@ class ServerResult(C.Structure):
                 ("t_admit", C.c_double), ("t_done", C.c_double)]
 
 
+class CGParams(C.Structure):
+    _fields_ = [("nu_l", C.c_double), ("nu_g", C.c_double), ("psi_solid", C.c_double), ("cap_a", C.c_double),
+                ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double), ("body_force_phase", C.c_int),
+                ("flux_psi", C.c_double), ("flux_umax", C.c_double), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class CGDiag(C.Structure):
+    _fields_ = [("step", C.c_longlong), ("saturation", C.c_double), ("q_l", C.c_double * 3),
+                ("q_g", C.c_double * 3), ("perm_l", C.c_double * 3), ("perm_g", C.c_double * 3),
+                ("perm_rel_change", C.c_double), ("u_ave", C.c_double), ("capillary", C.c_double),
+                ("mass", C.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        for k in ("q_l", "q_g", "perm_l", "perm_g"):
+            d[k] = list(d[k])
+        return d
+
+
 _lib = None
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -172,7 +191,80 @@ _SIGNATURES = {
     "lbm_server_poll": ([C.c_void_p, C.POINTER(ServerResult), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "lbm_server_now": ([C.c_void_p], C.c_double),
     "lbm_server_destroy": ([C.c_void_p], None),
+    "lbm_cg_create": ([C.POINTER(CGParams), _U8P, _F64P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_cg_step": ([C.c_void_p, C.c_int], C.c_int),
+    "lbm_cg_reduce": ([C.c_void_p, C.POINTER(CGDiag)], C.c_int),
+    "lbm_cg_get_fields": ([C.c_void_p] + [C.c_void_p] * 5, C.c_int),
+    "lbm_cg_get_populations": ([C.c_void_p, _F64P], C.c_int),
+    "lbm_cg_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                     C.POINTER(C.c_double)], C.c_int),
+    "lbm_cg_destroy": ([C.c_void_p], None),
 }
+
+
+class ColourGradient:
+    """Colour-gradient two-phase solve (periodic) on one GPU.
+
+    ``psi`` holds the initial phase per cell, (nz, ny, nx), +1 = component r."""
+
+    def __init__(self, mask, psi, nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0),
+                 body_force_phase=-1, flux_psi=0.99, flux_umax=0.01, precision="f32", device=0):
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        nz, ny, nx = m.shape
+        p = CGParams(float(nu_l), float(nu_g), float(psi_solid), float(cap_a), float(g[0]), float(g[1]), float(g[2]),
+                     int(body_force_phase), float(flux_psi), float(flux_umax),
+                     PRECISIONS[precision] if isinstance(precision, str) else int(precision), int(device))
+        h = C.c_void_p()
+        _check(lib().lbm_cg_create(C.byref(p), m.reshape(-1), np.ascontiguousarray(psi, dtype=np.float64).reshape(-1),
+                                   nx, ny, nz, C.byref(h)))
+        self._h = h
+        c, ph, st, ms = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
+        _check(lib().lbm_cg_info(h, C.byref(c), C.byref(ph), C.byref(st), C.byref(ms)))
+        self.count, self.porosity = c.value, ph.value
+
+    def step(self, n=1):
+        _check(lib().lbm_cg_step(self._h, int(n)))
+
+    def reduce(self):
+        d = CGDiag()
+        _check(lib().lbm_cg_reduce(self._h, C.byref(d)))
+        return d.as_dict()
+
+    def fields(self):
+        n = self.count + 1
+        out = {"rho": np.zeros(n), "u": np.zeros(n * 3), "psi": np.zeros(n), "rho_r": np.zeros(n),
+               "rho_b": np.zeros(n)}
+        _check(lib().lbm_cg_get_fields(self._h, out["rho"].ctypes.data, out["u"].ctypes.data, out["psi"].ctypes.data,
+                                       out["rho_r"].ctypes.data, out["rho_b"].ctypes.data))
+        out["u"] = out["u"].reshape(-1, 3)
+        return out
+
+    def populations(self):
+        f = np.zeros((self.count + 1) * 19)
+        _check(lib().lbm_cg_get_populations(self._h, f))
+        return f.reshape(-1, 19)
+
+    def last_step_ms(self):
+        c, ph, st, ms = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
+        _check(lib().lbm_cg_info(self._h, C.byref(c), C.byref(ph), C.byref(st), C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_cg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def _instance(mask, nu, g):

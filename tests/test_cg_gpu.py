@@ -1,0 +1,90 @@
+"""Colour-gradient two-phase kernels on the GPU against the oracle.
+
+Tolerances against the FP64 oracle (the reference colour-gradient solver):
+  FP64 (LBM_PREC_F64)  bit-exact: f, u, rho, psi, rho_r, rho_b; reductions 1e-12
+  FP32                 |d psi| mean <= 1e-3, saturation within 2e-3,
+                       liquid permeability within 2e-2 relative (short runs;
+                       the interface dynamics amplify round-off over long ones)
+"""
+import numpy as np
+import pytest
+
+from helpers import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def L():
+    import __graft_entry__
+
+    __graft_entry__.build_library()
+    import lbm_b200
+
+    return lbm_b200
+
+
+def kw_of(gd):
+    a = gd["args"]
+    return dict(nu_l=a[0], nu_g=a[1], psi_solid=a[2], cap_a=a[3], g=(a[4], a[5], a[6]),
+                body_force_phase=int(a[7]), flux_psi=a[8], flux_umax=a[9])
+
+
+def test_cg_fp64_bit_exact_vs_reference_fixture(L):
+    gd = load_golden("cg_small.npz")
+    with L.ColourGradient(gd["mask"], gd["psi0"], precision="f64", **kw_of(gd)) as s:
+        d0 = s.fields()
+        assert d0["psi"][1:].min() >= -1 and d0["psi"][1:].max() <= 1
+        s.step(int(gd["steps"]) - 16)
+        s.step(16)
+        f = s.populations()
+        d = s.fields()
+        assert np.array_equal(f, gd["f"])
+        for k in ("u", "rho", "psi", "rho_r", "rho_b"):
+            assert np.array_equal(d[k], gd[k]), k
+        r = s.reduce()
+        np.testing.assert_allclose(r["perm_l"][0], gd["perm_l"][0], rtol=1e-12)
+        np.testing.assert_allclose(r["perm_g"][0], gd["perm_g"][0], rtol=1e-12)
+        np.testing.assert_allclose(r["u_ave"], gd["u_ave"], rtol=1e-12)
+        assert r["saturation"] == gd["saturation"]
+
+
+def test_cg_fp32_close_to_fp64_oracle(L, oracle_mod):
+    from lbm_b200 import geometry as G
+
+    mask = G.random_cylinders((28, 24, 20), 0.6, 2.5, seed=41)
+    psi = G.blob_phase_field(mask, seed=42, saturation=0.5)
+    kw = dict(nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0), body_force_phase=-1,
+              flux_psi=0.99, flux_umax=0.01)
+    ref = oracle_mod.ColourGradientRun(mask, psi, **kw)
+    ref.step(300)
+    rd = ref.fields()
+    _, pl, pg, ua = ref.perm()
+    sat = ref.saturation()
+    with L.ColourGradient(mask, psi, precision="f32", **kw) as s:
+        s.step(300)
+        d = s.fields()
+        r = s.reduce()
+    assert np.abs(d["psi"][1:] - rd["psi"][1:]).mean() <= 1e-3
+    assert abs(r["saturation"] - sat) <= 2e-3
+    assert abs(r["perm_l"][0] - pl[0]) <= 2e-2 * abs(pl[0])
+    assert abs(r["mass"] - rd["rho"][1:].sum()) <= 1e-5 * s.count
+
+
+def test_cg_fp64_matches_oracle_over_longer_run(L, oracle_mod):
+    from lbm_b200 import geometry as G
+
+    mask = G.random_cylinders((20, 18, 16), 0.55, 2.0, seed=51)
+    psi = G.blob_phase_field(mask, seed=52, saturation=0.6)
+    kw = dict(nu_l=0.15, nu_g=0.05, psi_solid=-0.5, cap_a=4e-3, g=(0.0, 2e-5, 1e-5), body_force_phase=1,
+              flux_psi=0.9, flux_umax=0.05)
+    ref = oracle_mod.ColourGradientRun(mask, psi, **kw)
+    ref.step(250)
+    rd = ref.fields()
+    with L.ColourGradient(mask, psi, precision="f64", **kw) as s:
+        s.step(250)
+        d = s.fields()
+        f = s.populations()
+    assert np.array_equal(f, rd["f"])
+    for k in ("u", "psi", "rho_r", "rho_b"):
+        assert np.array_equal(d[k], rd[k]), k
