@@ -442,9 +442,48 @@ def run_serve(a):
     return 0
 
 
+def run_cg(a):
+    """Colour-gradient two-phase run (config 3) in FP32, compared with the FP64
+    kernel (bit-identical to the reference colour-gradient solver) on the
+    same input: saturation and phase fluxes."""
+    world, rank, local, pg = dist_setup()
+    import lbm_b200
+    from lbm_b200 import workloads as W
+
+    mask, psi = W.config3()
+    kw = dict(nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0), body_force_phase=-1,
+              flux_psi=0.99, flux_umax=0.01)
+    steps = a.cg_steps
+    out = {}
+    for prec in ("f32", "f64"):
+        with lbm_b200.ColourGradient(mask, psi, precision=prec, device=local, **kw) as s:
+            s.step(20)
+            s.step(steps - 20)
+            ms = s.last_step_ms()
+            out[prec] = (s.reduce(), ms / (steps - 20), s.count)
+    if rank != 0:
+        return 0
+    (d32, ms32, n), (d64, ms64, _) = out["f32"], out["f64"]
+    line = {"metric": "colour-gradient fluid MLUPS (FP32)", "value": n / (ms32 * 1e-3) / 1e6, "unit": "MLUPS",
+            "n_gpus": world, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "128^3 random cylinders r=3, porosity 0.6, blob phase field S_w=0.5, nu ratio 1, "
+                                   "CapA=1e-3, psi_solid=cos45, gx=1e-5 on the non-wetting phase", "steps": steps,
+                       "fluid_nodes": n},
+            "fp64_mlups": n / (ms64 * 1e-3) / 1e6,
+            "saturation": {"f32": d32["saturation"], "f64": d64["saturation"]},
+            "q_l_x": {"f32": d32["q_l"][0], "f64": d64["q_l"][0]},
+            "q_g_x": {"f32": d32["q_g"][0], "f64": d64["q_g"][0]},
+            "rel_err_vs_fp64": {"saturation": abs(d32["saturation"] - d64["saturation"]) / d64["saturation"],
+                                "q_l": abs(d32["q_l"][0] - d64["q_l"][0]) / (abs(d64["q_l"][0]) + 1e-300),
+                                "q_g": abs(d32["q_g"][0] - d64["q_g"][0]) / (abs(d64["q_g"][0]) + 1e-300)}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve"],
+    ap.add_argument("--cg-steps", type=int, default=20000)
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve", "cg"],
                     help="cfg2 = the headline single-domain bench; batch / serve = configs 4 / 5")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=8.0)
@@ -470,6 +509,8 @@ def main():
         return run_batch(a)
     if a.workload == "serve":
         return run_serve(a)
+    if a.workload == "cg":
+        return run_cg(a)
     return run_ours(a)
 
 

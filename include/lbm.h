@@ -271,6 +271,41 @@ LBM_API lbm_status lbm_cg_info(lbm_cg_handle* h, int* count, double* porosity, l
                                double* last_step_ms);
 LBM_API void lbm_cg_destroy(lbm_cg_handle* h);
 
+/* --------------------------------------------- D3Q7 solute (passive scalar) */
+
+typedef struct lbm_st7_params {
+  double diffusivity;  /* niu_s: tau_s = 3 niu_s + 1/2 (ST7:1262) */
+  int precision;       /* LBM_PREC_F64 (reference arithmetic) or LBM_PREC_F32 */
+  int device;
+} lbm_st7_params;
+
+typedef struct lbm_st7_handle lbm_st7_handle;
+
+/* u_nodes: advecting velocity per fluid node, [(count+1)*3] in the library's
+ * reference id order (SP3 compaction, the order lbm_get_fields returns);
+ * c0: initial concentration per cell [nz][ny][nx] (the reference's initial
+ * concentration file, ST7:1269). */
+LBM_API lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz,
+                                  const double* u_nodes, const double* c0, lbm_st7_handle** out);
+/* Same, taking the velocity of a single-phase solve's current state (the
+ * flow -> solute coupling of SP:5093-5120 / ST7:3640-3667 without files). */
+LBM_API lbm_status lbm_st7_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
+                                            lbm_st7_handle** out);
+/* collision + streaming + C = sum g (ST7:1345-1633), n times */
+LBM_API lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps);
+/* C per fluid node [(count+1)], reference id order, row 0 zero */
+LBM_API lbm_status lbm_st7_get_concentration(lbm_st7_handle* h, double* c);
+LBM_API lbm_status lbm_st7_info(lbm_st7_handle* h, int* count, long long* step, double* last_step_ms);
+LBM_API void lbm_st7_destroy(lbm_st7_handle* h);
+
+/* Velocity_for_solute_<n>.<rank>.bin (SP:5093-5120): Count*3 raw doubles in
+ * the slab solver's compaction order at one rank (i outer, j, k inner).
+ * Write from a single-phase solve's current velocity; read into the
+ * library's id order ([(count+1)*3], row 0 zero). */
+LBM_API lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path);
+LBM_API lbm_status lbm_read_velocity_for_solute(const char* path, const uint8_t* mask, int nx, int ny, int nz,
+                                                double* u_nodes);
+
 /* ------------------------------------------ many independent solves (pool) */
 
 /* One single-phase permeability solve: geometry and physics (fully periodic,

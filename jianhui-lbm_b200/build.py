@@ -36,8 +36,9 @@ CUDA_SOURCES = [
     ("setup_kernels.cu", []),
     ("cg_faithful.cu", ["-fmad=false"]),
     ("cg_fast.cu", []),
+    ("st7_kernels.cu", ["-fmad=false"]),
 ]
-CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp"]
+CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp"]
 
 
 def _headers():

@@ -106,6 +106,15 @@ struct lbm_handle {
   }
 };
 
+namespace lbm {
+const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz) {
+  *nx = h->geo.nx;
+  *ny = h->geo.ny;
+  *nz = h->geo.nz;
+  return h->mask.data();
+}
+}  // namespace lbm
+
 namespace {
 
 lbm_status upload_layout(lbm_handle* h) {

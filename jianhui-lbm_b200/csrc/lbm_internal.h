@@ -113,6 +113,9 @@ void build_pull_table(const uint8_t* mask, Geometry* g);
 void pull_to_push(const Geometry& g, int32_t* nei_loc);
 void set_window(const int window[6], Geometry* g);
 
+// Mask and box of a single-phase handle (for solvers coupled to it).
+const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz);
+
 // ---------------------------------------------------------------- errors
 void set_error(const std::string& msg);
 lbm_status fail(lbm_status s, const std::string& msg);

@@ -1,0 +1,262 @@
+// C ABI of the D3Q7 solute solver (lbm_st7_*) and the flow -> solute
+// velocity file of the reference.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "st7_api.h"
+
+namespace lbm {
+namespace {
+
+struct Mem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~Mem() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t b) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = b;
+    return b ? cudaMalloc(&p, b) : cudaSuccess;
+  }
+};
+
+// Slab-solver ids at one rank run over pore cells with i outer, k fastest
+// (SP:1168-1180), i.e. ascending coor = i*ny*nz + j*nz + k.  Returns, for each
+// slab id s (0-based), the library's reference id (1-based).
+std::vector<int32_t> slab_to_reference(const Geometry& g) {
+  std::vector<int32_t> ids(g.count);
+  std::iota(ids.begin(), ids.end(), 1);
+  std::sort(ids.begin(), ids.end(), [&](int32_t a, int32_t b) { return g.coor[a] < g.coor[b]; });
+  return ids;
+}
+
+}  // namespace
+}  // namespace lbm
+
+using namespace lbm;
+
+struct lbm_st7_handle {
+  lbm_st7_params prm{};
+  bool f64 = true;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Geometry geo;
+  Mem g[2], table, u, c0, ref_of;
+  int cur = 0;
+  bool given = true;
+  long long step = 0;
+  double tau_s = 1.0;
+  double last_ms = 0;
+  ~lbm_st7_handle() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+St7Args st7_args(lbm_st7_handle* h, bool given) {
+  St7Args a{};
+  a.src = h->g[h->cur].p;
+  a.dst = h->g[1 - h->cur].p;
+  a.table = static_cast<const int32_t*>(h->table.p);
+  a.u = h->u.p;
+  a.c_given = given ? h->c0.p : nullptr;
+  a.n = h->geo.count;
+  a.npad = h->geo.npad;
+  a.tau_s = h->tau_s;
+  return a;
+}
+
+template <typename T>
+std::vector<T> to_type(const std::vector<double>& v) {
+  return std::vector<T>(v.begin(), v.end());
+}
+
+lbm_status upload_as(lbm_st7_handle* h, Mem& m, const std::vector<double>& v) {
+  if (h->f64) {
+    LBM_CUDA_TRY(cudaMemcpyAsync(m.p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<float> f = to_type<float>(v);
+    LBM_CUDA_TRY(cudaMemcpyAsync(m.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz, const double* u_nodes,
+                          const double* c0, lbm_st7_handle** out) {
+  if (!p || !mask || !u_nodes || !c0 || !out || nx <= 0 || ny <= 0 || nz <= 0)
+    return fail(LBM_ERR_ARG, "lbm_st7_create: bad argument");
+  *out = nullptr;
+  if (!(p->diffusivity > 0)) return fail(LBM_ERR_ARG, "lbm_st7_create: diffusivity must be positive");
+  if (p->precision != LBM_PREC_F64 && p->precision != LBM_PREC_F32)
+    return fail(LBM_ERR_ARG, "lbm_st7_create: precision must be F64 or F32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device");
+  auto h = std::make_unique<lbm_st7_handle>();
+  h->prm = *p;
+  h->f64 = p->precision == LBM_PREC_F64;
+  h->device = p->device;
+  const double c_s2 = 1.0 * 1.0 / 3, dt = 1.0;
+  h->tau_s = p->diffusivity / (c_s2 * dt) + 0.5;  // ST7:1262
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  LBM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  LBM_CUDA_TRY(cudaEventCreate(&h->ev0));
+  LBM_CUDA_TRY(cudaEventCreate(&h->ev1));
+  Geometry& g = h->geo;
+  compact_reference(mask, nx, ny, nz, &g);
+  if (g.count == 0) return fail(LBM_ERR_ARG, "geometry has no pore cells");
+  order_nodes(mask, LBM_ORDER_REFERENCE, &g);
+  build_pull_table(mask, &g);
+  const int n = g.count, npad = g.npad;
+  const size_t s = h->f64 ? 8 : 4;
+  for (auto& b : h->g) LBM_CUDA_TRY(b.alloc((size_t)6 * npad * s));
+  LBM_CUDA_TRY(h->table.alloc((size_t)18 * npad * sizeof(int32_t)));
+  LBM_CUDA_TRY(h->u.alloc((size_t)3 * npad * s));
+  LBM_CUDA_TRY(h->c0.alloc((size_t)npad * s));
+  LBM_CUDA_TRY(h->ref_of.alloc((size_t)n * sizeof(int32_t)));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->table.p, g.src.data(), sizeof(int32_t) * 18 * (size_t)npad, cudaMemcpyHostToDevice,
+                               h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->ref_of.p, g.ref_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->stream));
+  std::vector<double> uu((size_t)3 * npad, 0.0), cc((size_t)npad, 0.0);
+  for (int x = 0; x < n; x++) {
+    const int r = g.ref_of[x];
+    for (int d = 0; d < 3; d++) uu[(size_t)d * npad + x] = u_nodes[(size_t)r * 3 + d];
+    const int c = g.coor[r];
+    const int i = c / (ny * nz), j = (c % (ny * nz)) / nz, k = c % nz;
+    cc[x] = c0[i + (size_t)nx * (j + (size_t)ny * k)];
+  }
+  lbm_status st;
+  if ((st = upload_as(h.get(), h->u, uu)) != LBM_OK) return st;
+  if ((st = upload_as(h.get(), h->c0, cc)) != LBM_OK) return st;
+  LBM_CUDA_TRY(cudaMemsetAsync(h->g[0].p, 0, h->g[0].bytes, h->stream));
+  St7Args a = st7_args(h.get(), true);
+  a.dst = h->g[0].p;  // the initial state is the pre-image of the first pull
+  LBM_CUDA_TRY(st7_launch_init(h->f64, a, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = h.release();
+  return LBM_OK;
+}
+
+lbm_status lbm_st7_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
+                                    lbm_st7_handle** out) {
+  if (!flow) return fail(LBM_ERR_ARG, "lbm_st7_create_from_flow: null flow handle");
+  int count = 0;
+  double por = 0;
+  long long step = 0;
+  lbm_status st = lbm_info(flow, &count, &por, &step);
+  if (st != LBM_OK) return st;
+  std::vector<double> u((size_t)(count + 1) * 3);
+  if ((st = lbm_get_fields(flow, nullptr, u.data())) != LBM_OK) return st;
+  int nx, ny, nz;
+  const uint8_t* mask = lbm_internal_mask(flow, &nx, &ny, &nz);
+  return lbm_st7_create(p, mask, nx, ny, nz, u.data(), c0, out);
+}
+
+lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return fail(LBM_ERR_ARG, "lbm_st7_step: bad argument");
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  for (int s = 0; s < nsteps; s++) {
+    LBM_CUDA_TRY(st7_launch_step(h->f64, st7_args(h, h->given), h->stream));
+    h->cur = 1 - h->cur;
+    h->given = false;
+  }
+  LBM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+  LBM_CUDA_TRY(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  LBM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  h->step += nsteps;
+  return LBM_OK;
+}
+
+lbm_status lbm_st7_get_concentration(lbm_st7_handle* h, double* c) {
+  if (!h || !c) return fail(LBM_ERR_ARG, "lbm_st7_get_concentration: bad argument");
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  const int n = h->geo.count;
+  Mem out;
+  LBM_CUDA_TRY(out.alloc(sizeof(double) * (size_t)h->geo.npad));
+  LBM_CUDA_TRY(st7_launch_conc(h->f64, st7_args(h, h->given), static_cast<double*>(out.p), h->stream));
+  std::vector<double> tmp(n);
+  LBM_CUDA_TRY(cudaMemcpyAsync(tmp.data(), out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  c[0] = 0.0;
+  for (int x = 0; x < n; x++) c[h->geo.ref_of[x]] = tmp[x];
+  return LBM_OK;
+}
+
+lbm_status lbm_st7_info(lbm_st7_handle* h, int* count, long long* step, double* last_step_ms) {
+  if (!h) return fail(LBM_ERR_ARG, "null st7 handle");
+  if (count) *count = h->geo.count;
+  if (step) *step = h->step;
+  if (last_step_ms) *last_step_ms = h->last_ms;
+  return LBM_OK;
+}
+
+void lbm_st7_destroy(lbm_st7_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  delete h;
+}
+
+lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path) {
+  if (!flow || !path) return fail(LBM_ERR_ARG, "lbm_write_velocity_for_solute: null argument");
+  int count = 0;
+  double por = 0;
+  long long step = 0;
+  lbm_status st = lbm_info(flow, &count, &por, &step);
+  if (st != LBM_OK) return st;
+  std::vector<double> u((size_t)(count + 1) * 3);
+  if ((st = lbm_get_fields(flow, nullptr, u.data())) != LBM_OK) return st;
+  int nx, ny, nz;
+  const uint8_t* mask = lbm_internal_mask(flow, &nx, &ny, &nz);
+  Geometry g;
+  compact_reference(mask, nx, ny, nz, &g);
+  const std::vector<int32_t> slab = slab_to_reference(g);
+  std::vector<double> out((size_t)count * 3);
+  for (int s = 0; s < count; s++)
+    for (int d = 0; d < 3; d++) out[(size_t)s * 3 + d] = u[(size_t)slab[s] * 3 + d];
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return fail(LBM_ERR_IO, std::string("cannot write ") + path);
+  const size_t w = std::fwrite(out.data(), sizeof(double), out.size(), fp);
+  std::fclose(fp);
+  if (w != out.size()) return fail(LBM_ERR_IO, std::string("short write to ") + path);
+  return LBM_OK;
+}
+
+lbm_status lbm_read_velocity_for_solute(const char* path, const uint8_t* mask, int nx, int ny, int nz,
+                                        double* u_nodes) {
+  if (!path || !mask || !u_nodes) return fail(LBM_ERR_ARG, "lbm_read_velocity_for_solute: null argument");
+  Geometry g;
+  compact_reference(mask, nx, ny, nz, &g);
+  std::vector<double> in((size_t)g.count * 3);
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return fail(LBM_ERR_IO, std::string("file open error on ") + path);
+  const size_t r = std::fread(in.data(), sizeof(double), in.size(), fp);
+  std::fclose(fp);
+  if (r != in.size()) return fail(LBM_ERR_FORMAT, std::string(path) + ": shorter than Count*3 doubles");
+  const std::vector<int32_t> slab = slab_to_reference(g);
+  std::memset(u_nodes, 0, sizeof(double) * 3);
+  for (int s = 0; s < g.count; s++)
+    for (int d = 0; d < 3; d++) u_nodes[(size_t)slab[s] * 3 + d] = in[(size_t)s * 3 + d];
+  return LBM_OK;
+}
+
+}  // extern "C"

@@ -199,7 +199,81 @@ _SIGNATURES = {
     "lbm_cg_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                      C.POINTER(C.c_double)], C.c_int),
     "lbm_cg_destroy": ([C.c_void_p], None),
+    "lbm_st7_create": ([C.c_void_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P, _F64P, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_st7_create_from_flow": ([C.c_void_p, C.c_void_p, _F64P, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_st7_step": ([C.c_void_p, C.c_int], C.c_int),
+    "lbm_st7_get_concentration": ([C.c_void_p, _F64P], C.c_int),
+    "lbm_st7_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_double)], C.c_int),
+    "lbm_st7_destroy": ([C.c_void_p], None),
+    "lbm_write_velocity_for_solute": ([C.c_void_p, C.c_char_p], C.c_int),
+    "lbm_read_velocity_for_solute": ([C.c_char_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
 }
+
+
+class ST7Params(C.Structure):
+    _fields_ = [("diffusivity", C.c_double), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class Solute:
+    """D3Q7 passive-scalar solve advected by a fixed velocity field.
+
+    Either ``u_nodes`` ([(count+1), 3], the order of SinglePhase.fields()) or
+    ``flow`` (a SinglePhase whose current velocity is used) must be given."""
+
+    def __init__(self, mask, c0, diffusivity, u_nodes=None, flow=None, precision="f64", device=0):
+        p = ST7Params(float(diffusivity), PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                      int(device))
+        c0 = np.ascontiguousarray(c0, dtype=np.float64).reshape(-1)
+        h = C.c_void_p()
+        if flow is not None:
+            _check(lib().lbm_st7_create_from_flow(C.byref(p), flow._h, c0, C.byref(h)))
+        else:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            nz, ny, nx = m.shape
+            u = np.ascontiguousarray(u_nodes, dtype=np.float64).reshape(-1)
+            _check(lib().lbm_st7_create(C.byref(p), m.reshape(-1), nx, ny, nz, u, c0, C.byref(h)))
+        self._h = h
+        c, st, ms = C.c_int(), C.c_longlong(), C.c_double()
+        _check(lib().lbm_st7_info(h, C.byref(c), C.byref(st), C.byref(ms)))
+        self.count = c.value
+
+    def step(self, n=1):
+        _check(lib().lbm_st7_step(self._h, int(n)))
+
+    def concentration(self):
+        c = np.zeros(self.count + 1)
+        _check(lib().lbm_st7_get_concentration(self._h, c))
+        return c
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_st7_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def write_velocity_for_solute(flow, path):
+    _check(lib().lbm_write_velocity_for_solute(flow._h, os.fsencode(path)))
+
+
+def read_velocity_for_solute(path, mask):
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    nz, ny, nx = m.shape
+    count = int((m == 0).sum())
+    u = np.zeros((count + 1) * 3)
+    _check(lib().lbm_read_velocity_for_solute(os.fsencode(path), m.reshape(-1), nx, ny, nz, u))
+    return u.reshape(-1, 3)
 
 
 class ColourGradient:

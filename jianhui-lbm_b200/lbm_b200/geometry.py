@@ -95,23 +95,24 @@ def random_cylinders(shape, target_porosity, radius, seed, max_cylinders=1_000_0
     nx, ny, nz = shape
     rng = np.random.default_rng(seed)
     mask = np.zeros((nz, ny, nx), dtype=np.uint8)
-    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
     goal = target_porosity * mask.size
     pores = mask.size
     n = 0
     L = np.array([nx, ny, nz], dtype=np.float64)
+
+    def nearest(c, size, p):  # per-axis nearest-image offsets (1-D)
+        d = np.arange(size, dtype=np.float64) - p
+        return d - size * np.round(d / size)
+
     while pores > goal and n < max_cylinders:
         p = rng.uniform(0, 1, 3) * L
         v = rng.normal(size=3)
         v /= np.linalg.norm(v)
-        dx = x - p[0]
-        dy = y - p[1]
-        dz = z - p[2]
-        dx -= nx * np.round(dx / nx)
-        dy -= ny * np.round(dy / ny)
-        dz -= nz * np.round(dz / nz)
-        t = dx * v[0] + dy * v[1] + dz * v[2]
-        d2 = dx * dx + dy * dy + dz * dz - t * t
+        dx = nearest(None, nx, p[0])[None, None, :]
+        dy = nearest(None, ny, p[1])[None, :, None]
+        dz = nearest(None, nz, p[2])[:, None, None]
+        t = (dz * v[2] + dy * v[1]) + dx * v[0]
+        d2 = (dz * dz + dy * dy) + dx * dx - t * t
         hit = (d2 <= radius * radius) & (mask == 0)
         pores -= int(np.count_nonzero(hit))
         mask[hit] = 1

@@ -220,6 +220,36 @@ class ColourGradientRun:
                 "psi": self.psi.copy(), "rho_r": self.rho_r.copy(), "rho_b": self.rho_b.copy()}
 
 
+class SoluteRun:
+    """D3Q7 solute restatement (lbm_oracle_st.c), periodic, fixed velocity."""
+
+    def __init__(self, mask, c0_cells, diffusivity, u_nodes):
+        L = _load("liboracle.so")
+        self.L = L
+        L.orc_st7_tau.argtypes = [C.c_double]
+        L.orc_st7_tau.restype = C.c_double
+        L.orc_st7_init.argtypes = [C.c_int, _F64P, _F64P, _F64P, _F64P]
+        L.orc_st7_step.argtypes = [C.c_int, _I32P, _F64P, C.c_double, _F64P, _F64P, _F64P]
+        R = Restatement()
+        self.mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        self.coor = R.compact(self.mask)
+        self.count = n = self.coor.size - 1
+        self.nei = np.ascontiguousarray(R.nei_loc(self.mask, self.coor).reshape(-1))
+        self.tau = L.orc_st7_tau(diffusivity)
+        self.u = np.ascontiguousarray(u_nodes, dtype=np.float64).reshape(-1)
+        c0 = np.zeros(n + 1)
+        c0[1:] = np.ascontiguousarray(c0_cells, dtype=np.float64).reshape(-1)[self.mask.reshape(-1) == 0]
+        self.g, self.G, self.C = np.zeros((n + 1) * 7), np.zeros((n + 1) * 7), np.zeros(n + 1)
+        L.orc_st7_init(n, self.u, c0, self.g, self.C)
+
+    def step(self, k=1):
+        for _ in range(k):
+            self.L.orc_st7_step(self.count, self.nei, self.u, self.tau, self.g, self.G, self.C)
+
+    def concentration(self):
+        return self.C.copy()
+
+
 def write_phase_file(path, psi):
     """Phase file of the colour-gradient solver: one value per cell, ASCII,
     x fastest (read with `fin >> pore2` into a float, CG3:2144-2150)."""
