@@ -225,6 +225,22 @@ LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
  * bytes one fluid-node update moves (2*19*s + 18*4). */
 LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
 
+/* ----------------------------------------------- reference output formats */
+
+/* ASCII VTK STRUCTURED_POINTS files of the reference, same header lines and
+ * number formatting: LBM_Geometry.vtk (SP3:3205-3247, 0 pore / 1 solid),
+ * LBM_velocity_Vector_<n>.vtk (SP3:3286-3377), LBM_Density_<n>.vtk
+ * (SP3:3379-3466).  The caller chooses the path. */
+LBM_API lbm_status lbm_write_vtk_geometry(const uint8_t* mask, int nx, int ny, int nz, const char* path);
+LBM_API lbm_status lbm_write_vtk_velocity(lbm_handle* h, const char* path);
+LBM_API lbm_status lbm_write_vtk_density(lbm_handle* h, const char* path);
+
+/* <prefix>LBM_checkpoint_{velocity,rho,f}_<m>.0.bin_input: raw doubles in the
+ * reference layout including row 0 (Backup SP3:3469-3516); reading restores
+ * the state like Backup_init (SP3:3652-3767). */
+LBM_API lbm_status lbm_write_checkpoint(lbm_handle* h, const char* prefix, long long m);
+LBM_API lbm_status lbm_read_checkpoint(lbm_handle* h, const char* prefix, long long m);
+
 /* --------------------------------------- colour-gradient two-phase solver */
 
 /* Physics of the colour-gradient model (the INPUT_CG_SPARSE fields of
@@ -305,6 +321,16 @@ LBM_API void lbm_st7_destroy(lbm_st7_handle* h);
 LBM_API lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path);
 LBM_API lbm_status lbm_read_velocity_for_solute(const char* path, const uint8_t* mask, int nx, int ny, int nz,
                                                 double* u_nodes);
+
+/* The same file in either record order.  LBM_SOLUTE_ORDER_SLAB is the one
+ * above (written by SP:5093-5120, read by the solute programs,
+ * Backup_input_v, Solute_Transport_MPI_Software_Spars.cpp:3649-3690); LBM_SOLUTE_ORDER_XFAST
+ * is what the 3-D partition program writes at one rank
+ * (output_velocity_for_solute, SP3:3769-3797): pore cells with x fastest. */
+typedef enum { LBM_SOLUTE_ORDER_SLAB = 0, LBM_SOLUTE_ORDER_XFAST = 1 } lbm_solute_order;
+LBM_API lbm_status lbm_write_velocity_for_solute_ordered(lbm_handle* flow, const char* path, int order);
+LBM_API lbm_status lbm_read_velocity_for_solute_ordered(const char* path, const uint8_t* mask, int nx, int ny,
+                                                        int nz, int order, double* u_nodes);
 
 /* ------------------------------------------ many independent solves (pool) */
 

@@ -38,7 +38,10 @@ CUDA_SOURCES = [
     ("cg_fast.cu", []),
     ("st7_kernels.cu", ["-fmad=false"]),
 ]
-CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp"]
+CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp", "output.cpp"]
+# Command-line drivers linked against liblbm.so: (source, executable name).
+EXECUTABLES = [("lbm_sp_main.cpp", "lbm_sp")]
+BIN = os.path.join(HERE, "lbm_b200")
 
 
 def _headers():
@@ -67,9 +70,11 @@ def build(verbose=False, ptxas_info=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
     sources = [os.path.join(CSRC, s) for s, _ in CUDA_SOURCES] + [os.path.join(CSRC, s) for s in CXX_SOURCES]
-    if not (force or ptxas_info) and os.path.exists(OUT):
+    exes = [os.path.join(BIN, name) for _, name in EXECUTABLES]
+    sources += [os.path.join(CSRC, s) for s, _ in EXECUTABLES]
+    if not (force or ptxas_info) and all(os.path.exists(p) for p in [OUT] + exes):
         newest = max(os.path.getmtime(p) for p in sources + headers + [os.path.abspath(__file__)])
-        if os.path.getmtime(OUT) >= newest:
+        if min(os.path.getmtime(p) for p in [OUT] + exes) >= newest:
             return OUT, ""
     objs = []
     logs = []
@@ -97,6 +102,13 @@ def build(verbose=False, ptxas_info=False, force=False):
                "-cudart", "static", "-Xlinker", "--exclude-libs,ALL"]
         logs.append(_run(cmd, verbose))
         shutil.move(tmp, OUT)
+    for src, name in EXECUTABLES:
+        s = os.path.join(CSRC, src)
+        exe = os.path.join(BIN, name)
+        if force or _stale(exe, s, headers + [OUT]):
+            cmd = [CXX, "-O2", "-std=c++17", "-Wall", *INCLUDES, s, "-o", exe, "-L", BIN, "-llbm",
+                   "-Wl,-rpath,$ORIGIN"]
+            logs.append(_run(cmd, verbose))
     return OUT, "".join(logs)
 
 

@@ -216,8 +216,10 @@ void lbm_st7_destroy(lbm_st7_handle* h) {
   delete h;
 }
 
-lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path) {
+lbm_status lbm_write_velocity_for_solute_ordered(lbm_handle* flow, const char* path, int order) {
   if (!flow || !path) return fail(LBM_ERR_ARG, "lbm_write_velocity_for_solute: null argument");
+  if (order != LBM_SOLUTE_ORDER_SLAB && order != LBM_SOLUTE_ORDER_XFAST)
+    return fail(LBM_ERR_ARG, "lbm_write_velocity_for_solute: unknown record order");
   int count = 0;
   double por = 0;
   long long step = 0;
@@ -225,14 +227,19 @@ lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path) {
   if (st != LBM_OK) return st;
   std::vector<double> u((size_t)(count + 1) * 3);
   if ((st = lbm_get_fields(flow, nullptr, u.data())) != LBM_OK) return st;
-  int nx, ny, nz;
-  const uint8_t* mask = lbm_internal_mask(flow, &nx, &ny, &nz);
-  Geometry g;
-  compact_reference(mask, nx, ny, nz, &g);
-  const std::vector<int32_t> slab = slab_to_reference(g);
   std::vector<double> out((size_t)count * 3);
-  for (int s = 0; s < count; s++)
-    for (int d = 0; d < 3; d++) out[(size_t)s * 3 + d] = u[(size_t)slab[s] * 3 + d];
+  if (order == LBM_SOLUTE_ORDER_XFAST) {
+    // the library's ids are the x-fastest compaction: record s is id s+1
+    std::copy(u.begin() + 3, u.end(), out.begin());
+  } else {
+    int nx, ny, nz;
+    const uint8_t* mask = lbm_internal_mask(flow, &nx, &ny, &nz);
+    Geometry g;
+    compact_reference(mask, nx, ny, nz, &g);
+    const std::vector<int32_t> slab = slab_to_reference(g);
+    for (int s = 0; s < count; s++)
+      for (int d = 0; d < 3; d++) out[(size_t)s * 3 + d] = u[(size_t)slab[s] * 3 + d];
+  }
   FILE* fp = std::fopen(path, "wb");
   if (!fp) return fail(LBM_ERR_IO, std::string("cannot write ") + path);
   const size_t w = std::fwrite(out.data(), sizeof(double), out.size(), fp);
@@ -241,9 +248,15 @@ lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path) {
   return LBM_OK;
 }
 
-lbm_status lbm_read_velocity_for_solute(const char* path, const uint8_t* mask, int nx, int ny, int nz,
-                                        double* u_nodes) {
+lbm_status lbm_write_velocity_for_solute(lbm_handle* flow, const char* path) {
+  return lbm_write_velocity_for_solute_ordered(flow, path, LBM_SOLUTE_ORDER_SLAB);
+}
+
+lbm_status lbm_read_velocity_for_solute_ordered(const char* path, const uint8_t* mask, int nx, int ny, int nz,
+                                                int order, double* u_nodes) {
   if (!path || !mask || !u_nodes) return fail(LBM_ERR_ARG, "lbm_read_velocity_for_solute: null argument");
+  if (order != LBM_SOLUTE_ORDER_SLAB && order != LBM_SOLUTE_ORDER_XFAST)
+    return fail(LBM_ERR_ARG, "lbm_read_velocity_for_solute: unknown record order");
   Geometry g;
   compact_reference(mask, nx, ny, nz, &g);
   std::vector<double> in((size_t)g.count * 3);
@@ -252,11 +265,20 @@ lbm_status lbm_read_velocity_for_solute(const char* path, const uint8_t* mask, i
   const size_t r = std::fread(in.data(), sizeof(double), in.size(), fp);
   std::fclose(fp);
   if (r != in.size()) return fail(LBM_ERR_FORMAT, std::string(path) + ": shorter than Count*3 doubles");
-  const std::vector<int32_t> slab = slab_to_reference(g);
   std::memset(u_nodes, 0, sizeof(double) * 3);
+  if (order == LBM_SOLUTE_ORDER_XFAST) {
+    std::copy(in.begin(), in.end(), u_nodes + 3);
+    return LBM_OK;
+  }
+  const std::vector<int32_t> slab = slab_to_reference(g);
   for (int s = 0; s < g.count; s++)
     for (int d = 0; d < 3; d++) u_nodes[(size_t)slab[s] * 3 + d] = in[(size_t)s * 3 + d];
   return LBM_OK;
+}
+
+lbm_status lbm_read_velocity_for_solute(const char* path, const uint8_t* mask, int nx, int ny, int nz,
+                                        double* u_nodes) {
+  return lbm_read_velocity_for_solute_ordered(path, mask, nx, ny, nz, LBM_SOLUTE_ORDER_SLAB, u_nodes);
 }
 
 }  // extern "C"

@@ -207,7 +207,43 @@ _SIGNATURES = {
     "lbm_st7_destroy": ([C.c_void_p], None),
     "lbm_write_velocity_for_solute": ([C.c_void_p, C.c_char_p], C.c_int),
     "lbm_read_velocity_for_solute": ([C.c_char_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
+    "lbm_write_velocity_for_solute_ordered": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
+    "lbm_read_velocity_for_solute_ordered": ([C.c_char_p, _U8P, C.c_int, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
+    "lbm_write_vtk_geometry": ([_U8P, C.c_int, C.c_int, C.c_int, C.c_char_p], C.c_int),
+    "lbm_write_vtk_velocity": ([C.c_void_p, C.c_char_p], C.c_int),
+    "lbm_write_vtk_density": ([C.c_void_p, C.c_char_p], C.c_int),
+    "lbm_write_checkpoint": ([C.c_void_p, C.c_char_p, C.c_longlong], C.c_int),
+    "lbm_read_checkpoint": ([C.c_void_p, C.c_char_p, C.c_longlong], C.c_int),
 }
+
+
+def write_vtk_geometry(mask, path):
+    """LBM_Geometry.vtk of a [nz, ny, nx] mask (non-zero = solid)."""
+    m = np.ascontiguousarray(mask != 0, dtype=np.uint8)
+    nz, ny, nx = m.shape
+    _check(lib().lbm_write_vtk_geometry(m.reshape(-1), nx, ny, nz, os.fsencode(path)))
+
+
+def write_vtk_velocity(flow, path):
+    _check(lib().lbm_write_vtk_velocity(flow._h, os.fsencode(path)))
+
+
+def write_vtk_density(flow, path):
+    _check(lib().lbm_write_vtk_density(flow._h, os.fsencode(path)))
+
+
+def write_checkpoint(flow, prefix, m):
+    """Writes <prefix>LBM_checkpoint_{velocity,rho,f}_<m>.0.bin_input."""
+    _check(lib().lbm_write_checkpoint(flow._h, os.fsencode(prefix), int(m)))
+
+
+def read_checkpoint(flow, prefix, m):
+    _check(lib().lbm_read_checkpoint(flow._h, os.fsencode(prefix), int(m)))
+
+
+def driver_path():
+    """Path of the lbm_sp command-line driver built beside liblbm.so."""
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "lbm_sp")
 
 
 class ST7Params(C.Structure):
@@ -263,16 +299,22 @@ class Solute:
         self.close()
 
 
-def write_velocity_for_solute(flow, path):
-    _check(lib().lbm_write_velocity_for_solute(flow._h, os.fsencode(path)))
+SOLUTE_ORDERS = {"slab": 0, "xfast": 1}
 
 
-def read_velocity_for_solute(path, mask):
+def write_velocity_for_solute(flow, path, order="slab"):
+    """Velocity_for_solute file; ``order`` "slab" is what the solute programs
+    read, "xfast" what the 3-D partition program writes."""
+    _check(lib().lbm_write_velocity_for_solute_ordered(flow._h, os.fsencode(path), SOLUTE_ORDERS[order]))
+
+
+def read_velocity_for_solute(path, mask, order="slab"):
     m = np.ascontiguousarray(mask, dtype=np.uint8)
     nz, ny, nx = m.shape
     count = int((m == 0).sum())
     u = np.zeros((count + 1) * 3)
-    _check(lib().lbm_read_velocity_for_solute(os.fsencode(path), m.reshape(-1), nx, ny, nz, u))
+    _check(lib().lbm_read_velocity_for_solute_ordered(os.fsencode(path), m.reshape(-1), nx, ny, nz,
+                                                      SOLUTE_ORDERS[order], u))
     return u.reshape(-1, 3)
 
 

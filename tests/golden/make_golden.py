@@ -2,10 +2,13 @@
 solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
 compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
 
-    python tests/golden/make_golden.py [--cfg1]
+    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs]
 
 Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
+  sp_outputs.npz  the reference program itself (oracle/_ref/ref_sp3_main)
+                run on an INPUT.dat: every file it writes  (--outputs)
+  cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
   sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
                 M^-1, f/u/rho after 20 steps, Error and Comput_Perm outputs
   sp_24.npz     24^3 spheres, 200 steps: compaction digest, u, rho, f digest,
@@ -119,14 +122,86 @@ def cg_small():
     print("cg_small", mask.shape, ref.count)
 
 
+def input_text(**kv):
+    """INPUT.dat for the reference program: INPUT_sp.dat with some values
+    replaced; keys are the 0-based line numbers of the file."""
+    lines = open(os.path.join(HERE, "INPUT_sp.dat")).read().splitlines()
+    for i, v in kv.items():
+        lines[int(i[1:])] = f"{v}\t\t:{lines[int(i[1:])].split(':', 1)[1]}"
+    return "\n".join(lines) + "\n"
+
+
+# Files the reference program writes; rows 0 of the rho/velocity checkpoints
+# are uninitialised memory in the reference and are not compared.
+TEXT_OUTPUTS = ["Results.txt", "Permeability_error_local_Perm.txt", "Velocity_ave_max.txt", "bodyforce.txt",
+                "General_Results.txt"]
+
+
+def run_program(workdir, input_txt, mask, args=()):
+    import subprocess
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_sp3_main")
+    G.write_ascii(os.path.join(workdir, "mask.dat"), mask)
+    with open(os.path.join(workdir, "INPUT.dat"), "w") as f:
+        f.write(input_txt)
+    subprocess.run([exe, "INPUT.dat", *args], cwd=workdir, check=True, capture_output=True)
+
+
+def collect(workdir, prefix="out_"):
+    out = {}
+    for name in sorted(os.listdir(workdir)):
+        if not name.startswith(prefix):
+            continue
+        key = name[len(prefix):]
+        data = open(os.path.join(workdir, name), "rb").read()
+        if key.startswith("LBM_checkpoint_"):
+            width = {"rho": 1, "velocity": 3, "f": 19}[key.split("_")[2]]
+            out[key] = digest(np.frombuffer(data, dtype=np.float64).reshape(-1, width)[1:])
+        elif key.startswith("Velocity_for_solute_"):
+            out[key] = digest(np.frombuffer(data, dtype=np.float64))
+        else:
+            out[key] = data
+    return out
+
+
+def program_outputs():
+    """The reference program run end to end on 14x12x10 spheres: 251 steps
+    (n_max=250) writing every output family (reports every 50 steps, VTK
+    every 100, checkpoints every 100 and at the end, solute velocity at 200).
+    Stored: the INPUT file, the mask, text and VTK outputs verbatim, sha256 of
+    checkpoint rows 1.. and of the solute velocity file.
+
+    The reference's restart path (USE BACKUP DATA) is not recorded: its
+    Backup_init (SP3:3663) divides by the global Zoom, which only init() sets,
+    so a restarted run has dt = dx = inf and stops at its first report with
+    NaN."""
+    import tempfile
+
+    mask = G.overlapping_spheres((14, 12, 10), 0.6, 2.5, seed=21)
+    in_a = input_text(L1="mask.dat", L2="14 12 10", L3=250, L17=1, L18=50, L20=100, L21=100, L32=100, L34=200)
+    with tempfile.TemporaryDirectory() as d:
+        run_program(d, in_a, mask)
+        a = collect(d, "out_")
+    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "input": np.frombuffer(in_a.encode(), np.uint8),
+            "names": np.array(sorted(a))}
+    for k, v in a.items():
+        blob[k] = np.frombuffer(v, np.uint8) if isinstance(v, bytes) else np.array(v)
+    np.savez_compressed(os.path.join(HERE, "sp_outputs.npz"), **blob)
+    print("sp_outputs", sorted(a))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg1", action="store_true")
     ap.add_argument("--cg", action="store_true")
+    ap.add_argument("--outputs", action="store_true")
     a = ap.parse_args()
     oracle.build()
     if a.cg:
         cg_small()
+        return
+    if a.outputs:
+        program_outputs()
         return
     ref = oracle.ReferenceSP3()
     if a.cfg1:

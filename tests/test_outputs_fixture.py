@@ -1,0 +1,43 @@
+"""The output-file fixture is what the reference program writes.
+
+Re-runs oracle/_ref/ref_sp3_main (the reference's own program compiled from
+its source, single rank) on the stored INPUT.dat and mask and compares every
+file with tests/golden/sp_outputs.npz.  Skipped where the program was not
+built (no reference sources on the machine).
+"""
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, unpack_mask
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PROGRAM = os.path.join(ROOT, "oracle", "_ref", "ref_sp3_main")
+TIMING = (b"Elapsed time is", b"The expected completion time is")
+
+
+@pytest.mark.skipif(not os.path.exists(PROGRAM), reason="reference program not built")
+def test_fixture_is_the_reference_programs_output(tmp_path):
+    from lbm_b200 import geometry as G
+
+    z = np.load(os.path.join(GOLDEN, "sp_outputs.npz"))
+    G.write_ascii(str(tmp_path / "mask.dat"), unpack_mask(z["mask"], z["shape"]))
+    (tmp_path / "INPUT.dat").write_bytes(z["input"].tobytes())
+    subprocess.run([PROGRAM, "INPUT.dat"], cwd=tmp_path, check=True, capture_output=True, timeout=120)
+    for name in (str(n) for n in z["names"]):
+        data = (tmp_path / ("out_" + name)).read_bytes()
+        if name.startswith("LBM_checkpoint_"):
+            width = {"rho": 1, "velocity": 3, "f": 19}[name.split("_")[2]]
+            rows = np.frombuffer(data, dtype=np.float64).reshape(-1, width)[1:]
+            assert hashlib.sha256(rows.tobytes()).hexdigest() == str(z[name]), name
+        elif name.startswith("Velocity_for_solute_"):
+            assert hashlib.sha256(data).hexdigest() == str(z[name]), name
+        else:
+            want = z[name].tobytes()
+            if name == "Results.txt":
+                keep = lambda b: b"\n".join(l for l in b.split(b"\n") if not l.startswith(TIMING))  # noqa: E731
+                data, want = keep(data), keep(want)
+            assert data == want, name
