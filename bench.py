@@ -130,33 +130,22 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
+    from lbm_b200 import dispatch
 
-        import torch.distributed as dist
-
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-        pg = dist
-    return world, rank, local, pg
+    world, rank, local = dispatch.dist_env()
+    return world, rank, local, dispatch.init_process_group()
 
 
 def allmax(pg, x):
-    if pg is None:
-        return x
-    import torch
+    from lbm_b200 import dispatch
 
-    t = torch.tensor([float(x)], dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    return dispatch.max_over_ranks(pg, x)
 
 
 def barrier(pg):
-    if pg is not None:
-        pg.barrier()
+    from lbm_b200 import dispatch
+
+    dispatch.barrier(pg)
 
 
 # ------------------------------------------------------------ reference arm
@@ -309,17 +298,9 @@ def run_ours(a):
 
 # ------------------------------------------------------------ batch / serve
 def shard(items, world, rank, weight):
-    """Greedy longest-first assignment of independent solves to ranks (no
-    collective needed: each rank runs its own share)."""
-    order = sorted(range(len(items)), key=lambda i: -weight(items[i]))
-    load = [0.0] * world
-    mine = []
-    for i in order:
-        r = min(range(world), key=lambda k: load[k])
-        load[r] += weight(items[i])
-        if r == rank:
-            mine.append(i)
-    return sorted(mine)
+    from lbm_b200 import dispatch
+
+    return dispatch.shard([weight(x) for x in items], world, rank)
 
 
 def run_batch(a):
