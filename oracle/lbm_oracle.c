@@ -248,9 +248,31 @@ static inline double rowdot(const double* A, int r, const double* x) {
  * halfway bounce-back through nei_loc) followed by `comput_macro_variables`
  * (SP3:2401-2446: f <- F, rho = sum f, u = (sum e f + dt g/2)/rho, u0 <- old u).
  * MI must be the matrix from orc_mrt_matrices. */
+static void sp_boundaries(int count, const int32_t* nei, const double* M, const double* MI, int sub_bc,
+                          const int* pre, const double* p, const int* vel, const double* v,
+                          const int32_t* lists, const int* len, const double* rho, const double* u,
+                          const double* f, double* F);
+
+void orc_sp_step_bc(int count, const int32_t* nei, const double* M, const double* MI, const double* S,
+                    double gx, double gy, double gz, double* rho, double* u, double* u0, double* f, double* F,
+                    int sub_bc, const int* pre, const double* p, const int* vel, const double* v,
+                    const int32_t* lists, const int* len);
+
 void orc_sp_step(int count, const int32_t* nei, const double* M, const double* MI, const double* S,
                  double gx, double gy, double gz, double* rho, double* u, double* u0, double* f,
                  double* F) {
+  orc_sp_step_bc(count, nei, M, MI, S, gx, gy, gz, rho, u, u0, f, F, 0, NULL, NULL, NULL, NULL, NULL, NULL);
+}
+
+/* As orc_sp_step, with the reference's pressure and velocity boundaries
+ * applied between streaming and the macro step (SP3:580-585); pre/p/vel/v are
+ * NULL for none.  Faces of pre, p, vel, v in INPUT.dat order xp, xn, yp, yn,
+ * zp, zn; lists/len are the six boundary-node lists of orc_face_list in the
+ * order xn, xp, yn, yp, zn, zp, concatenated. */
+void orc_sp_step_bc(int count, const int32_t* nei, const double* M, const double* MI, const double* S,
+                    double gx, double gy, double gz, double* rho, double* u, double* u0, double* f, double* F,
+                    int sub_bc, const int* pre, const double* p, const int* vel, const double* v,
+                    const int32_t* lists, const int* len) {
   const double c_l = 1.0, dt = 1.0;
   const double c_s2 = c_l * c_l / 3;
   const double g[3] = {gx, gy, gz};
@@ -282,6 +304,7 @@ void orc_sp_step(int count, const int32_t* nei, const double* M, const double* M
         F[(long)c * Q19 + OPP19[q]] = mi[q];
     }
   }
+  if (lists) sp_boundaries(count, nei, M, MI, sub_bc, pre, p, vel, v, lists, len, rho, u, f, F);
   for (int c = 1; c <= count; c++) {
     double* uc = &u[(long)c * 3];
     for (int d = 0; d < 3; d++) u0[(long)c * 3 + d] = uc[d];
@@ -298,6 +321,174 @@ void orc_sp_step(int count, const int32_t* nei, const double* M, const double* M
     uc[0] = (ux + dt * g[0] / 2) / r;
     uc[1] = (uy + dt * g[1] / 2) / r;
     uc[2] = (uz + dt * g[2] / 2) / r;
+  }
+}
+
+/* Boundary-node list of one face (SP3:1164-1222 at one rank): the pore cells
+ * of the face in the reference's loop order, as fluid ids.  face: 0 x=0
+ * (bclx, k outer, j inner), 1 x=nx-1 (bcrx), 2 y=0 (bcly, k outer, i inner),
+ * 3 y=ny-1 (bcry), 4 z=0 (bclz, j outer, i inner), 5 z=nz-1 (bcrz).  Returns
+ * the length; out may be NULL to count only. */
+int orc_face_list(const uint8_t* mask, int nx, int ny, int nz, int face, int32_t* out) {
+  int32_t* id = (int32_t*)calloc((size_t)nx * ny * nz, sizeof(int32_t));
+  int count = 0;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        if (mask[i + (long)nx * (j + (long)ny * k)] == 0) id[i + (long)nx * (j + (long)ny * k)] = ++count;
+  const int axis = face / 2, side = face % 2;
+  const int n0 = axis == 0 ? nz : (axis == 1 ? nz : ny);  /* outer loop extent */
+  const int n1 = axis == 0 ? ny : nx;                      /* inner loop extent */
+  int len = 0;
+  for (int a = 0; a < n0; a++)
+    for (int b = 0; b < n1; b++) {
+      int i, j, k;
+      if (axis == 0) { i = side ? nx - 1 : 0; j = b; k = a; }
+      else if (axis == 1) { i = b; j = side ? ny - 1 : 0; k = a; }
+      else { i = b; j = a; k = side ? nz - 1 : 0; }
+      const int32_t c = id[i + (long)nx * (j + (long)ny * k)];
+      if (c > 0) {
+        if (out) out[len] = c;
+        len++;
+      }
+    }
+  free(id);
+  return len;
+}
+
+/* `boundary_pressure` (SP3:2656-3116) then `boundary_velocity`
+ * (SP3:2450-2655) at one rank, each called only when one of its faces is on
+ * (SP3:580-585).  They overwrite post-streaming F of the face nodes from the
+ * previous step's f, rho, u (the reference calls them before the macro step)
+ * and, for Sub_BC 2 velocity faces, from F itself.  Kept as the reference
+ * has them:
+ *   - pressure Sub_BC 1: a node whose inward neighbour is solid writes the
+ *     rest-state equilibrium into the i-th node of the y=ny-1 list, whatever
+ *     face it belongs to (SP3:2733-2790); an index past that list's end is
+ *     outside the reference's array and is skipped here;
+ *   - pressure Sub_BC 3 takes the non-equilibrium part from the -y neighbour
+ *     (nei_loc[.][4]) on every face (SP3:3000-3110), row 0 when that is solid;
+ *   - velocity Sub_BC 2: the x flags drive the z faces with the z velocities
+ *     and the z flags the x faces (SP3:2556-2591).
+ * Face order of every pass: pressure yp, yn, xp, xn, zp, zn; velocity Sub_BC
+ * 0/1 yn, yp, zn, zp, xn, xp; Sub_BC 2 and 3 yp, yn, then (as above) x, z. */
+static void sp_boundaries(int count, const int32_t* nei, const double* M, const double* MI, int sub_bc,
+                          const int* pre, const double* p, const int* vel, const double* v,
+                          const int32_t* lists, const int* len, const double* rho, const double* u,
+                          const double* f, double* F) {
+  (void)count;
+  const int32_t* L[6];
+  int off = 0;
+  for (int s = 0; s < 6; s++) {
+    L[s] = lists + off;
+    off += len[s];
+  }
+  /* INPUT order index (xp, xn, yp, yn, zp, zn) -> list slot (xn, xp, yn, yp, zn, zp) and the push
+   * direction towards the inside */
+  static const int slot_of[6] = {1, 0, 3, 2, 5, 4};
+  static const int dir_in[6] = {2, 1, 4, 3, 6, 5};
+  const double zero[3] = {0.0, 0.0, 0.0};
+  int any_pre = 0, any_vel = 0;
+  for (int s = 0; s < 6; s++) {
+    any_pre |= pre && pre[s] == 1;
+    any_vel |= vel && vel[s] == 1;
+  }
+  if (any_pre) {
+    static const int order[6] = {2, 3, 0, 1, 4, 5}; /* yp, yn, xp, xn, zp, zn */
+    for (int oi = 0; oi < 6; oi++) {
+      const int fc = order[oi];
+      if (pre[fc] != 1) continue;
+      const int32_t* lst = L[slot_of[fc]];
+      const int n = len[slot_of[fc]];
+      const double rb = p[fc];
+      for (int i = 0; i < n; i++) {
+        const int32_t b = lst[i];
+        const int32_t nb = nei[(long)b * Q19 + dir_in[fc]];
+        double* Fb = &F[(long)b * Q19];
+        if (sub_bc == 0) {
+          for (int ks = 0; ks < Q19; ks++) Fb[ks] = feq_ref(ks, rb, zero);
+        } else if (sub_bc == 1) {
+          if (nb > 0) {
+            for (int ks = 0; ks < Q19; ks++) Fb[ks] = feq_ref(ks, rb, &u[(long)nb * 3]);
+          } else if (i < len[3]) {
+            double* Ft = &F[(long)L[3][i] * Q19];
+            for (int ks = 0; ks < Q19; ks++) Ft[ks] = feq_ref(ks, rb, zero);
+          }
+        } else if (sub_bc == 2) {
+          if (nb > 0) {
+            double ml[Q19];
+            for (int mi = 0; mi < Q19; mi++) {
+              ml[mi] = 0;
+              for (int mj = 0; mj < Q19; mj++) ml[mi] += M[mi * Q19 + mj] * f[(long)nb * Q19 + mj];
+            }
+            ml[0] = rb;
+            for (int mi = 0; mi < Q19; mi++) {
+              Fb[mi] = 0;
+              for (int mj = 0; mj < Q19; mj++) Fb[mi] += MI[mi * Q19 + mj] * ml[mj];
+            }
+          } else {
+            for (int ks = 0; ks < Q19; ks++) Fb[ks] = feq_ref(ks, rb, zero);
+          }
+        } else if (sub_bc == 3) {
+          if (nb > 0) {
+            const int32_t n4 = nei[(long)b * Q19 + 4];
+            for (int ks = 0; ks < Q19; ks++)
+              Fb[ks] = feq_ref(ks, rb, &u[(long)nb * 3]) + f[(long)n4 * Q19 + ks] -
+                       feq_ref(ks, rho[nb], &u[(long)nb * 3]);
+          } else {
+            for (int ks = 0; ks < Q19; ks++) Fb[ks] = feq_ref(ks, rb, zero);
+          }
+        }
+      }
+    }
+  }
+  if (any_vel) {
+    double uf[6][3];
+    for (int s = 0; s < 6; s++) {
+      uf[s][0] = uf[s][1] = uf[s][2] = 0.0;
+      uf[s][s / 2] = v[s];
+    }
+    if (sub_bc == 0 || sub_bc == 1) {
+      static const int order[6] = {3, 2, 5, 4, 1, 0}; /* yn, yp, zn, zp, xn, xp */
+      for (int oi = 0; oi < 6; oi++) {
+        const int fc = order[oi];
+        if (vel[fc] != 1) continue;
+        const int32_t* lst = L[slot_of[fc]];
+        for (int i = 0; i < len[slot_of[fc]]; i++)
+          for (int ks = 0; ks < Q19; ks++) F[(long)lst[i] * Q19 + ks] = feq_ref(ks, 1.0, uf[fc]);
+      }
+    } else if (sub_bc == 2) {
+      /* (flag, face whose list, velocity and incoming sign are used) */
+      static const int flag_of[6] = {2, 3, 0, 1, 4, 5};  /* yp, yn, xp, xn, zp, zn flags */
+      static const int face_of[6] = {2, 3, 4, 5, 0, 1};  /* yp, yn, zp, zn, xp, xn faces */
+      for (int oi = 0; oi < 6; oi++) {
+        if (vel[flag_of[oi]] != 1) continue;
+        const int fc = face_of[oi];
+        const int axis = fc / 2, plus = (fc % 2) == 0;
+        const int32_t* lst = L[slot_of[fc]];
+        for (int i = 0; i < len[slot_of[fc]]; i++) {
+          double* Fb = &F[(long)lst[i] * Q19];
+          for (int ks = 0; ks < Q19; ks++) {
+            const int e = E19[ks][axis];
+            if (plus ? e < 0 : e > 0)
+              Fb[ks] = feq_ref(OPP19[ks], 1.0, uf[fc]) - Fb[OPP19[ks]] + feq_ref(ks, 1.0, uf[fc]);
+          }
+        }
+      }
+    } else if (sub_bc == 3) {
+      static const int order[6] = {2, 3, 0, 1, 4, 5}; /* yp, yn, xp, xn, zp, zn */
+      for (int oi = 0; oi < 6; oi++) {
+        const int fc = order[oi];
+        if (vel[fc] != 1) continue;
+        const int32_t* lst = L[slot_of[fc]];
+        for (int i = 0; i < len[slot_of[fc]]; i++) {
+          const int32_t b = lst[i];
+          const int32_t nb = nei[(long)b * Q19 + dir_in[fc]];
+          for (int ks = 0; ks < Q19; ks++)
+            if (nb > 0) F[(long)b * Q19 + ks] = feq_ref(ks, rho[nb], uf[fc]);
+        }
+      }
+    }
   }
 }
 
@@ -322,17 +513,19 @@ double orc_sp_error(int count, const double* u, const double* u0, int nx, int ny
   return t1 / (t2 + 1e-30);
 }
 
-/* `Comput_Perm` (SP3:3518-3648) at one rank, whole-box window, no pressure
- * boundary (dp = 0): Q = sum u, k_d = Q_d / V * nu / g_d, u_ave = |Q|/(V phi).
+/* `Comput_Perm` (SP3:3518-3648) at one rank, whole-box window: Q = sum u,
+ * k_d = Q_d / V * nu / (g_d + dp), u_ave = |Q|/(V phi).  dp is the pressure
+ * gradient term, 0 without pressure boundaries (in_BC = 0) and otherwise
+ * |p_+ - p_-| c_s^2 / L along perdir (SP3:3543-3556, see orc_sp_dp).
  * perm_prev holds the previous permeability (the reference's Permia); the
  * return value is the relative change along direction perdir (1..3). */
-double orc_sp_perm(int count, const double* u, int nx, int ny, int nz, double porosity, double nu,
-                   double gx, double gy, double gz, int perdir, double* perm_prev, double* uave_out) {
+double orc_sp_perm_dp(int count, const double* u, int nx, int ny, int nz, double porosity, double nu,
+                      double gx, double gy, double gz, double dp, int perdir, double* perm_prev,
+                      double* uave_out) {
   double Q[3] = {0, 0, 0};
   for (int c = 1; c <= count; c++)
     for (int d = 0; d < 3; d++) Q[d] += u[(long)c * 3 + d];
   const int V = nx * ny * nz;
-  const double dp = 0;
   double perm[3];
   perm[0] = Q[0] / V * nu / (gx + dp);
   perm[1] = Q[1] / V * nu / (gy + dp);
@@ -343,4 +536,23 @@ double orc_sp_perm(int count, const double* u, int nx, int ny, int nz, double po
   const double ax = Q[0] / (V * porosity), ay = Q[1] / (V * porosity), az = Q[2] / (V * porosity);
   if (uave_out) *uave_out = sqrt(ax * ax + ay * ay + az * az);
   return err;
+}
+
+double orc_sp_perm(int count, const double* u, int nx, int ny, int nz, double porosity, double nu,
+                   double gx, double gy, double gz, int perdir, double* perm_prev, double* uave_out) {
+  return orc_sp_perm_dp(count, u, nx, ny, nz, porosity, nu, gx, gy, gz, 0.0, perdir, perm_prev, uave_out);
+}
+
+/* dp of Comput_Perm (SP3:3543-3556) for the whole box: in_bc = 0 gives 0;
+ * else |p_+ - p_-| * c_s^2 / (extent along perdir) / dx with c_s^2 = 1/3,
+ * dx = 1; p in INPUT.dat order xp, xn, yp, yn, zp, zn. */
+double orc_sp_dp(int in_bc, int perdir, const double* p, int nx, int ny, int nz) {
+  if (in_bc == 0) return 0.0;
+  const double c_s2 = 1.0 * 1.0 / 3;
+  const double dx = 1.0;
+  switch (perdir) {
+    case 2: return fabs(p[2] - p[3]) * c_s2 / (ny - 1 - 0 + 1) / dx;
+    case 3: return fabs(p[4] - p[5]) * c_s2 / (nz - 1 - 0 + 1) / dx;
+    default: return fabs(p[0] - p[1]) * c_s2 / (nx - 1 - 0 + 1) / dx;
+  }
 }

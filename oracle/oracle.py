@@ -73,6 +73,15 @@ class Restatement:
         L.orc_sp_perm.restype = C.c_double
         L.orc_porosity.argtypes = [_U8P, C.c_int, C.c_int, C.c_int]
         L.orc_porosity.restype = C.c_double
+        L.orc_sp_step_bc.argtypes = L.orc_sp_step.argtypes + [C.c_int, _I32P, _F64P, _I32P, _F64P, _I32P, _I32P]
+        L.orc_face_list.argtypes = [_U8P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.orc_face_list.restype = C.c_int
+        L.orc_sp_perm_dp.argtypes = [C.c_int, _F64P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _F64P,
+                                     C.POINTER(C.c_double)]
+        L.orc_sp_perm_dp.restype = C.c_double
+        L.orc_sp_dp.argtypes = [C.c_int, C.c_int, _F64P, C.c_int, C.c_int, C.c_int]
+        L.orc_sp_dp.restype = C.c_double
 
     def matrices(self):
         M = np.zeros((19, 19))
@@ -105,12 +114,35 @@ class Restatement:
         nz, ny, nx = mask.shape
         return self.L.orc_porosity(np.ascontiguousarray(mask, dtype=np.uint8), nx, ny, nz)
 
+    def face_list(self, mask, face):
+        """Boundary-node ids of face 0..5 = x=0, x=nx-1, y=0, y=ny-1, z=0, z=nz-1."""
+        nz, ny, nx = mask.shape
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        n = self.L.orc_face_list(m, nx, ny, nz, face, None)
+        out = np.zeros(max(n, 1), dtype=np.int32)
+        self.L.orc_face_list(m, nx, ny, nz, face, out.ctypes.data)
+        return out[:n]
+
+
+class Boundaries:
+    """Pressure/velocity boundary settings of INPUT.dat (SP3:299-305, 318).
+    Faces in INPUT order xp, xn, yp, yn, zp, zn; pre/vel 1 = on."""
+
+    def __init__(self, sub_bc=0, in_bc=0, pre=(0,) * 6, p=(1.0,) * 6, vel=(0,) * 6, v=(0.0,) * 6):
+        self.sub_bc = int(sub_bc)
+        self.in_bc = int(in_bc)
+        self.pre = np.array(pre, dtype=np.int32)
+        self.p = np.array(p, dtype=np.float64)
+        self.vel = np.array(vel, dtype=np.int32)
+        self.v = np.array(v, dtype=np.float64)
+
 
 class SinglePhaseRun:
     """A single-phase solve driven step by step through the restatement."""
 
-    def __init__(self, mask, nu, g=(1e-6, 0.0, 0.0), u_init=(0.0, 0.0, 0.0)):
+    def __init__(self, mask, nu, g=(1e-6, 0.0, 0.0), u_init=(0.0, 0.0, 0.0), bc=None):
         self.R = Restatement()
+        self.bc = bc
         self.mask = np.ascontiguousarray(mask, dtype=np.uint8)
         self.nz, self.ny, self.nx = mask.shape
         self.coor = self.R.compact(self.mask)
@@ -131,11 +163,21 @@ class SinglePhaseRun:
         self.F = np.zeros(n * 19)
         self.perm_prev = np.zeros(3)
         self.R.L.orc_sp_init(self.count, np.array(u_init, dtype=np.float64), self.rho, self.u, self.f)
+        if bc is not None:
+            lists = [self.R.face_list(self.mask, fc) for fc in range(6)]
+            self.face_len = np.array([x.size for x in lists], dtype=np.int32)
+            self.face_ids = np.ascontiguousarray(np.concatenate(lists + [np.zeros(1, np.int32)]).astype(np.int32))
 
     def step(self, n=1):
         for _ in range(n):
-            self.R.L.orc_sp_step(self.count, self.nei, self.M, self.MI, self.S, *self.g,
-                                 self.rho, self.u, self.u0, self.f, self.F)
+            if self.bc is None:
+                self.R.L.orc_sp_step(self.count, self.nei, self.M, self.MI, self.S, *self.g,
+                                     self.rho, self.u, self.u0, self.f, self.F)
+            else:
+                b = self.bc
+                self.R.L.orc_sp_step_bc(self.count, self.nei, self.M, self.MI, self.S, *self.g,
+                                        self.rho, self.u, self.u0, self.f, self.F, b.sub_bc, b.pre, b.p, b.vel,
+                                        b.v, self.face_ids, self.face_len)
 
     def error(self):
         um = C.c_double()
@@ -146,8 +188,11 @@ class SinglePhaseRun:
 
     def perm(self, perdir=1):
         ua = C.c_double()
-        e = self.R.L.orc_sp_perm(self.count, self.u, self.nx, self.ny, self.nz, self.porosity, self.nu,
-                                 *self.g, perdir, self.perm_prev, C.byref(ua))
+        dp = 0.0
+        if self.bc is not None:
+            dp = self.R.L.orc_sp_dp(self.bc.in_bc, perdir, self.bc.p, self.nx, self.ny, self.nz)
+        e = self.R.L.orc_sp_perm_dp(self.count, self.u, self.nx, self.ny, self.nz, self.porosity, self.nu,
+                                    *self.g, dp, perdir, self.perm_prev, C.byref(ua))
         return e, self.perm_prev.copy(), ua.value
 
     def fields(self):
@@ -367,7 +412,23 @@ class ReferenceSP3:
             getattr(L, "ref_sp3_" + nm).argtypes = [_F64P]
         L.ref_sp3_get_coor.argtypes = [_I32P]
         L.ref_sp3_get_nei_loc.argtypes = [_I32P]
+        L.ref_sp3_set_boundaries.argtypes = [C.c_int, C.c_int, _I32P, _F64P, _I32P, _F64P, C.c_int]
+        L.ref_sp3_get_face_list.argtypes = [C.c_int, C.c_void_p]
+        L.ref_sp3_get_face_list.restype = C.c_int
         self.count = 0
+        self.set_boundaries(None)
+
+    def set_boundaries(self, bc, perdir=1):
+        """Boundary settings (a Boundaries, or None for the periodic path) and
+        PerDir for the next create()."""
+        b = bc if bc is not None else Boundaries()
+        self.L.ref_sp3_set_boundaries(b.sub_bc, b.in_bc, b.pre, b.p, b.vel, b.v, int(perdir))
+
+    def face_list(self, face):
+        n = self.L.ref_sp3_get_face_list(face, None)
+        out = np.zeros(max(n, 1), dtype=np.int32)
+        self.L.ref_sp3_get_face_list(face, out.ctypes.data)
+        return out[:n]
 
     def create(self, mask, nu, g=(1e-6, 0.0, 0.0), binary=True, workdir=None):
         from_path = None

@@ -2,13 +2,14 @@
 solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
 compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
 
-    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs]
+    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --bc]
 
 Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
   sp_outputs.npz  the reference program itself (oracle/_ref/ref_sp3_main)
                 run on an INPUT.dat: every file it writes  (--outputs)
   cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
+  sp_bc.npz     pressure/velocity boundaries, Sub_BC 0..3, see bc_fixture()  (--bc)
   sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
                 M^-1, f/u/rho after 20 steps, Error and Comput_Perm outputs
   sp_24.npz     24^3 spheres, 200 steps: compaction digest, u, rho, f digest,
@@ -190,8 +191,54 @@ def program_outputs():
     print("sp_outputs", sorted(a))
 
 
+def bc_cases():
+    """(name, Boundaries, g, perdir) of the boundary-condition fixture: for
+    each Sub_BC 0..3, pressure on the two x faces, pressure on all six faces
+    with a body force, velocity on all six faces, and pressure on y with
+    velocity on x+ and z-."""
+    B = oracle.Boundaries
+    out = []
+    for sb in range(4):
+        out.append((f"pre_x_{sb}", B(sub_bc=sb, in_bc=1, pre=(1, 1, 0, 0, 0, 0), p=(1.0, 1.01, 1, 1, 1, 1)),
+                    (0.0, 0.0, 0.0), 1))
+        out.append((f"pre_all_{sb}", B(sub_bc=sb, in_bc=1, pre=(1,) * 6, p=(1.0, 1.01, 1.002, 0.999, 1.003, 1.001)),
+                    (1e-5, 0.0, 0.0), 1))
+        out.append((f"vel_all_{sb}", B(sub_bc=sb, in_bc=0, vel=(1,) * 6, v=(0.01, 0.01, 0.002, -0.003, 0.001, 0.004)),
+                    (1e-5, 0.0, 0.0), 1))
+        out.append((f"mix_{sb}", B(sub_bc=sb, in_bc=1, pre=(0, 0, 1, 1, 0, 0), p=(1, 1, 1.0, 1.01, 1, 1),
+                                   vel=(1, 0, 0, 0, 0, 1), v=(0.01, 0.02, 0, 0, 0.003, 0.004)), (0.0, 0.0, 0.0), 2))
+    return out
+
+
+BC_SHAPE, BC_SEED, BC_NU, BC_STEPS = (14, 8, 10), 11, 0.1, 21
+
+
+def bc_fixture():
+    """Pressure/velocity boundaries: the reference (boundary_pressure,
+    boundary_velocity at one rank) on 14x8x10 spheres, 21 steps per case: the
+    face lists, SHA-256 of f, u, rho (rows 1..) and Comput_Perm's output."""
+    mask = G.overlapping_spheres(BC_SHAPE, 0.6, 2.5, seed=BC_SEED)
+    ref = oracle.ReferenceSP3()
+    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "nu": BC_NU, "steps": BC_STEPS}
+    for name, bc, g, perdir in bc_cases():
+        ref.set_boundaries(bc, perdir)
+        ref.create(mask, BC_NU, g)
+        if name == "pre_x_0":
+            for fc in range(6):
+                blob[f"face_{fc}"] = ref.face_list(fc)
+        ref.step(BC_STEPS)
+        f, u, rho = ref.fields()
+        e, perm, ua = ref.perm()
+        blob[name] = np.array([digest(f[1:]), digest(u[1:]), digest(rho[1:])])
+        blob[name + ":perm"] = np.array([*perm, ua])
+    ref.set_boundaries(None)
+    np.savez_compressed(os.path.join(HERE, "sp_bc.npz"), **blob)
+    print("sp_bc", len(bc_cases()), "cases")
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--bc", action="store_true")
     ap.add_argument("--cfg1", action="store_true")
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
@@ -202,6 +249,9 @@ def main():
         return
     if a.outputs:
         program_outputs()
+        return
+    if a.bc:
+        bc_fixture()
         return
     ref = oracle.ReferenceSP3()
     if a.cfg1:
