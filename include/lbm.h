@@ -75,6 +75,28 @@ typedef enum {
   LBM_ORDER_AUTO = -1      /* picked by lbm_autotune */
 } lbm_ordering;
 
+/* Pressure / velocity boundaries (INPUT.dat lines SP3:299-305, 318;
+ * boundary_pressure SP3:2656-3116, boundary_velocity SP3:2450-2655).  Faces
+ * in INPUT.dat order: xp (x = nx-1), xn (x = 0), yp, yn, zp, zn.  A face with
+ * pressure[i] == 1 or velocity[i] == 1 overwrites the post-streaming
+ * populations of its pore nodes every step, by the Sub_BC rule:
+ *   pressure 0: f_eq(rho_b, 0);  1: f_eq(rho_b, u of the inward neighbour);
+ *            2: moments of the inward neighbour with rho replaced by rho_b;
+ *            3: f_eq(rho_b, u_nb) + (f - f_eq) of the -y neighbour;
+ *   velocity 0, 1: f_eq(1, u_b);  2: non-equilibrium bounce-back of the
+ *            incoming directions (x flags act on the z faces and z flags on
+ *            the x faces, as in the reference);  3: f_eq(rho of the inward
+ *            neighbour, u_b).
+ * in_bc = 1 adds |p_+ - p_-| c_s^2 / L to the force in Comput_Perm. */
+typedef struct lbm_boundary {
+  int sub_bc;        /* Sub_BC 0..3 */
+  int in_bc;         /* in_BC */
+  int pressure[6];   /* pre_xp, pre_xn, pre_yp, pre_yn, pre_zp, pre_zn */
+  double rho[6];     /* p_xp .. p_zn: boundary density */
+  int velocity[6];   /* vel_xp .. vel_zn */
+  double vel[6];     /* v_xp .. v_zn: normal velocity of the face */
+} lbm_boundary;
+
 /* Run parameters of the single-phase solver (the physics subset of INPUT.dat,
  * SP3:283-338).  lbm_params_default() fills reference defaults. */
 typedef struct lbm_params {
@@ -88,6 +110,7 @@ typedef struct lbm_params {
   int window[6];      /* per_xn,per_xp,per_yn,per_yp,per_zn,per_zp; all -1 = whole box */
   double fp16_scale;  /* LBM_PREC_F16 storage scale; 0 = derived from nu and |g| */
   int device;         /* CUDA device ordinal */
+  lbm_boundary bc;    /* pressure/velocity boundaries; all faces off by default (fully periodic) */
 } lbm_params;
 
 /* Diagnostics of one reporting step: Error (SP3:3118-3196) and

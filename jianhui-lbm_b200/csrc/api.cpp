@@ -70,6 +70,10 @@ struct lbm_handle {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf pop[2], table, ref_of, window, rho_given, u_given, rho_prev, u_prev, partials, result;
+  // pressure/velocity faces: plan, per-step records (ping-pong like pop),
+  // operations, M^-1 for the moment rule, post-rule populations of the state
+  BcPlan bc;
+  DevBuf snap[2], bc_ops, bc_off, bc_mi, bnd_f;
   int cur = 0;
   long long step = 0;
   bool given_macro = true;  // next step / reduce takes rho, u from rho_given / u_given
@@ -146,13 +150,43 @@ void ensure_host_geometry(lbm_handle* h) {
   h->host_geo = true;
 }
 
+lbm_status upload_bc(lbm_handle* h) {
+  const BcPlan& b = h->bc;
+  if (!b.active) return LBM_OK;
+  const int n = h->geo.count;
+  const size_t nsnap = (size_t)std::max(n - b.snap_begin, 1), nbnd = (size_t)std::max(n - b.n_main, 1);
+  for (auto& sb : h->snap) {
+    if (sb.bytes != kSnapRows * nsnap * sizeof(double)) LBM_CUDA_TRY(sb.alloc(kSnapRows * nsnap * sizeof(double)));
+    LBM_CUDA_TRY(cudaMemsetAsync(sb.p, 0, sb.bytes, h->stream));
+  }
+  if (h->bnd_f.bytes != (size_t)kQ * nbnd * sizeof(double)) LBM_CUDA_TRY(h->bnd_f.alloc((size_t)kQ * nbnd * sizeof(double)));
+  LBM_CUDA_TRY(h->bc_ops.alloc(std::max<size_t>(b.ops.size(), 1) * sizeof(BcOp)));
+  LBM_CUDA_TRY(h->bc_off.alloc(b.op_off.size() * sizeof(int32_t)));
+  if (!b.ops.empty())
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_ops.p, b.ops.data(), b.ops.size() * sizeof(BcOp), cudaMemcpyHostToDevice,
+                                 h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_off.p, b.op_off.data(), b.op_off.size() * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, h->stream));
+  if (!h->bc_mi.p) {
+    LBM_CUDA_TRY(h->bc_mi.alloc(kQ * kQ * sizeof(double)));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_mi.p, &h->mrt.MI[0][0], kQ * kQ * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
+  }
+  // host copies of the plan arrays must outlive the asynchronous copies
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
 lbm_status layout(lbm_handle* h, int ordering) {
   ensure_host_geometry(h);
   order_nodes(h->mask.data(), ordering, &h->geo);
+  bc_partition(h->mask.data(), h->prm.bc, &h->geo, &h->bc);
   build_pull_table(h->mask.data(), &h->geo);
   set_window(h->prm.window, &h->geo);
   h->ordering = ordering;
-  return upload_layout(h);
+  lbm_status st = upload_layout(h);
+  if (st != LBM_OK) return st;
+  return upload_bc(h);
 }
 
 lbm_status alloc_device(lbm_handle* h) {
@@ -203,12 +237,60 @@ StepArgs step_args(lbm_handle* h, bool write) {
   a.s_v = h->mrt.s_v;
   a.s_o = h->mrt.s_o;
   a.fp16_scale = h->fp16_scale;
+  const int n = h->geo.count;
+  a.n_main = h->bc.active ? h->bc.n_main : n;
+  a.snap_begin = h->bc.active ? h->bc.snap_begin : n;
+  a.nsnap = std::max(n - a.snap_begin, 1);
+  a.snap_dst = h->bc.active ? h->snap[1 - h->cur].as<double>() : nullptr;
   return a;
+}
+
+// Arguments of the face-node kernel for a step whose step arguments are s and
+// whose source buffers have parity c.
+BcArgs bc_args(lbm_handle* h, const StepArgs& s, int c) {
+  BcArgs b{};
+  b.s = s;
+  b.snap_src = h->snap[c].as<double>();
+  b.op_off = h->bc_off.as<int32_t>();
+  b.ops = h->bc_ops.as<BcOp>();
+  b.mi = h->bc_mi.as<double>();
+  const lbm_boundary& bc = h->prm.bc;
+  for (int f = 0; f < 6; f++) {
+    b.face_rho[f] = bc.rho[f];
+    b.face_u[f][0] = b.face_u[f][1] = b.face_u[f][2] = 0.0;
+    b.face_u[f][f / 2] = bc.vel[f];
+  }
+  b.bnd_f = nullptr;
+  return b;
+}
+
+// One step: the step kernel over [0, n_main) and, with faces, the face kernel.
+cudaError_t launch_full_step(lbm_handle* h, const StepArgs& a, int c) {
+  cudaError_t e = launch_step(h->kind, a, h->block, h->stream);
+  if (e != cudaSuccess || !h->bc.active) return e;
+  return launch_boundary(h->kind, bc_args(h, a, c), h->stream);
+}
+
+// Face nodes of the current state after their rules, for reductions and
+// exports (the state itself is the post-collision populations of the last
+// step; the reference's f of face nodes is the result of the rules).
+lbm_status finalize_faces(lbm_handle* h, int* n_main, const double** bnd_f) {
+  *n_main = h->geo.count;
+  *bnd_f = nullptr;
+  if (!h->bc.active || h->given_macro) return LBM_OK;
+  StepArgs s = step_args(h, false);
+  s.rho_in = s.u_in = nullptr;
+  BcArgs b = bc_args(h, s, h->cur);
+  b.bnd_f = h->bnd_f.as<double>();
+  LBM_CUDA_TRY(launch_boundary(h->kind, b, h->stream));
+  *n_main = h->bc.n_main;
+  *bnd_f = h->bnd_f.as<double>();
+  return LBM_OK;
 }
 
 lbm_status one_step(lbm_handle* h, bool write) {
   const StepArgs a = step_args(h, write);
-  LBM_CUDA_TRY(launch_step(h->kind, a, h->block, h->stream));
+  LBM_CUDA_TRY(launch_full_step(h, a, h->cur));
   h->cur = 1 - h->cur;
   h->given_macro = false;
   h->step++;
@@ -229,7 +311,8 @@ lbm_status ensure_graph(lbm_handle* h) {
     a.src_pop = h->pop[c].p;
     a.dst_pop = h->pop[1 - c].p;
     a.rho_in = a.u_in = nullptr;
-    err = launch_step(h->kind, a, h->block, h->stream);
+    if (h->bc.active) a.snap_dst = h->snap[1 - c].as<double>();
+    err = launch_full_step(h, a, c);
     c = 1 - c;
   }
   const cudaError_t end = cudaStreamEndCapture(h->stream, &g);
@@ -308,6 +391,8 @@ lbm_status reduce_raw(lbm_handle* h, double r[8], double* rho_out_int, double* u
   a.u_out = u_out_int;
   a.partials = h->partials.as<double>();
   a.result = h->result.as<double>();
+  lbm_status st = finalize_faces(h, &a.n_main, &a.bnd_f);
+  if (st != LBM_OK) return st;
   LBM_CUDA_TRY(launch_reduce(h->kind, a, h->stream));
   LBM_CUDA_TRY(cudaMemcpyAsync(r, a.result, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -323,7 +408,17 @@ void fill_diag(lbm_handle* h, const double r[8], lbm_diag* d) {
   d->u_max = std::sqrt(r[3]);                                             // SP3:3152
   d->u_mean_speed = r[2] / ((double)g.nx * g.ny * g.nz * g.porosity);    // SP3:3183
   const double V = (double)g.window_volume;
-  const double dp = 0.0;
+  // pressure-gradient term of Comput_Perm (SP3:3543-3556): |p_+ - p_-| c_s^2 / L / dx
+  double dp = 0.0;
+  if (h->prm.bc.in_bc != 0) {
+    const int dir = (h->prm.perdir >= 1 && h->prm.perdir <= 3) ? h->prm.perdir - 1 : 0;
+    const int* w = h->prm.window;
+    const bool full = w[0] < 0 && w[1] < 0 && w[2] < 0 && w[3] < 0 && w[4] < 0 && w[5] < 0;
+    const int ext[3] = {g.nx, g.ny, g.nz};
+    const int L = full ? ext[dir] : w[2 * dir + 1] - w[2 * dir] + 1;
+    const double c_s2 = 1.0 * 1.0 / 3, dx = 1.0;
+    dp = std::fabs(h->prm.bc.rho[2 * dir] - h->prm.bc.rho[2 * dir + 1]) * c_s2 / L / dx;
+  }
   const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
   double perm[3];
   for (int i = 0; i < 3; i++) perm[i] = r[4 + i] / V * h->prm.nu / (gg[i] + dp);  // SP3:3611-3613
@@ -428,7 +523,7 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
   const int ord = p->ordering == LBM_ORDER_AUTO ? LBM_ORDER_REFERENCE : p->ordering;
   const bool full_window = p->window[0] < 0 && p->window[1] < 0 && p->window[2] < 0 && p->window[3] < 0 &&
                            p->window[4] < 0 && p->window[5] < 0;
-  const bool on_device = ord == LBM_ORDER_REFERENCE && full_window;
+  const bool on_device = ord == LBM_ORDER_REFERENCE && full_window && !bc_active(p->bc);
   if (on_device) {
     // count only; numbering and table are built on the device
     const size_t cells = (size_t)nx * ny * nz;
@@ -483,9 +578,6 @@ lbm_status lbm_create_from_input(const char* input_path, int precision, int orde
   lbm_status st = read_input_file(input_path, &in);
   if (st != LBM_OK) return st;
   if (parsed_out) *parsed_out = in;
-  if (in.in_bc != 0 || in.pre_xp || in.pre_xn || in.pre_yp || in.pre_yn || in.pre_zp || in.pre_zn || in.vel_xp ||
-      in.vel_xn || in.vel_yp || in.vel_yn || in.vel_zp || in.vel_zn)
-    return fail(LBM_ERR_ARG, "pressure/velocity boundaries are not supported (fully periodic solver)");
   if (in.nnf_module != 0) return fail(LBM_ERR_ARG, "non-Newtonian module is not supported");
   if (in.lattice_v != 0) return fail(LBM_ERR_ARG, "self-defined lattice velocity is not supported");
   std::vector<uint8_t> mask((size_t)in.nx * in.ny * in.nz);
@@ -504,6 +596,19 @@ lbm_status lbm_create_from_input(const char* input_path, int precision, int orde
   p.precision = precision;
   p.ordering = ordering;
   p.perdir = in.perdir;
+  // pressure / velocity faces (SP3:299-305, 318), INPUT.dat order xp, xn, yp, yn, zp, zn
+  p.bc.sub_bc = in.sub_bc;
+  p.bc.in_bc = in.in_bc;
+  const int pre[6] = {in.pre_xp, in.pre_xn, in.pre_yp, in.pre_yn, in.pre_zp, in.pre_zn};
+  const double prho[6] = {in.p_xp, in.p_xn, in.p_yp, in.p_yn, in.p_zp, in.p_zn};
+  const int vel[6] = {in.vel_xp, in.vel_xn, in.vel_yp, in.vel_yn, in.vel_zp, in.vel_zn};
+  const double vv[6] = {in.v_xp, in.v_xn, in.v_yp, in.v_yn, in.v_zp, in.v_zn};
+  for (int f = 0; f < 6; f++) {
+    p.bc.pressure[f] = pre[f];
+    p.bc.rho[f] = prho[f];
+    p.bc.velocity[f] = vel[f];
+    p.bc.vel[f] = vv[f];
+  }
   if (in.par_per_x || in.par_per_y || in.par_per_z) {
     // SP3:1005-1010: an axis without a partial window spans the whole box
     p.window[0] = in.par_per_x ? in.per_xn : 0;
@@ -607,8 +712,11 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f) {
   DevBuf out;
   LBM_CUDA_TRY(out.alloc((size_t)(n + 1) * kQ * sizeof(double)));
   LBM_CUDA_TRY(cudaMemsetAsync(out.p, 0, out.bytes, h->stream));
+  int n_main;
+  const double* bnd_f;
+  if ((st = finalize_faces(h, &n_main, &bnd_f)) != LBM_OK) return st;
   LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
-                                 h->geo.npad, h->fp16_scale, out.as<double>(), h->stream));
+                                 h->geo.npad, h->fp16_scale, out.as<double>(), h->stream, n_main, bnd_f));
   LBM_CUDA_TRY(cudaMemcpyAsync(f, out.p, out.bytes, cudaMemcpyDeviceToHost, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return LBM_OK;
@@ -669,7 +777,8 @@ lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu)
   if (device_bytes) {
     size_t b = 0;
     for (const DevBuf* d : {&h->pop[0], &h->pop[1], &h->table, &h->ref_of, &h->window, &h->rho_given, &h->u_given,
-                            &h->rho_prev, &h->u_prev, &h->partials, &h->result})
+                            &h->rho_prev, &h->u_prev, &h->partials, &h->result, &h->snap[0], &h->snap[1],
+                            &h->bc_ops, &h->bc_off, &h->bc_mi, &h->bnd_f})
       b += d->bytes;
     *device_bytes = b;
   }
@@ -688,12 +797,20 @@ lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* 
   LBM_CUDA_TRY(rsave.alloc((size_t)h->geo.npad * sizeof(double)));
   LBM_CUDA_TRY(usave.alloc((size_t)3 * h->geo.npad * sizeof(double)));
   LBM_CUDA_TRY(cudaMemsetAsync(fsave.p, 0, fsave.bytes, h->stream));
-  LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
-                                 h->geo.npad, h->fp16_scale, fsave.as<double>(), h->stream));
+  {
+    int n_main;
+    const double* bnd_f;
+    if ((st = finalize_faces(h, &n_main, &bnd_f)) != LBM_OK) return st;
+    LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
+                                   h->geo.npad, h->fp16_scale, fsave.as<double>(), h->stream, n_main, bnd_f));
+  }
   DevBuf rref, uref;
   LBM_CUDA_TRY(rref.alloc((size_t)(n + 1) * sizeof(double)));
   LBM_CUDA_TRY(uref.alloc((size_t)(n + 1) * 3 * sizeof(double)));
-  const bool given = h->given_macro;
+  // With pressure/velocity faces the restored state restarts as a given one
+  // (populations after the face rules plus their macro fields): the per-step
+  // records the next step's rules read are overwritten by the trial steps.
+  const bool given = h->given_macro || h->bc.active;
   if (given) {
     // the given macro fields are part of the state: round-trip them too
     double r[8];

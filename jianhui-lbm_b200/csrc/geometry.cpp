@@ -196,6 +196,165 @@ void fill_pool_rows(const uint8_t* mask, const Geometry& g, int64_t cap, int beg
   }
 }
 
+bool bc_active(const lbm_boundary& bc) {
+  for (int s = 0; s < 6; s++)
+    if (bc.pressure[s] == 1 || bc.velocity[s] == 1) return true;
+  return false;
+}
+
+// The boundary program of one step, as boundary_pressure (SP3:2656-3116) and
+// boundary_velocity (SP3:2450-2655) run it at one rank, flattened into
+// per-node operation lists.  Face lists are the reference's (SP3:1164-1222):
+// x faces k outer / j inner, y faces k outer / i inner, z faces j outer /
+// i inner.  Kept as the reference has them:
+//   - pressure Sub_BC 1, inward neighbour solid: the rest equilibrium of this
+//     face's density goes to the i-th node of the y = ny-1 list (an index
+//     past that list is outside the reference's array; it is dropped);
+//   - pressure Sub_BC 3 takes f - f_eq from the -y neighbour on every face;
+//   - velocity Sub_BC 2: x flags act on the z faces, z flags on the x faces.
+void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPlan* plan) {
+  *plan = BcPlan{};
+  const int n = g->count;
+  if (!bc_active(bc) || n == 0) {
+    plan->n_main = plan->snap_begin = n;
+    return;
+  }
+  plan->active = true;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  std::vector<int32_t> rid((size_t)nx * ny * nz, 0);  // x-fastest cell -> reference id, 0 = solid
+  for (int id = 1; id <= n; id++) {
+    int i, j, k;
+    cell_of(*g, id, &i, &j, &k);
+    rid[i + (size_t)nx * (j + (size_t)ny * k)] = id;
+  }
+  auto at = [&](int i, int j, int k) { return rid[i + (size_t)nx * (j + (size_t)ny * k)]; };
+  // lists in slot order xn, xp, yn, yp, zn, zp
+  std::vector<int32_t> list[6];
+  for (int a = 0; a < nz; a++)
+    for (int b = 0; b < ny; b++) {
+      if (int32_t c = at(0, b, a)) list[0].push_back(c);
+      if (int32_t c = at(nx - 1, b, a)) list[1].push_back(c);
+    }
+  for (int a = 0; a < nz; a++)
+    for (int b = 0; b < nx; b++) {
+      if (int32_t c = at(b, 0, a)) list[2].push_back(c);
+      if (int32_t c = at(b, ny - 1, a)) list[3].push_back(c);
+    }
+  for (int a = 0; a < ny; a++)
+    for (int b = 0; b < nx; b++) {
+      if (int32_t c = at(b, a, 0)) list[4].push_back(c);
+      if (int32_t c = at(b, a, nz - 1)) list[5].push_back(c);
+    }
+  // push neighbour id along direction q with periodic wrap (nei_loc), 0 if solid
+  auto nei = [&](int32_t id, int q) {
+    int i, j, k;
+    cell_of(*g, id, &i, &j, &k);
+    int ip = i + cx(q), jp = j + cy(q), kp = k + cz(q);
+    ip = ip < 0 ? nx - 1 : (ip >= nx ? 0 : ip);
+    jp = jp < 0 ? ny - 1 : (jp >= ny ? 0 : jp);
+    kp = kp < 0 ? nz - 1 : (kp >= nz ? 0 : kp);
+    return at(ip, jp, kp);
+  };
+  // INPUT face index (xp, xn, yp, yn, zp, zn) -> list slot, inward push direction
+  static const int slot_of[6] = {1, 0, 3, 2, 5, 4};
+  static const int dir_in[6] = {2, 1, 4, 3, 6, 5};
+  struct Raw {
+    int32_t target;
+    BcOp op;  // nb / nb4 as reference ids here
+  };
+  std::vector<Raw> prog;
+  auto emit = [&](int32_t target, int8_t kind, int face, int32_t nb, int32_t nb4, int axis = 0, int sign = 0) {
+    prog.push_back(Raw{target, BcOp{kind, (int8_t)face, (int8_t)axis, (int8_t)sign, nb, nb4}});
+  };
+  bool any_pre = false, any_vel = false;
+  for (int s = 0; s < 6; s++) {
+    any_pre |= bc.pressure[s] == 1;
+    any_vel |= bc.velocity[s] == 1;
+  }
+  const int sb = bc.sub_bc;
+  if (any_pre && sb >= 0 && sb <= 3) {
+    static const int order[6] = {2, 3, 0, 1, 4, 5};  // yp, yn, xp, xn, zp, zn
+    for (int fc : order) {
+      if (bc.pressure[fc] != 1) continue;
+      const std::vector<int32_t>& L = list[slot_of[fc]];
+      for (size_t i = 0; i < L.size(); i++) {
+        const int32_t b = L[i], nb = nei(b, dir_in[fc]);
+        if (sb == 0) {
+          emit(b, kBcPressureRest, fc, 0, 0);
+        } else if (nb == 0) {
+          if (sb != 1)
+            emit(b, kBcPressureRest, fc, 0, 0);
+          else if (i < list[3].size())
+            emit(list[3][i], kBcPressureRest, fc, 0, 0);
+        } else if (sb == 1) {
+          emit(b, kBcPressureNbU, fc, nb, 0);
+        } else if (sb == 2) {
+          emit(b, kBcPressureMoment, fc, nb, 0);
+        } else {
+          emit(b, kBcPressureNeq, fc, nb, nei(b, 4));
+        }
+      }
+    }
+  }
+  if (any_vel) {
+    if (sb == 0 || sb == 1) {
+      static const int order[6] = {3, 2, 5, 4, 1, 0};  // yn, yp, zn, zp, xn, xp
+      for (int fc : order)
+        if (bc.velocity[fc] == 1)
+          for (int32_t b : list[slot_of[fc]]) emit(b, kBcVelocityEq, fc, 0, 0);
+    } else if (sb == 2) {
+      static const int flag_of[6] = {2, 3, 0, 1, 4, 5};  // yp, yn, xp, xn, zp, zn flags
+      static const int face_of[6] = {2, 3, 4, 5, 0, 1};  // ... drive yp, yn, zp, zn, xp, xn
+      for (int oi = 0; oi < 6; oi++) {
+        if (bc.velocity[flag_of[oi]] != 1) continue;
+        const int fc = face_of[oi];
+        for (int32_t b : list[slot_of[fc]]) emit(b, kBcVelocityNeq, fc, 0, 0, fc / 2, fc % 2 == 0 ? 1 : -1);
+      }
+    } else if (sb == 3) {
+      static const int order[6] = {2, 3, 0, 1, 4, 5};  // yp, yn, xp, xn, zp, zn
+      for (int fc : order)
+        if (bc.velocity[fc] == 1)
+          for (int32_t b : list[slot_of[fc]]) {
+            const int32_t nb = nei(b, dir_in[fc]);
+            if (nb != 0) emit(b, kBcVelocityNbRho, fc, nb, 0);
+          }
+    }
+  }
+  // classes: 2 = written, 1 = read, 0 = neither
+  std::vector<uint8_t> cls((size_t)n + 1, 0);
+  for (const Raw& r : prog) cls[r.target] = 2;
+  for (const Raw& r : prog) {
+    if (r.op.nb > 0 && cls[r.op.nb] == 0) cls[r.op.nb] = 1;
+    if (r.op.nb4 > 0 && cls[r.op.nb4] == 0) cls[r.op.nb4] = 1;
+  }
+  std::vector<int32_t> order;
+  order.reserve(n);
+  for (int c = 0; c < 3; c++)
+    for (int p = 0; p < n; p++)
+      if (cls[g->ref_of[p]] == c) order.push_back(g->ref_of[p]);
+  int n0 = 0, n1 = 0;
+  for (int id = 1; id <= n; id++) (cls[id] == 0 ? n0 : (cls[id] == 1 ? n1 : plan->n_main)) += 1;
+  const int n2 = plan->n_main;
+  plan->snap_begin = n0;
+  plan->n_main = n0 + n1;
+  g->ref_of = order;
+  for (int p = 0; p < n; p++) g->int_of[g->ref_of[p]] = p;
+  // per boundary node, its operations in program order
+  const int nb_nodes = n2;
+  plan->op_off.assign((size_t)nb_nodes + 1, 0);
+  for (const Raw& r : prog) plan->op_off[g->int_of[r.target] - plan->n_main + 1]++;
+  for (int i = 0; i < nb_nodes; i++) plan->op_off[i + 1] += plan->op_off[i];
+  plan->ops.resize(prog.size());
+  std::vector<int32_t> fill(plan->op_off.begin(), plan->op_off.end() - 1);
+  auto slot = [&](int32_t id) { return id > 0 ? g->int_of[id] - plan->snap_begin : -1; };
+  for (const Raw& r : prog) {
+    BcOp op = r.op;
+    op.nb = slot(r.op.nb);
+    op.nb4 = slot(r.op.nb4);
+    plan->ops[fill[g->int_of[r.target] - plan->n_main]++] = op;
+  }
+}
+
 // Permeability window (per_xn..per_zp, SP3:1005-1020, 3581-3590).
 void set_window(const int w[6], Geometry* g) {
   const bool full = (w[0] < 0 && w[1] < 0 && w[2] < 0 && w[3] < 0 && w[4] < 0 && w[5] < 0);

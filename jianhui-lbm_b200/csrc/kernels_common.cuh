@@ -317,9 +317,17 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(ReduceArgs a) {
       uz = u[2 * a.npad + p];
     } else {
       A f[kQ];
-      f[0] = load_pop<K>(pop + p, inv_scale);
+      if (a.bnd_f != nullptr && p >= a.n_main) {
+        // face node: populations after this state's boundary rules
+        const size_t nb = (size_t)(a.n - a.n_main), b = (size_t)(p - a.n_main);
 #pragma unroll
-      for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(pop + __ldg(a.table + (size_t)(q - 1) * a.npad + p), inv_scale);
+        for (int q = 0; q < kQ; q++) f[q] = from_full<K>(a.bnd_f[(size_t)q * nb + b], q);
+      } else {
+        f[0] = load_pop<K>(pop + p, inv_scale);
+#pragma unroll
+        for (int q = 1; q < kQ; q++)
+          f[q] = load_pop<K>(pop + __ldg(a.table + (size_t)(q - 1) * a.npad + p), inv_scale);
+      }
       if constexpr (K == Store::F64) {
         macro_faithful(f, a.gx / 2, a.gy / 2, a.gz / 2, rho, ux, uy, uz);
       } else {
@@ -364,13 +372,20 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(ReduceArgs a) {
 }
 
 // Reference-layout export: out[ref_of[p]*19 + q] = f_q(p) (post-streaming, full f).
+// Face nodes [n_main, n) take their populations from bnd_f when it is set.
 template <Store K>
 __global__ void export_pop_kernel(const typename Traits<K>::T* __restrict__ pop, const int32_t* __restrict__ table,
                                   const int32_t* __restrict__ ref_of, int n, int npad, float inv_scale,
-                                  double* __restrict__ out) {
+                                  double* __restrict__ out, int n_main, const double* __restrict__ bnd_f) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   double* row = out + (size_t)ref_of[p] * kQ;
+  if (bnd_f != nullptr && p >= n_main) {
+    const size_t nb = (size_t)(n - n_main), b = (size_t)(p - n_main);
+#pragma unroll
+    for (int q = 0; q < kQ; q++) row[q] = bnd_f[(size_t)q * nb + b];
+    return;
+  }
   row[0] = to_full<K>(load_pop<K>(pop + p, inv_scale), 0);
 #pragma unroll
   for (int q = 1; q < kQ; q++)
@@ -414,10 +429,12 @@ cudaError_t reduce_dispatch(const ReduceArgs& a, cudaStream_t st) {
 
 template <Store K>
 cudaError_t export_dispatch(const void* pop, const int32_t* table, const int32_t* ref_of, int n, int npad,
-                            double fp16_scale, double* out, cudaStream_t st) {
+                            double fp16_scale, double* out, cudaStream_t st, int n_main = 0,
+                            const double* bnd_f = nullptr) {
   if (n == 0) return cudaSuccess;
   export_pop_kernel<K><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const typename Traits<K>::T*>(pop), table,
-                                                        ref_of, n, npad, (float)(1.0 / fp16_scale), out);
+                                                        ref_of, n, npad, (float)(1.0 / fp16_scale), out, n_main,
+                                                        bnd_f);
   return cudaGetLastError();
 }
 

@@ -113,6 +113,46 @@ void build_pull_table(const uint8_t* mask, Geometry* g);
 void pull_to_push(const Geometry& g, int32_t* nei_loc);
 void set_window(const int window[6], Geometry* g);
 
+// ------------------------------------------------- pressure/velocity faces
+// One boundary operation on the post-streaming populations F of a face node,
+// in the reference's program order (boundary_pressure then
+// boundary_velocity).  nb / nb4 are snapshot slots (internal index -
+// snap_begin) of the nodes whose previous-step state the rule reads, -1 for
+// none (the reference's row 0, zero).
+enum BcKind : int8_t {
+  kBcPressureRest = 0,    // F = f_eq(rho_b, 0)
+  kBcPressureNbU = 1,     // F = f_eq(rho_b, u[nb])
+  kBcPressureMoment = 2,  // F = MI (M f[nb] with m_0 = rho_b)
+  kBcPressureNeq = 3,     // F = f_eq(rho_b, u[nb]) + f[nb4] - f_eq(rho[nb], u[nb])
+  kBcVelocityEq = 4,      // F = f_eq(1, u_b)
+  kBcVelocityNeq = 5,     // incoming q: F_q = f_eq(opp q; 1, u_b) - F_opp q + f_eq(q; 1, u_b)
+  kBcVelocityNbRho = 6,   // F = f_eq(rho[nb], u_b)
+};
+struct BcOp {
+  int8_t kind;
+  int8_t face;  // INPUT.dat face index 0..5 = xp, xn, yp, yn, zp, zn (density / velocity of the rule)
+  int8_t axis;  // kBcVelocityNeq: axis of the incoming test
+  int8_t sign;  // kBcVelocityNeq: +1 -> q with e_axis < 0 are incoming, -1 -> e_axis > 0
+  int32_t nb;
+  int32_t nb4;
+};
+// Node classes after bc_partition, in internal order:
+//   [0, snap_begin)          interior nodes (no boundary involvement)
+//   [snap_begin, n_main)     nodes whose state a boundary rule reads
+//   [n_main, count)          nodes a boundary rule writes (face nodes)
+// The main step kernel runs over [0, n_main) and records the post-streaming
+// state of [snap_begin, n_main); the boundary kernel runs over [n_main, count).
+struct BcPlan {
+  bool active = false;
+  int n_main = 0, snap_begin = 0;
+  std::vector<int32_t> op_off;  // [count - n_main + 1] CSR over boundary nodes
+  std::vector<BcOp> ops;
+};
+bool bc_active(const lbm_boundary& bc);
+// Reorders g (ref_of / int_of) into the three classes, keeping the order
+// within each class, and builds the per-node operation lists.
+void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPlan* plan);
+
 // Mask and box of a single-phase handle (for solvers coupled to it).
 const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz);
 
@@ -148,8 +188,33 @@ struct StepArgs {
   double gx, gy, gz;
   double s_v, s_o;
   double fp16_scale;
+  // pressure/velocity faces: nodes [n_main, n) are left to the boundary
+  // kernel; nodes [snap_begin, n_main) record their post-streaming state in
+  // snap_dst ([23][nsnap] doubles: f_0..f_18, rho, ux, uy, uz; slot = p -
+  // snap_begin).  Without faces n_main = n and snap_dst = null.
+  int n_main;
+  int snap_begin;
+  int nsnap;
+  double* snap_dst;
 };
 cudaError_t launch_step(Store kind, const StepArgs& a, int block, cudaStream_t st);
+
+constexpr int kSnapRows = kQ + 4;  // per-step record of a node: f_0..f_18, rho, ux, uy, uz
+
+// Boundary kernel: the face nodes [n_main, n) of one step (pull, rules, macro,
+// record, collide) or, with bnd_f set, only the post-rule populations of the
+// current state ([19][n - n_main] doubles) for reductions and exports.
+struct BcArgs {
+  StepArgs s;               // pops, table, macro in/out, rates, n_main, snap_begin, nsnap, snap_dst
+  const double* snap_src;   // the previous step's record
+  const int32_t* op_off;
+  const BcOp* ops;
+  const double* mi;         // [19*19] M^-1 (kBcPressureMoment)
+  double face_rho[6];
+  double face_u[6][3];
+  double* bnd_f;            // finalize mode output, or null
+};
+cudaError_t launch_boundary(Store kind, const BcArgs& a, cudaStream_t st);
 
 struct ReduceArgs {
   const void* pop;        // [19][npad] post-collision of the last step
@@ -166,6 +231,8 @@ struct ReduceArgs {
   double* u_out;          // optional double[3][npad]
   double* partials;       // [blocks][8]
   double* result;         // [8]
+  int n_main;             // nodes [n_main, n) read their populations from bnd_f
+  const double* bnd_f;    // [19][n - n_main] post-rule populations, or null
 };
 // result: t1, t2, t3, umax2, Qx, Qy, Qz, mass
 cudaError_t launch_reduce(Store kind, const ReduceArgs& a, cudaStream_t st);
@@ -173,7 +240,8 @@ int reduce_blocks(int n);
 
 // f[(count+1)*19] reference AoS <-> device storage
 cudaError_t launch_export_pop(Store kind, const void* pop, const int32_t* table, const int32_t* ref_of,
-                              int n, int npad, double fp16_scale, double* out, cudaStream_t st);
+                              int n, int npad, double fp16_scale, double* out, cudaStream_t st,
+                              int n_main = 0, const double* bnd_f = nullptr);
 cudaError_t launch_import_pop(Store kind, void* pop, const int32_t* table, const int32_t* ref_of, int n,
                               int npad, double fp16_scale, const double* in, cudaStream_t st);
 // rho/u reference-layout doubles -> device macro arrays of the storage's type

@@ -12,7 +12,7 @@
 // entries of MI are applied, so its round-off entries count as they do in the
 // reference.  Streaming is a pull through the table instead of the
 // reference's push through nei_loc, which moves values without arithmetic.
-#include "kernels_common.cuh"
+#include "bc_kernels.cuh"
 
 namespace lbm {
 
@@ -28,36 +28,11 @@ __device__ __forceinline__ double srate(int k, double sv, double so) {
   return conserved ? 0.0 : (viscous ? sv : so);
 }
 
-template <int BS, bool GIVEN, bool WRITE>
-__global__ void __launch_bounds__(BS) step_f64_faithful(StepArgs a) {
-  const int p = blockIdx.x * BS + threadIdx.x;
-  if (p >= a.n) return;
-  const double* __restrict__ src = static_cast<const double*>(a.src_pop);
+// Collision of one node in the reference's operation order; writes the 19
+// post-collision populations of node p.
+__device__ __forceinline__ void collide_faithful(const double (&f)[kQ], double rho, double ux, double uy, double uz,
+                                                 const StepArgs& a, int p) {
   double* __restrict__ dst = static_cast<double*>(a.dst_pop);
-  double f[kQ];
-  f[0] = __ldg(src + p);
-#pragma unroll
-  for (int q = 1; q < kQ; q++) f[q] = __ldg(src + __ldg(a.table + (size_t)(q - 1) * a.npad + p));
-
-  double rho, ux, uy, uz;
-  if (GIVEN) {
-    const double* r = static_cast<const double*>(a.rho_in);
-    const double* u = static_cast<const double*>(a.u_in);
-    rho = r[p];
-    ux = u[p];
-    uy = u[a.npad + p];
-    uz = u[2 * a.npad + p];
-  } else {
-    macro_faithful(f, a.gx / 2, a.gy / 2, a.gz / 2, rho, ux, uy, uz);
-  }
-  if (WRITE) {
-    static_cast<double*>(a.rho_out)[p] = rho;
-    double* u = static_cast<double*>(a.u_out);
-    u[p] = ux;
-    u[a.npad + p] = uy;
-    u[2 * a.npad + p] = uz;
-  }
-
   const double c_s2 = 1.0 * 1.0 / 3;
   const double gx = a.gx, gy = a.gy, gz = a.gz;
   double guo[kQ], feq[kQ];
@@ -104,6 +79,82 @@ __global__ void __launch_bounds__(BS) step_f64_faithful(StepArgs a) {
   }
 }
 
+__device__ __forceinline__ void pull_f64(const StepArgs& a, int p, double (&f)[kQ]) {
+  const double* __restrict__ src = static_cast<const double*>(a.src_pop);
+  f[0] = __ldg(src + p);
+#pragma unroll
+  for (int q = 1; q < kQ; q++) f[q] = __ldg(src + __ldg(a.table + (size_t)(q - 1) * a.npad + p));
+}
+
+__device__ __forceinline__ void macro_in_out(const StepArgs& a, int p, bool given, bool write, const double (&f)[kQ],
+                                             double& rho, double& ux, double& uy, double& uz) {
+  if (given) {
+    const double* r = static_cast<const double*>(a.rho_in);
+    const double* u = static_cast<const double*>(a.u_in);
+    rho = r[p];
+    ux = u[p];
+    uy = u[a.npad + p];
+    uz = u[2 * a.npad + p];
+  } else {
+    macro_faithful(f, a.gx / 2, a.gy / 2, a.gz / 2, rho, ux, uy, uz);
+  }
+  if (write) {
+    static_cast<double*>(a.rho_out)[p] = rho;
+    double* u = static_cast<double*>(a.u_out);
+    u[p] = ux;
+    u[a.npad + p] = uy;
+    u[2 * a.npad + p] = uz;
+  }
+}
+
+template <int BS, bool GIVEN, bool WRITE>
+__global__ void __launch_bounds__(BS) step_f64_faithful(StepArgs a) {
+  const int p = blockIdx.x * BS + threadIdx.x;
+  if (p >= a.n_main) return;
+  double f[kQ];
+  pull_f64(a, p, f);
+  double rho, ux, uy, uz;
+  macro_in_out(a, p, GIVEN, WRITE, f, rho, ux, uy, uz);
+  if (a.snap_dst != nullptr && p >= a.snap_begin) snap_write(a.snap_dst, a.nsnap, p - a.snap_begin, f, rho, ux, uy, uz);
+  collide_faithful(f, rho, ux, uy, uz, a, p);
+}
+
+// Face nodes: pull, the boundary rules, macro step, record, collision.  With
+// a.bnd_f set: only the populations after the rules (current state).
+template <bool GIVEN, bool FINAL>
+__global__ void __launch_bounds__(128) bc_f64_faithful(BcArgs a) {
+  const int b = blockIdx.x * 128 + threadIdx.x;
+  const int p = a.s.n_main + b;
+  if (p >= a.s.n) return;
+  double f[kQ];
+  pull_f64(a.s, p, f);
+  if (!GIVEN) bc_apply(a, b, f);
+  if (FINAL) {
+    const size_t nb = (size_t)(a.s.n - a.s.n_main);
+#pragma unroll
+    for (int q = 0; q < kQ; q++) a.bnd_f[(size_t)q * nb + b] = f[q];
+    return;
+  }
+  double rho, ux, uy, uz;
+  macro_in_out(a.s, p, GIVEN, a.s.rho_out != nullptr, f, rho, ux, uy, uz);
+  snap_write(a.s.snap_dst, a.s.nsnap, p - a.s.snap_begin, f, rho, ux, uy, uz);
+  collide_faithful(f, rho, ux, uy, uz, a.s, p);
+}
+
+cudaError_t launch_boundary_f64(const BcArgs& a, cudaStream_t st) {
+  const int nb = a.s.n - a.s.n_main;
+  if (nb <= 0) return cudaSuccess;
+  const int grid = (nb + 127) / 128;
+  const bool given = a.s.rho_in != nullptr;
+  if (a.bnd_f)
+    bc_f64_faithful<false, true><<<grid, 128, 0, st>>>(a);
+  else if (given)
+    bc_f64_faithful<true, false><<<grid, 128, 0, st>>>(a);
+  else
+    bc_f64_faithful<false, false><<<grid, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 // final pass of the diagnostics reduction (shared by all kinds)
 __global__ void reduce_final_kernel(const double* __restrict__ partials, int nblocks, double* __restrict__ result) {
   __shared__ double smem[8 * 32];
@@ -116,7 +167,7 @@ __global__ void reduce_final_kernel(const double* __restrict__ partials, int nbl
 
 template <int BS>
 static cudaError_t launch_f64_bs(const StepArgs& a, cudaStream_t st) {
-  const int grid = (a.n + BS - 1) / BS;
+  const int grid = (a.n_main + BS - 1) / BS;
   if (grid == 0) return cudaSuccess;
   const bool given = a.rho_in != nullptr, write = a.rho_out != nullptr;
   if (given && write)
@@ -141,8 +192,8 @@ cudaError_t launch_step_f64(const StepArgs& a, int block, cudaStream_t st) {
 
 cudaError_t reduce_f64(const ReduceArgs& a, cudaStream_t st) { return reduce_dispatch<Store::F64>(a, st); }
 cudaError_t export_f64(const void* pop, const int32_t* table, const int32_t* ref_of, int n, int npad, double* out,
-                       cudaStream_t st) {
-  return export_dispatch<Store::F64>(pop, table, ref_of, n, npad, 1.0, out, st);
+                       cudaStream_t st, int n_main, const double* bnd_f) {
+  return export_dispatch<Store::F64>(pop, table, ref_of, n, npad, 1.0, out, st, n_main, bnd_f);
 }
 cudaError_t import_f64(void* pop, const int32_t* table, const int32_t* ref_of, int n, int npad, const double* in,
                        cudaStream_t st) {

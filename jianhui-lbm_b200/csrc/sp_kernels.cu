@@ -6,13 +6,15 @@
 //   through the table; neighbours are close in the node order), 19
 //   post-collision populations (coalesced stores)
 // = 2*19*s + 18*4 bytes, s = bytes per stored population.
-#include "kernels_common.cuh"
+#include "bc_kernels.cuh"
 
 namespace lbm {
 
 cudaError_t launch_step_f64(const StepArgs& a, int block, cudaStream_t st);
 cudaError_t reduce_f64(const ReduceArgs& a, cudaStream_t st);
-cudaError_t export_f64(const void*, const int32_t*, const int32_t*, int, int, double*, cudaStream_t);
+cudaError_t export_f64(const void*, const int32_t*, const int32_t*, int, int, double*, cudaStream_t, int,
+                       const double*);
+cudaError_t launch_boundary_f64(const BcArgs& a, cudaStream_t st);
 cudaError_t import_f64(void*, const int32_t*, const int32_t*, int, int, const double*, cudaStream_t);
 cudaError_t import_macro_f64(void*, void*, const int32_t*, int, int, const double*, const double*, cudaStream_t);
 
@@ -22,7 +24,7 @@ __global__ void __launch_bounds__(BS) step_dev_kernel(StepArgs a) {
   using A = typename Traits<K>::A;
   using Mac = typename Traits<K>::Mac;
   const int p = blockIdx.x * BS + threadIdx.x;
-  if (p >= a.n) return;
+  if (p >= a.n_main) return;
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
   const float scale = (float)a.fp16_scale;
@@ -54,14 +56,101 @@ __global__ void __launch_bounds__(BS) step_dev_kernel(StepArgs a) {
     u[a.npad + p] = (Mac)uy;
     u[2 * a.npad + p] = (Mac)uz;
   }
+  if (a.snap_dst != nullptr && p >= a.snap_begin) {
+    double full[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; q++) full[q] = to_full<K>(f[q], q);
+    snap_write(a.snap_dst, a.nsnap, p - a.snap_begin, full, rho, ux, uy, uz);
+  }
   mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(a.gx), A(a.gy), A(a.gz), A(a.s_v), A(a.s_o));
 #pragma unroll
   for (int q = 0; q < kQ; q++) store_pop<K>(dst + (size_t)q * a.npad + p, f[q], scale);
 }
 
+// Face nodes in deviation storage: the rules act on full populations in
+// double, the macro step and collision are the step kernel's.
+template <Store K, bool GIVEN, bool FINAL>
+__global__ void __launch_bounds__(128) bc_dev_kernel(BcArgs a) {
+  using T = typename Traits<K>::T;
+  using A = typename Traits<K>::A;
+  using Mac = typename Traits<K>::Mac;
+  const int b = blockIdx.x * 128 + threadIdx.x;
+  const int p = a.s.n_main + b;
+  if (p >= a.s.n) return;
+  const StepArgs& s = a.s;
+  const T* __restrict__ src = static_cast<const T*>(s.src_pop);
+  const float scale = (float)s.fp16_scale;
+  const float inv_scale = (float)(1.0 / s.fp16_scale);
+  double F[kQ];
+  F[0] = to_full<K>(load_pop<K>(src + p, inv_scale), 0);
+#pragma unroll
+  for (int q = 1; q < kQ; q++)
+    F[q] = to_full<K>(load_pop<K>(src + __ldg(s.table + (size_t)(q - 1) * s.npad + p), inv_scale), q);
+  if (!GIVEN) bc_apply(a, b, F);
+  if (FINAL) {
+    const size_t nb = (size_t)(s.n - s.n_main);
+#pragma unroll
+    for (int q = 0; q < kQ; q++) a.bnd_f[(size_t)q * nb + b] = F[q];
+    return;
+  }
+  A f[kQ];
+#pragma unroll
+  for (int q = 0; q < kQ; q++) f[q] = from_full<K>(F[q], q);
+  PairSplit<A> ps;
+  split_pairs(f, ps);
+  A drho, rho, ux, uy, uz;
+  if (GIVEN) {
+    const Mac* r = static_cast<const Mac*>(s.rho_in);
+    const Mac* u = static_cast<const Mac*>(s.u_in);
+    rho = (A)r[p];
+    drho = rho - A(1);
+    ux = (A)u[p];
+    uy = (A)u[s.npad + p];
+    uz = (A)u[2 * s.npad + p];
+  } else {
+    macro_dev<A>(f, ps, A(0.5 * s.gx), A(0.5 * s.gy), A(0.5 * s.gz), drho, rho, ux, uy, uz);
+  }
+  if (s.rho_out != nullptr) {
+    static_cast<Mac*>(s.rho_out)[p] = (Mac)rho;
+    Mac* u = static_cast<Mac*>(s.u_out);
+    u[p] = (Mac)ux;
+    u[s.npad + p] = (Mac)uy;
+    u[2 * s.npad + p] = (Mac)uz;
+  }
+  snap_write(s.snap_dst, s.nsnap, p - s.snap_begin, F, rho, ux, uy, uz);
+  mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(s.gx), A(s.gy), A(s.gz), A(s.s_v), A(s.s_o));
+  T* __restrict__ dst = static_cast<T*>(s.dst_pop);
+#pragma unroll
+  for (int q = 0; q < kQ; q++) store_pop<K>(dst + (size_t)q * s.npad + p, f[q], scale);
+}
+
+template <Store K>
+static cudaError_t launch_bc_dev(const BcArgs& a, cudaStream_t st) {
+  const int nb = a.s.n - a.s.n_main;
+  if (nb <= 0) return cudaSuccess;
+  const int grid = (nb + 127) / 128;
+  if (a.bnd_f)
+    bc_dev_kernel<K, false, true><<<grid, 128, 0, st>>>(a);
+  else if (a.s.rho_in != nullptr)
+    bc_dev_kernel<K, true, false><<<grid, 128, 0, st>>>(a);
+  else
+    bc_dev_kernel<K, false, false><<<grid, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_boundary(Store kind, const BcArgs& a, cudaStream_t st) {
+  switch (kind) {
+    case Store::F64: return launch_boundary_f64(a, st);
+    case Store::F64D: return launch_bc_dev<Store::F64D>(a, st);
+    case Store::F32: return launch_bc_dev<Store::F32>(a, st);
+    case Store::F16: return launch_bc_dev<Store::F16>(a, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
 template <Store K, int BS>
 static cudaError_t launch_dev_bs(const StepArgs& a, cudaStream_t st) {
-  const int grid = (a.n + BS - 1) / BS;
+  const int grid = (a.n_main + BS - 1) / BS;
   if (grid == 0) return cudaSuccess;
   const bool given = a.rho_in != nullptr, write = a.rho_out != nullptr;
   if (given && write)
@@ -111,12 +200,16 @@ cudaError_t launch_reduce(Store kind, const ReduceArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_export_pop(Store kind, const void* pop, const int32_t* table, const int32_t* ref_of, int n,
-                              int npad, double fp16_scale, double* out, cudaStream_t st) {
+                              int npad, double fp16_scale, double* out, cudaStream_t st, int n_main,
+                              const double* bnd_f) {
   switch (kind) {
-    case Store::F64: return export_f64(pop, table, ref_of, n, npad, out, st);
-    case Store::F64D: return export_dispatch<Store::F64D>(pop, table, ref_of, n, npad, fp16_scale, out, st);
-    case Store::F32: return export_dispatch<Store::F32>(pop, table, ref_of, n, npad, fp16_scale, out, st);
-    case Store::F16: return export_dispatch<Store::F16>(pop, table, ref_of, n, npad, fp16_scale, out, st);
+    case Store::F64: return export_f64(pop, table, ref_of, n, npad, out, st, n_main, bnd_f);
+    case Store::F64D:
+      return export_dispatch<Store::F64D>(pop, table, ref_of, n, npad, fp16_scale, out, st, n_main, bnd_f);
+    case Store::F32:
+      return export_dispatch<Store::F32>(pop, table, ref_of, n, npad, fp16_scale, out, st, n_main, bnd_f);
+    case Store::F16:
+      return export_dispatch<Store::F16>(pop, table, ref_of, n, npad, fp16_scale, out, st, n_main, bnd_f);
   }
   return cudaErrorInvalidValue;
 }

@@ -41,12 +41,26 @@ class LbmError(RuntimeError):
         self.status = status
 
 
+class Boundary(C.Structure):
+    """lbm_boundary: pressure/velocity faces, INPUT.dat order xp, xn, yp, yn, zp, zn."""
+    _fields_ = [
+        ("sub_bc", C.c_int), ("in_bc", C.c_int), ("pressure", C.c_int * 6), ("rho", C.c_double * 6),
+        ("velocity", C.c_int * 6), ("vel", C.c_double * 6),
+    ]
+
+    @classmethod
+    def make(cls, sub_bc=0, in_bc=0, pressure=(0,) * 6, rho=(1.0,) * 6, velocity=(0,) * 6, vel=(0.0,) * 6):
+        return cls(int(sub_bc), int(in_bc), (C.c_int * 6)(*[int(x) for x in pressure]),
+                   (C.c_double * 6)(*[float(x) for x in rho]), (C.c_int * 6)(*[int(x) for x in velocity]),
+                   (C.c_double * 6)(*[float(x) for x in vel]))
+
+
 class Params(C.Structure):
     _fields_ = [
         ("nu", C.c_double), ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
         ("u_init", C.c_double * 3), ("precision", C.c_int), ("ordering", C.c_int),
         ("block_size", C.c_int), ("perdir", C.c_int), ("window", C.c_int * 6),
-        ("fp16_scale", C.c_double), ("device", C.c_int),
+        ("fp16_scale", C.c_double), ("device", C.c_int), ("bc", Boundary),
     ]
 
 
@@ -573,7 +587,7 @@ class SinglePhase:
 
     def __init__(self, mask, nu, g=(1e-6, 0.0, 0.0), precision="f32", ordering="reference",
                  block_size=256, u_init=(0.0, 0.0, 0.0), perdir=1, window=None, fp16_scale=0.0, device=0,
-                 _handle=None):
+                 bc=None, _handle=None):
         self._h = None
         if _handle is not None:
             self._h = _handle
@@ -593,6 +607,8 @@ class SinglePhase:
             p.window = (C.c_int * 6)(*[int(x) for x in window])
         p.fp16_scale = float(fp16_scale)
         p.device = int(device)
+        if bc is not None:
+            p.bc = bc if isinstance(bc, Boundary) else Boundary.make(**bc)
         h = C.c_void_p()
         _check(lib().lbm_create(C.byref(p), mask.reshape(-1), nx, ny, nz, C.byref(h)))
         self._h = h
