@@ -445,11 +445,17 @@ def run_cg(a):
     if rank != 0:
         return 0
     (d32, ms32, n), (d64, ms64, _) = out["f32"], out["f64"]
+    peak, peak_src = measured_peak()
+    # colour pass 2*19*4 + 18*4 + 3*4, collide pass 19*4 + 18*4 + 3*4 + 3*19*4 (FP32)
+    cg_bytes = (2 * 19 * 4 + 72 + 12) + (19 * 4 + 72 + 12 + 3 * 19 * 4)
+    achieved = n * cg_bytes / (ms32 * 1e-3) / 1e9
     line = {"metric": "colour-gradient fluid MLUPS (FP32)", "value": n / (ms32 * 1e-3) / 1e6, "unit": "MLUPS",
             "n_gpus": world, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "128^3 random cylinders r=3, porosity 0.6, blob phase field S_w=0.5, nu ratio 1, "
                                    "CapA=1e-3, psi_solid=cos45, gx=1e-5 on the non-wetting phase", "steps": steps,
                        "fluid_nodes": n},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_src, "bytes_per_lu": cg_bytes},
             "fp64_mlups": n / (ms64 * 1e-3) / 1e6,
             "saturation": {"f32": d32["saturation"], "f64": d64["saturation"]},
             "q_l_x": {"f32": d32["q_l"][0], "f64": d64["q_l"][0]},
@@ -461,10 +467,48 @@ def run_cg(a):
     return 0
 
 
+def run_solute(a):
+    """D3Q7 solute transport on the config-2 geometry (256^3 spheres, 5.87 M
+    fluid nodes) advected by the FP32 flow after 300 steps: solute MLUPS in
+    FP32 and FP64, against the 2*6*s + 6*4 + 3*s bytes per update."""
+    world, rank, local, pg = dist_setup()
+    import lbm_b200
+
+    mask = workload_mask()
+    rng = np.random.default_rng(7)
+    c0 = rng.uniform(0.0, 1.0, mask.shape)
+    steps = max(a.steps // 4, 50)
+    out = {}
+    with lbm_b200.SinglePhase(mask, NU, (GX, 0.0, 0.0), precision="f32", device=local) as flow:
+        flow.step(300)
+        for prec in ("f32", "f64"):
+            with lbm_b200.Solute(None, c0, 0.01, flow=flow, precision=prec, device=local) as s:
+                s.step(a.warmup)
+                s.step(steps)
+                out[prec] = (s.last_step_ms() / steps, s.count, float(s.concentration()[1:].sum()))
+    if rank != 0:
+        return 0
+    peak, peak_src = measured_peak()
+    (ms32, n, m32), (ms64, _, m64) = out["f32"], out["f64"]
+    b32, b64 = 2 * 6 * 4 + 6 * 4 + 3 * 4, 2 * 6 * 8 + 6 * 4 + 3 * 8
+    line = {"metric": "D3Q7 solute MLUPS (FP32)", "value": n / (ms32 * 1e-3) / 1e6, "unit": "MLUPS",
+            "n_gpus": world, "higher_is_better": True, "dtype": "f32", "data": "synthetic", "steps": steps,
+            "warmup": a.warmup,
+            "config": {"workload": "256^3 overlapping spheres r=U[4,10], phi=0.35 (config-2 geometry), D=0.01, "
+                                   "velocity of the FP32 flow after 300 steps", "fluid_nodes": n},
+            "roofline": {"bound": "hbm", "achieved": n * b32 / (ms32 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": n * b32 / (ms32 * 1e-3) / 1e9 / peak, "traffic": None, "peak_source": peak_src,
+                         "bytes_per_lu": b32},
+            "fp64": {"mlups": n / (ms64 * 1e-3) / 1e6, "gbs": n * b64 / (ms64 * 1e-3) / 1e9, "bytes_per_lu": b64},
+            "mass_rel_diff_f32_vs_f64": abs(m32 - m64) / abs(m64)}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cg-steps", type=int, default=20000)
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve", "cg"],
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve", "cg", "solute"],
                     help="cfg2 = the headline single-domain bench; batch / serve = configs 4 / 5")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=8.0)
@@ -492,6 +536,8 @@ def main():
         return run_serve(a)
     if a.workload == "cg":
         return run_cg(a)
+    if a.workload == "solute":
+        return run_solute(a)
     return run_ours(a)
 
 

@@ -295,6 +295,12 @@ class Solute:
         _check(lib().lbm_st7_get_concentration(self._h, c))
         return c
 
+    def last_step_ms(self):
+        """Device time of the last step() call in ms (CUDA events on the solver's stream)."""
+        c, st, ms = C.c_int(), C.c_longlong(), C.c_double()
+        _check(lib().lbm_st7_info(self._h, C.byref(c), C.byref(st), C.byref(ms)))
+        return ms.value
+
     def close(self):
         if getattr(self, "_h", None):
             lib().lbm_st7_destroy(self._h)

@@ -8,6 +8,7 @@ Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
   sp_outputs.npz  the reference program itself (oracle/_ref/ref_sp3_main)
                 run on an INPUT.dat: every file it writes  (--outputs)
+  sp_outputs_bc.npz  the same with pressure faces on x (Sub_BC 2, in_BC 1)  (--outputs)
   cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
   sp_bc.npz     pressure/velocity boundaries, Sub_BC 0..3, see bc_fixture()  (--bc)
   sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
@@ -176,19 +177,29 @@ def program_outputs():
     Backup_init (SP3:3663) divides by the global Zoom, which only init() sets,
     so a restarted run has dt = dx = inf and stops at its first report with
     NaN."""
-    import tempfile
-
     mask = G.overlapping_spheres((14, 12, 10), 0.6, 2.5, seed=21)
     in_a = input_text(L1="mask.dat", L2="14 12 10", L3=250, L17=1, L18=50, L20=100, L21=100, L32=100, L34=200)
+    save_program_outputs("sp_outputs.npz", mask, in_a)
+    # pressure faces on x (Sub_BC 2, in_BC 1: the permeability includes the
+    # pressure gradient), no body force: reports every 50 steps, velocity VTK
+    # at 150
+    in_b = input_text(L1="mask.dat", L2="14 12 10", L3=150, L4=7.5, L5=1, L6="0 0 0", L7="1 1.0 1 1.005", L17=1,
+                      L18=50, L20=150, L21=-1, L25=2, L32=-1, L34=-1)
+    save_program_outputs("sp_outputs_bc.npz", mask, in_b)
+
+
+def save_program_outputs(fname, mask, input_txt):
+    import tempfile
+
     with tempfile.TemporaryDirectory() as d:
-        run_program(d, in_a, mask)
+        run_program(d, input_txt, mask)
         a = collect(d, "out_")
-    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "input": np.frombuffer(in_a.encode(), np.uint8),
+    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "input": np.frombuffer(input_txt.encode(), np.uint8),
             "names": np.array(sorted(a))}
     for k, v in a.items():
         blob[k] = np.frombuffer(v, np.uint8) if isinstance(v, bytes) else np.array(v)
-    np.savez_compressed(os.path.join(HERE, "sp_outputs.npz"), **blob)
-    print("sp_outputs", sorted(a))
+    np.savez_compressed(os.path.join(HERE, fname), **blob)
+    print(fname, sorted(a))
 
 
 def bc_cases():

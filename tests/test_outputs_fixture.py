@@ -20,10 +20,11 @@ TIMING = (b"Elapsed time is", b"The expected completion time is")
 
 
 @pytest.mark.skipif(not os.path.exists(PROGRAM), reason="reference program not built")
-def test_fixture_is_the_reference_programs_output(tmp_path):
+@pytest.mark.parametrize("fixture", ["sp_outputs.npz", "sp_outputs_bc.npz"])
+def test_fixture_is_the_reference_programs_output(tmp_path, fixture):
     from lbm_b200 import geometry as G
 
-    z = np.load(os.path.join(GOLDEN, "sp_outputs.npz"))
+    z = np.load(os.path.join(GOLDEN, fixture))
     G.write_ascii(str(tmp_path / "mask.dat"), unpack_mask(z["mask"], z["shape"]))
     (tmp_path / "INPUT.dat").write_bytes(z["input"].tobytes())
     subprocess.run([PROGRAM, "INPUT.dat"], cwd=tmp_path, check=True, capture_output=True, timeout=120)
@@ -40,4 +41,6 @@ def test_fixture_is_the_reference_programs_output(tmp_path):
             if name == "Results.txt":
                 keep = lambda b: b"\n".join(l for l in b.split(b"\n") if not l.startswith(TIMING))  # noqa: E731
                 data, want = keep(data), keep(want)
+            if name == "Permeability_error_local_Perm.txt":  # first change divides by the unset Permia
+                data, want = data.split(b" ", 1)[1].split(b"\n", 1)[1], want.split(b" ", 1)[1].split(b"\n", 1)[1]
             assert data == want, name
