@@ -210,6 +210,27 @@ LBM_API lbm_status lbm_reduce(lbm_handle* h, lbm_diag* out);
 LBM_API lbm_status lbm_run_to_convergence(lbm_handle* h, double tol, int check_every, int max_steps,
                                   lbm_diag* out);
 
+/* Sub-volume flux sums of the current state: for each box (xn, xp, yn, yp,
+ * zn, zp inclusive, clipped to the grid) the sums of u_x, u_y, u_z over its
+ * pore cells and the number of pore cells, out[4*b .. 4*b+3].  The flux sums
+ * of Comput_Perm's window (SP3:3559-3590), Comput_Grop_Perm's cubes
+ * (SP:4886-5091) and Comput_Perm_LOCAL's plane (SP:4831-4884).  Sums run in
+ * a fixed order on the device (reproducible, not the reference's order). */
+LBM_API lbm_status lbm_box_sums(lbm_handle* h, int nbox, const int32_t* boxes, double* out);
+
+/* Comput_Grop_Perm (SP:4886-5091): division d has n_sub[d]^3 cubes of edge
+ * size[d], the first with low corner corner[3d .. 3d+2]; cube (a, b, c), in
+ * the reference's loop order (a = x outer, c = z inner), starts at corner +
+ * (a, b, c) * size[d].  out[4*cube ..] = permeability (x, y, z; lattice
+ * units: Q / size^3 * nu / (g + dp)) and porosity (pores / size^3).  dp uses
+ * the whole box length (SP:4928-4941). */
+LBM_API lbm_status lbm_group_perm(lbm_handle* h, int ndiv, const int* n_sub, const int* size, const int* corner,
+                                  double* out);
+
+/* Comput_Perm_LOCAL (SP:4831-4884): permeability from the flux through the
+ * plane x = nx-2, normalised by the window's cross-sections. */
+LBM_API lbm_status lbm_local_perm(lbm_handle* h, double perm[3]);
+
 /* Number of fluid nodes (the reference's Count) and geometry facts. */
 LBM_API lbm_status lbm_info(lbm_handle* h, int* count, double* porosity, long long* step);
 

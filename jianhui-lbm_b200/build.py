@@ -37,6 +37,7 @@ CUDA_SOURCES = [
     ("cg_faithful.cu", ["-fmad=false"]),
     ("cg_fast.cu", []),
     ("st7_kernels.cu", ["-fmad=false"]),
+    ("box_sums.cu", []),
 ]
 CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp", "output.cpp"]
 # Command-line drivers linked against liblbm.so: (source, executable name).

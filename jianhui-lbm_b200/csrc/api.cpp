@@ -12,6 +12,8 @@
 namespace lbm {
 
 lbm_status read_input_file(const char* path, lbm_input* o);
+cudaError_t launch_box_sums(const int32_t* cell_idx, const double* u, int npad, int nx, int ny, const int32_t* boxes,
+                            int nbox, int chunks, double* partials, double* out, cudaStream_t st);
 lbm_status read_mask_file(const char* path, int nx, int ny, int nz, int decbin, uint8_t* mask);
 
 static thread_local std::string g_last_error;
@@ -74,6 +76,9 @@ struct lbm_handle {
   // operations, M^-1 for the moment rule, post-rule populations of the state
   BcPlan bc;
   DevBuf snap[2], bc_ops, bc_off, bc_mi, bnd_f;
+  // dense cell -> internal index map for box sums, built on first use
+  DevBuf cell_idx;
+  bool cell_idx_valid = false;
   int cur = 0;
   long long step = 0;
   bool given_macro = true;  // next step / reduce takes rho, u from rho_given / u_given
@@ -134,6 +139,7 @@ lbm_status upload_layout(lbm_handle* h) {
   }
   h->last_p = g.count > 0 ? g.int_of[g.count] : -1;
   h->drop_graphs();
+  h->cell_idx_valid = false;
   return LBM_OK;
 }
 
@@ -861,6 +867,129 @@ lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* 
   if (ordering_out) *ordering_out = best_o;
   if (block_out) *block_out = best_b;
   if (mlups_out) *mlups_out = best;
+  return LBM_OK;
+}
+
+
+// ------------------------------------------------------------ box sums
+lbm_status lbm_box_sums(lbm_handle* h, int nbox, const int32_t* boxes, double* out) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (nbox < 0 || (nbox > 0 && (!boxes || !out))) return fail(LBM_ERR_ARG, "lbm_box_sums: bad argument");
+  if (nbox == 0) return LBM_OK;
+  if (nbox > 65535) return fail(LBM_ERR_ARG, "lbm_box_sums: at most 65535 boxes per call");
+  const Geometry& g = h->geo;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  // clip to the grid; an empty box sums to zero
+  std::vector<int32_t> clipped((size_t)nbox * 6);
+  std::vector<int> live;
+  long long cells = 0;
+  for (int b = 0; b < nbox; b++) {
+    const int32_t* in = boxes + (size_t)b * 6;
+    const int32_t lo[3] = {std::max(in[0], 0), std::max(in[2], 0), std::max(in[4], 0)};
+    const int32_t hi[3] = {std::min(in[1], nx - 1), std::min(in[3], ny - 1), std::min(in[5], nz - 1)};
+    if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
+    int32_t* c = &clipped[live.size() * 6];
+    c[0] = lo[0]; c[1] = hi[0]; c[2] = lo[1]; c[3] = hi[1]; c[4] = lo[2]; c[5] = hi[2];
+    cells += (long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    live.push_back(b);
+  }
+  std::memset(out, 0, sizeof(double) * 4 * (size_t)nbox);
+  if (live.empty()) return LBM_OK;
+  if (!h->cell_idx_valid) {
+    ensure_host_geometry(h);
+    std::vector<int32_t> idx((size_t)nx * ny * nz, -1);
+    for (int p = 0; p < g.count; p++) {
+      const int c = g.coor[g.ref_of[p]];
+      const int i = c / (ny * nz), j = (c % (ny * nz)) / nz, k = c % nz;
+      idx[i + (size_t)nx * (j + (size_t)ny * k)] = p;
+    }
+    if (h->cell_idx.bytes != idx.size() * sizeof(int32_t)) LBM_CUDA_TRY(h->cell_idx.alloc(idx.size() * sizeof(int32_t)));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->cell_idx.p, idx.data(), idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                 h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->cell_idx_valid = true;
+  }
+  const int nl = (int)live.size();
+  const long long avg = cells / nl;
+  const int chunks = (int)std::max<long long>(1, std::min<long long>(256, avg / 32768));
+  DevBuf u, dboxes, partials, dout;
+  LBM_CUDA_TRY(u.alloc((size_t)3 * g.npad * sizeof(double)));
+  LBM_CUDA_TRY(dboxes.alloc((size_t)nl * 6 * sizeof(int32_t)));
+  LBM_CUDA_TRY(partials.alloc((size_t)nl * chunks * 8 * sizeof(double)));
+  LBM_CUDA_TRY(dout.alloc((size_t)nl * 4 * sizeof(double)));
+  double r[8];
+  if ((st = reduce_raw(h, r, nullptr, u.as<double>())) != LBM_OK) return st;
+  LBM_CUDA_TRY(cudaMemcpyAsync(dboxes.p, clipped.data(), (size_t)nl * 6 * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               h->stream));
+  LBM_CUDA_TRY(launch_box_sums(h->cell_idx.as<int32_t>(), u.as<double>(), g.npad, nx, ny, dboxes.as<int32_t>(), nl,
+                               chunks, partials.as<double>(), dout.as<double>(), h->stream));
+  std::vector<double> res((size_t)nl * 4);
+  LBM_CUDA_TRY(cudaMemcpyAsync(res.data(), dout.p, res.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (int l = 0; l < nl; l++)
+    for (int i = 0; i < 4; i++) out[(size_t)live[l] * 4 + i] = res[(size_t)l * 4 + i];
+  return LBM_OK;
+}
+
+// dp of the slab program's sub-volume permeabilities: whole-box length
+// (SP:4844-4857, 4928-4941).
+static double sp_dp(const lbm_handle* h) {
+  if (h->prm.bc.in_bc == 0) return 0.0;
+  const int dir = (h->prm.perdir >= 1 && h->prm.perdir <= 3) ? h->prm.perdir - 1 : 0;
+  const int ext[3] = {h->geo.nx, h->geo.ny, h->geo.nz};
+  const double c_s2 = 1.0 * 1.0 / 3, dx = 1.0;
+  return std::fabs(h->prm.bc.rho[2 * dir] - h->prm.bc.rho[2 * dir + 1]) * c_s2 / ext[dir] / dx;
+}
+
+lbm_status lbm_group_perm(lbm_handle* h, int ndiv, const int* n_sub, const int* size, const int* corner,
+                          double* out) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (ndiv < 0 || (ndiv > 0 && (!n_sub || !size || !corner || !out))) return fail(LBM_ERR_ARG, "lbm_group_perm: bad argument");
+  std::vector<int32_t> boxes;
+  std::vector<int> vol;
+  for (int d = 0; d < ndiv; d++) {
+    if (n_sub[d] < 0 || size[d] <= 0) return fail(LBM_ERR_ARG, "lbm_group_perm: bad division");
+    for (int a = 0; a < n_sub[d]; a++)
+      for (int b = 0; b < n_sub[d]; b++)
+        for (int c = 0; c < n_sub[d]; c++) {
+          const int lo[3] = {corner[3 * d] + a * size[d], corner[3 * d + 1] + b * size[d], corner[3 * d + 2] + c * size[d]};
+          for (int ax = 0; ax < 3; ax++) {
+            boxes.push_back(lo[ax]);
+            boxes.push_back(lo[ax] + size[d] - 1);
+          }
+          vol.push_back(size[d] * size[d] * size[d]);
+        }
+  }
+  const int nbox = (int)vol.size();
+  std::vector<double> sums((size_t)nbox * 4);
+  if ((st = lbm_box_sums(h, nbox, boxes.data(), sums.data())) != LBM_OK) return st;
+  const double dp = sp_dp(h), nu = h->prm.nu;
+  const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
+  for (int b = 0; b < nbox; b++) {
+    for (int i = 0; i < 3; i++) out[(size_t)b * 4 + i] = sums[(size_t)b * 4 + i] / (vol[b]) * (nu) / (gg[i] + dp);
+    out[(size_t)b * 4 + 3] = sums[(size_t)b * 4 + 3] / vol[b];
+  }
+  return LBM_OK;
+}
+
+lbm_status lbm_local_perm(lbm_handle* h, double perm[3]) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (!perm) return fail(LBM_ERR_ARG, "lbm_local_perm: null output");
+  const Geometry& g = h->geo;
+  const int x = g.nx >= 2 ? g.nx - 2 : 0;
+  const int32_t box[6] = {x, x, 0, g.ny - 1, 0, g.nz - 1};
+  double s[4];
+  if ((st = lbm_box_sums(h, 1, box, s)) != LBM_OK) return st;
+  const int* w = h->prm.window;
+  const bool full = w[0] < 0 && w[1] < 0 && w[2] < 0 && w[3] < 0 && w[4] < 0 && w[5] < 0;
+  const int lx = full ? g.nx : w[1] - w[0] + 1, ly = full ? g.ny : w[3] - w[2] + 1, lz = full ? g.nz : w[5] - w[4] + 1;
+  const double dp = sp_dp(h), nu = h->prm.nu;
+  perm[0] = s[0] / (ly * lz) * (nu) / (h->prm.gx + dp);
+  perm[1] = s[1] / (lx * lz) * (nu) / (h->prm.gy + dp);
+  perm[2] = s[2] / (lx * ly) * (nu) / (h->prm.gz + dp);
   return LBM_OK;
 }
 

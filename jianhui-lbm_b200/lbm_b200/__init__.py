@@ -223,6 +223,9 @@ _SIGNATURES = {
     "lbm_read_velocity_for_solute": ([C.c_char_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
     "lbm_write_velocity_for_solute_ordered": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
     "lbm_read_velocity_for_solute_ordered": ([C.c_char_p, _U8P, C.c_int, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
+    "lbm_box_sums": ([C.c_void_p, C.c_int, _I32P, _F64P], C.c_int),
+    "lbm_group_perm": ([C.c_void_p, C.c_int, _I32P, _I32P, _I32P, _F64P], C.c_int),
+    "lbm_local_perm": ([C.c_void_p, _F64P], C.c_int),
     "lbm_write_vtk_geometry": ([_U8P, C.c_int, C.c_int, C.c_int, C.c_char_p], C.c_int),
     "lbm_write_vtk_velocity": ([C.c_void_p, C.c_char_p], C.c_int),
     "lbm_write_vtk_density": ([C.c_void_p, C.c_char_p], C.c_int),
@@ -688,6 +691,28 @@ class SinglePhase:
         u = np.zeros((self.count + 1) * 3)
         _check(lib().lbm_get_fields(self._h, rho.ctypes.data, u.ctypes.data))
         return rho, u.reshape(-1, 3)
+
+    def box_sums(self, boxes):
+        """[(xn, xp, yn, yp, zn, zp), ...] -> array [nbox, 4]: sum u_x, u_y, u_z, pore cells."""
+        b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int32).reshape(-1, 6))
+        out = np.zeros(b.shape[0] * 4)
+        _check(lib().lbm_box_sums(self._h, b.shape[0], b.reshape(-1), out))
+        return out.reshape(-1, 4)
+
+    def group_perm(self, n_sub, size, corner):
+        """Comput_Grop_Perm: per cube (perm_x, perm_y, perm_z, porosity), divisions concatenated."""
+        n_sub = np.ascontiguousarray(n_sub, dtype=np.int32)
+        size = np.ascontiguousarray(size, dtype=np.int32)
+        corner = np.ascontiguousarray(np.asarray(corner, dtype=np.int32).reshape(-1))
+        ncube = int((n_sub.astype(np.int64) ** 3).sum())
+        out = np.zeros(max(ncube, 1) * 4)
+        _check(lib().lbm_group_perm(self._h, n_sub.size, n_sub, size, corner, out))
+        return out[: ncube * 4].reshape(-1, 4)
+
+    def local_perm(self):
+        out = np.zeros(3)
+        _check(lib().lbm_local_perm(self._h, out))
+        return out
 
     def populations(self):
         f = np.zeros((self.count + 1) * 19)

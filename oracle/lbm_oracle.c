@@ -556,3 +556,45 @@ double orc_sp_dp(int in_bc, int perdir, const double* p, int nx, int ny, int nz)
     default: return fabs(p[0] - p[1]) * c_s2 / (nx - 1 - 0 + 1) / dx;
   }
 }
+
+/* `Comput_Grop_Perm` (SP:4886-5091) at one rank: for each division d, the
+ * n_sub[d]^3 cubes of edge size[d] whose first low corner is corner[3*d..];
+ * cube (a, b, c) (loop order a = x outer, b = y, c = z inner) spans
+ * [corner + (a, b, c) * size, + size - 1] on each axis.  Per cube:
+ * Q = sum of u over the fluid nodes inside (id order), perm_d = Q_d / size^3
+ * * nu / (g_d + dp), porosity = pores / size^3; written to out as
+ * (perm_x, perm_y, perm_z, porosity).  SP's dp uses the whole box:
+ * |p_+ - p_-| c_s^2 / (N+1) / dx (SP:4928-4941).  Returns the number of cubes. */
+int orc_sp_group_perm(int count, const double* u, const int32_t* coor, int nx, int ny, int nz, double nu, double gx,
+                      double gy, double gz, double dp, int ndiv, const int* n_sub, const int* size,
+                      const int* corner, double* out) {
+  (void)nx;
+  int cube = 0;
+  for (int d = 0; d < ndiv; d++) {
+    const int vol = size[d] * size[d] * size[d];
+    for (int a = 0; a < n_sub[d]; a++)
+      for (int b = 0; b < n_sub[d]; b++)
+        for (int c = 0; c < n_sub[d]; c++) {
+          const int xn = corner[3 * d + 0] + a * size[d], xp = corner[3 * d + 0] + a * size[d] + size[d] - 1;
+          const int yn = corner[3 * d + 1] + b * size[d], yp = corner[3 * d + 1] + b * size[d] + size[d] - 1;
+          const int zn = corner[3 * d + 2] + c * size[d], zp = corner[3 * d + 2] + c * size[d] + size[d] - 1;
+          double Q[3] = {0, 0, 0};
+          int pores = 0;
+          for (int i = 1; i <= count; i++) {
+            const int si = coor[i] / (ny * nz), sj = (coor[i] % (ny * nz)) / nz, sm = coor[i] % nz;
+            if (si >= xn && si <= xp && sj >= yn && sj <= yp && sm >= zn && sm <= zp) {
+              Q[0] += u[(long)i * 3 + 0];
+              Q[1] += u[(long)i * 3 + 1];
+              Q[2] += u[(long)i * 3 + 2];
+              pores += 1;
+            }
+          }
+          out[cube * 4 + 0] = Q[0] / (vol) * (nu) / (gx + dp);
+          out[cube * 4 + 1] = Q[1] / (vol) * (nu) / (gy + dp);
+          out[cube * 4 + 2] = Q[2] / (vol) * (nu) / (gz + dp);
+          out[cube * 4 + 3] = (double)pores / vol;
+          cube++;
+        }
+  }
+  return cube;
+}

@@ -82,6 +82,9 @@ class Restatement:
         L.orc_sp_perm_dp.restype = C.c_double
         L.orc_sp_dp.argtypes = [C.c_int, C.c_int, _F64P, C.c_int, C.c_int, C.c_int]
         L.orc_sp_dp.restype = C.c_double
+        L.orc_sp_group_perm.argtypes = [C.c_int, _F64P, _I32P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, C.c_double, C.c_int, _I32P, _I32P, _I32P, _F64P]
+        L.orc_sp_group_perm.restype = C.c_int
 
     def matrices(self):
         M = np.zeros((19, 19))
@@ -197,6 +200,17 @@ class SinglePhaseRun:
 
     def fields(self):
         return (self.f.reshape(-1, 19).copy(), self.u.reshape(-1, 3).copy(), self.rho.copy())
+
+    def group_perm(self, n_sub, size, corner, dp=0.0):
+        """Comput_Grop_Perm (SP:4886-5091): per cube (perm_x, perm_y, perm_z, porosity)."""
+        n_sub = np.ascontiguousarray(n_sub, dtype=np.int32)
+        size = np.ascontiguousarray(size, dtype=np.int32)
+        corner = np.ascontiguousarray(np.asarray(corner, dtype=np.int32).reshape(-1))
+        ncube = int((n_sub.astype(np.int64) ** 3).sum())
+        out = np.zeros(max(ncube, 1) * 4)
+        self.R.L.orc_sp_group_perm(self.count, self.u, self.coor, self.nx, self.ny, self.nz, self.nu, *self.g, dp,
+                                   n_sub.size, n_sub, size, corner, out)
+        return out[: ncube * 4].reshape(-1, 4)
 
 
 class CGParams(C.Structure):
