@@ -12,12 +12,227 @@ __device__ __forceinline__ float cg_mi<false>(int q, int j) {
   return c_MIcg_f[q * kQ + j];
 }
 
+// M^-1 split by parity.  Moments of even degree (rows kEven) depend only on
+// f_0 and the pair sums s_i = f_{2i-1} + f_{2i}; odd ones (kOdd) only on the
+// pair differences d_i = f_{2i-1} - f_{2i} (the CG order keeps opposite
+// directions adjacent).  So f*_0 and h_i = (f*_{2i-1} + f*_{2i})/2 come from
+// the even moments and g_i = (f*_{2i-1} - f*_{2i})/2 from the odd ones:
+// 10x10 + 9x9 products instead of 19x19.
+__host__ __device__ constexpr int kEven(int c) { return c < 3 ? c : c + 6; }   // 0, 1, 2, 9 .. 15
+__host__ __device__ constexpr int kOdd(int c) { return c < 6 ? c + 3 : c + 10; }  // 3 .. 8, 16, 17, 18
+__constant__ float c_MIe[10 * 10];
+__constant__ float c_MIo[9 * 9];
+
 cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st) {
-  float m[kQ * kQ];
+  float m[kQ * kQ], me[100], mo[81];
   for (int i = 0; i < kQ * kQ; i++) m[i] = (float)mi[i];
-  const cudaError_t e = cudaMemcpyToSymbolAsync(c_MIcg_f, m, sizeof(m), 0, cudaMemcpyHostToDevice, st);
+  for (int c = 0; c < 10; c++) me[c] = (float)mi[kEven(c)];
+  for (int i = 1; i <= 9; i++) {
+    for (int c = 0; c < 10; c++)
+      me[i * 10 + c] = (float)(0.5 * (mi[(2 * i - 1) * kQ + kEven(c)] + mi[(2 * i) * kQ + kEven(c)]));
+    for (int c = 0; c < 9; c++)
+      mo[(i - 1) * 9 + c] = (float)(0.5 * (mi[(2 * i - 1) * kQ + kOdd(c)] - mi[(2 * i) * kQ + kOdd(c)]));
+  }
+  cudaError_t e = cudaMemcpyToSymbolAsync(c_MIcg_f, m, sizeof(m), 0, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_MIe, me, sizeof(me), 0, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_MIo, mo, sizeof(mo), 0, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return e;
-  return cudaStreamSynchronize(st);  // m is a host temporary
+  return cudaStreamSynchronize(st);  // the arrays are host temporaries
+}
+
+// FP32 collide pass: the operator of the FP64 kernel (CG3:2684-3505) with
+// the arithmetic arranged for the GPU: the 18 table entries are read once and
+// serve both the population pull and the neighbour psi of the colour
+// gradient; moments, Guo moments and the back-transform use the opposite-pair
+// split; divisions by constants and repeated divisions become reciprocal
+// multiplies.
+__global__ void __launch_bounds__(256, 3) cg_collide_fast_kernel(CgArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  const float* __restrict__ fs = static_cast<const float*>(a.f_src);
+  float* __restrict__ fd = static_cast<float*>(a.f_dst);
+  const float* __restrict__ psi = static_cast<const float*>(a.psi);
+  const int npad = a.npad;
+
+  int32_t tb[kQ];  // tb[q] = pull source of storage row q (q >= 1)
+  tb[0] = x;
+#pragma unroll
+  for (int q = 1; q < kQ; q++) tb[q] = __ldg(a.table + (size_t)(q - 1) * npad + x);
+
+  // pulled deviations in CG order, pair sums / differences
+  const float f0 = __ldg(fs + x);
+  float sp[10], dp[10];
+#pragma unroll
+  for (int i = 1; i <= 9; i++) {
+    const float fa = __ldg(fs + tb[cg::row(2 * i - 1)]), fb = __ldg(fs + tb[cg::row(2 * i)]);
+    sp[i] = fa + fb;
+    dp[i] = fa - fb;
+  }
+
+  // colour gradient (CG3:2684-2712): psi at x + e_t is the source node of
+  // row opp(row(t)); the table entries are dead after this
+  const float psi_x = psi[x];
+  const float psi_s = (float)a.p.psi_solid;
+  float C0 = 0.f, C1 = 0.f, C2 = 0.f;
+  bool wall = false;
+#pragma unroll
+  for (int t = 1; t < kQ; t++) {
+    const int q = opp(cg::row(t));
+    const int32_t s = tb[q];
+    const int32_t lo = q * npad;
+    float pn;
+    if (s >= lo && s < lo + npad) {
+      pn = psi[s - lo];
+    } else {
+      pn = psi_s;
+      wall = true;
+    }
+    const float c3w = (float)(3.0 * weight(t));
+    if (cg::ex(t)) C0 += (c3w * (float)cg::ex(t)) * pn;
+    if (cg::ey(t)) C1 += (c3w * (float)cg::ey(t)) * pn;
+    if (cg::ez(t)) C2 += (c3w * (float)cg::ez(t)) * pn;
+  }
+  const float gx = (float)a.p.g[0], gy = (float)a.p.g[1], gz = (float)a.p.g[2];
+  float drho, rho, ux, uy, uz;
+  if (a.given) {
+    drho = 0.f;
+    rho = 1.f;
+    ux = uy = uz = 0.f;
+  } else {
+    float r = f0, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int i = 1; i <= 9; i++) {
+      r += sp[i];
+      if (cg::ex(2 * i - 1)) jx += (float)cg::ex(2 * i - 1) * dp[i];
+      if (cg::ey(2 * i - 1)) jy += (float)cg::ey(2 * i - 1) * dp[i];
+      if (cg::ez(2 * i - 1)) jz += (float)cg::ez(2 * i - 1) * dp[i];
+    }
+    drho = r;
+    rho = 1.f + r;
+    const float ir = 1.f / rho;
+    ux = (jx + 0.5f * gx) * ir;
+    uy = (jy + 0.5f * gy) * ir;
+    uz = (jz + 0.5f * gz) * ir;
+  }
+
+  const float* __restrict__ rrp = static_cast<const float*>(a.rho_r);
+  const float* __restrict__ rbp = static_cast<const float*>(a.rho_b);
+  const float rr = rrp[x], rb = rbp[x];
+  if (fabsf(rr - rb) >= 0.9f && wall) C0 = C1 = C2 = 0.f;
+  const float cc = sqrtf(C0 * C0 + C1 * C1 + C2 * C2);
+  const float icc = cc > 0.f ? 1.f / cc : 0.f;
+  const float nx = C0 * icc, ny = C1 * icc, nz = C2 * icc;
+
+  // Guo force moments from closed-form pair sums / differences:
+  //   G_0 = -3 w_0 u.g,  G_a + G_b = w (18 (e.u)(e.g) - 6 u.g),  G_a - G_b = 6 w e.g
+  const bool no_force = ((a.p.body_force_phase == 1) && (psi_x < (float)a.p.flux_psi)) ||
+                        ((a.p.body_force_phase == -1) && (psi_x > -(float)a.p.flux_psi));
+  const float ug = ux * gx + uy * gy + uz * gz;
+  const float G0 = no_force ? 0.f : (float)(-3.0 * weight(0)) * ug;
+  float gs[10], gd[10];
+#pragma unroll
+  for (int i = 1; i <= 9; i++) {
+    const int k = 2 * i - 1;
+    const float eu = (float)cg::ex(k) * ux + (float)cg::ey(k) * uy + (float)cg::ez(k) * uz;
+    const float eg = (float)cg::ex(k) * gx + (float)cg::ey(k) * gy + (float)cg::ez(k) * gz;
+    const float w = (float)weight(k);
+    gs[i] = no_force ? 0.f : w * (18.f * eu * eg - 6.f * ug);
+    gd[i] = no_force ? 0.f : (6.f * w) * eg;
+  }
+
+  // equilibrium moments with the surface-tension perturbation (CG3:2836-2851)
+  const float cap = (float)a.p.cap_a;
+  const float cc5 = 0.5f * cap * cc;
+  float meq[kQ];
+#pragma unroll
+  for (int k = 0; k < kQ; k++) meq[k] = 0.f;
+  meq[0] = drho;
+  meq[3] = ux;
+  meq[5] = uy;
+  meq[7] = uz;
+  meq[1] = (ux * ux + uy * uy + uz * uz) + cap * cc;
+  meq[9] = (2.f * ux * ux - uy * uy - uz * uz) + cc5 * (2.f * nx * nx - ny * ny - nz * nz);
+  meq[11] = (uy * uy - uz * uz) + cc5 * (ny * ny - nz * nz);
+  meq[13] = ux * uy + cc5 * (nx * ny);
+  meq[14] = uy * uz + cc5 * (ny * nz);
+  meq[15] = ux * uz + cc5 * (nx * nz);
+
+  // viscosity interpolation in psi (CG3:2862-2872)
+  float s_v;
+  if (psi_x > 0.f)
+    s_v = psi_x > (float)a.p.delta ? (float)a.p.wl : (float)a.p.lg0 + (float)a.p.l1 * psi_x + (float)a.p.l2 * psi_x * psi_x;
+  else
+    s_v = psi_x < -(float)a.p.delta ? (float)a.p.wg : (float)a.p.lg0 + (float)a.p.g1 * psi_x + (float)a.p.g2 * psi_x * psi_x;
+  const float s_o = 8.f * (2.f - s_v) / (8.f - s_v);
+
+  // relaxed moments m* = m - S (m - meq) + (1 - S/2) M G
+  float ml[kQ];
+#pragma unroll
+  for (int k = 0; k < kQ; k++) {
+    const bool odd = (k >= 3 && k <= 8) || k >= 16;
+    float m = odd ? 0.f : (float)cg::mcoef(k, 0) * f0;
+    float fh = odd ? 0.f : (float)cg::mcoef(k, 0) * G0;
+#pragma unroll
+    for (int i = 1; i <= 9; i++) {
+      const int c = cg::mcoef(k, 2 * i - 1);
+      if (c == 0) continue;
+      m += (float)c * (odd ? dp[i] : sp[i]);
+      fh += (float)c * (odd ? gd[i] : gs[i]);
+    }
+    const bool cons = (k == 0 || k == 3 || k == 5 || k == 7);
+    const bool visc = (k == 1 || k == 2 || (k >= 9 && k <= 15));
+    const float S = cons ? 0.f : (visc ? s_v : s_o);
+    ml[k] = m - S * (m - meq[k]) + (1.f - 0.5f * S) * fh;
+  }
+
+  // back-transform by parity blocks
+  {
+    float v = 0.f;
+#pragma unroll
+    for (int c = 0; c < 10; c++) v += c_MIe[c] * ml[kEven(c)];
+    fd[x] = v;
+  }
+#pragma unroll
+  for (int i = 1; i <= 9; i++) {
+    float h = 0.f, g = 0.f;
+#pragma unroll
+    for (int c = 0; c < 10; c++) h += c_MIe[i * 10 + c] * ml[kEven(c)];
+#pragma unroll
+    for (int c = 0; c < 9; c++) g += c_MIo[(i - 1) * 9 + c] * ml[kOdd(c)];
+    fd[(size_t)cg::row(2 * i - 1) * npad + x] = h + g;
+    fd[(size_t)cg::row(2 * i) * npad + x] = h - g;
+  }
+
+  // equilibrium colour distributions and recolouring (CG3:3472-3505)
+  const float uu = ux * ux + uy * uy + uz * uz;
+  const float base = 1.f - 1.5f * uu;
+  float* __restrict__ grp = static_cast<float*>(a.gr);
+  float* __restrict__ gbp = static_cast<float*>(a.gb);
+  {
+    const float w0 = (float)weight(0);
+    grp[x] = w0 * rr * base;
+    gbp[x] = w0 * rb * base;
+  }
+#pragma unroll
+  for (int i = 1; i <= 9; i++) {
+    const int ka = 2 * i - 1, kb = 2 * i;
+    const float eu = (float)cg::ex(ka) * ux + (float)cg::ey(ka) * uy + (float)cg::ez(ka) * uz;
+    const float w = (float)weight(ka);
+    const float Ea = base + 3.f * eu + 4.5f * eu * eu, Eb = base - 3.f * eu + 4.5f * eu * eu;
+    float ra = w * rr * Ea, rbb = w * rr * Eb, ba = w * rb * Ea, bb = w * rb * Eb;
+    if (cc > 0.f) {
+      const float ef = (float)cg::ex(ka) * C0 + (float)cg::ey(ka) * C1 + (float)cg::ez(ka) * C2;
+      const float cp = fminf(fminf(ra, rbb), fminf(ba, bb)) * (ef * icc);
+      ra += cp;
+      rbb -= cp;
+      ba -= cp;
+      bb += cp;
+    }
+    grp[(size_t)cg::row(ka) * npad + x] = ra;
+    grp[(size_t)cg::row(kb) * npad + x] = rbb;
+    gbp[(size_t)cg::row(ka) * npad + x] = ba;
+    gbp[(size_t)cg::row(kb) * npad + x] = bb;
+  }
 }
 
 cudaError_t cg_colour_f32(const CgArgs& a, cudaStream_t st) {
@@ -26,7 +241,7 @@ cudaError_t cg_colour_f32(const CgArgs& a, cudaStream_t st) {
 }
 
 cudaError_t cg_collide_f32(const CgArgs& a, cudaStream_t st) {
-  if (a.n > 0) cg_collide_kernel<false><<<(a.n + 255) / 256, 256, 0, st>>>(a);
+  if (a.n > 0) cg_collide_fast_kernel<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
