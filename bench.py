@@ -514,7 +514,7 @@ def main():
     ap.add_argument("--rate", type=float, default=8.0)
     ap.add_argument("--pool-nodes", type=int, default=96 * 1024 * 1024)
     ap.add_argument("--fp64-sample", type=int, default=6)
-    ap.add_argument("--target-nodes", type=int, default=8 * 1024 * 1024,
+    ap.add_argument("--target-nodes", type=int, default=1024 * 1024,
                     help="serve: resident-node target (0 = admit while memory allows)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)

@@ -27,9 +27,17 @@ __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int cha
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
   const size_t cap = (size_t)a.cap;
   const int na = *a.n_active;
-  for (int i = blockIdx.x; i < na; i += gridDim.x) {
-    const int t = a.active_tiles[i];
-    const int slot = a.tile_inst[t];
+  // tile -> slot lookups of the next tile are issued before this tile's
+  // work, so their latency hides behind it instead of starting every tile
+  int i = blockIdx.x;
+  int t_next = i < na ? a.active_tiles[i] : 0;
+  int s_next = i < na ? a.tile_inst[t_next] : 0;
+  for (; i < na; i += gridDim.x) {
+    const int t = t_next, slot = s_next;
+    if (i + (int)gridDim.x < na) {
+      t_next = a.active_tiles[i + gridDim.x];
+      s_next = a.tile_inst[t_next];
+    }
     const InstParams ip = a.inst[slot];
     const bool given = (chain_step == 0) && a.state[slot].fresh;
     const float scale = ip.fp16_scale, inv_scale = 1.0f / ip.fp16_scale;

@@ -43,10 +43,10 @@ cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st) {
 // FP32 collide pass: the operator of the FP64 kernel (CG3:2684-3505) with
 // the arithmetic arranged for the GPU: the 18 table entries are read once and
 // serve both the population pull and the neighbour psi of the colour
-// gradient; moments, Guo moments and the back-transform use the opposite-pair
-// split; divisions by constants and repeated divisions become reciprocal
-// multiplies.
-__global__ void __launch_bounds__(256, 3) cg_collide_fast_kernel(CgArgs a) {
+// gradient; moments and the back-transform use the opposite-pair split, the
+// Guo moments their closed forms; divisions by constants and repeated
+// divisions become reciprocal multiplies.
+__global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= a.n) return;
   const float* __restrict__ fs = static_cast<const float*>(a.f_src);
@@ -123,21 +123,26 @@ __global__ void __launch_bounds__(256, 3) cg_collide_fast_kernel(CgArgs a) {
   const float icc = cc > 0.f ? 1.f / cc : 0.f;
   const float nx = C0 * icc, ny = C1 * icc, nz = C2 * icc;
 
-  // Guo force moments from closed-form pair sums / differences:
-  //   G_0 = -3 w_0 u.g,  G_a + G_b = w (18 (e.u)(e.g) - 6 u.g),  G_a - G_b = 6 w e.g
+  // Guo forcing moments M G (CG3:2745-2825, G_q = w_q [3 (e_q - u).g +
+  // 9 (e_q.u)(e_q.g)]) in closed form for this basis: the lattice sums of
+  // c_kq w_q e_q and c_kq w_q e_q e_q leave nine non-zero rows; zero where
+  // the phase is not driven
   const bool no_force = ((a.p.body_force_phase == 1) && (psi_x < (float)a.p.flux_psi)) ||
                         ((a.p.body_force_phase == -1) && (psi_x > -(float)a.p.flux_psi));
-  const float ug = ux * gx + uy * gy + uz * gz;
-  const float G0 = no_force ? 0.f : (float)(-3.0 * weight(0)) * ug;
-  float gs[10], gd[10];
+  float MG[kQ];
 #pragma unroll
-  for (int i = 1; i <= 9; i++) {
-    const int k = 2 * i - 1;
-    const float eu = (float)cg::ex(k) * ux + (float)cg::ey(k) * uy + (float)cg::ez(k) * uz;
-    const float eg = (float)cg::ex(k) * gx + (float)cg::ey(k) * gy + (float)cg::ez(k) * gz;
-    const float w = (float)weight(k);
-    gs[i] = no_force ? 0.f : w * (18.f * eu * eg - 6.f * ug);
-    gd[i] = no_force ? 0.f : (6.f * w) * eg;
+  for (int k = 0; k < kQ; k++) MG[k] = 0.f;
+  if (!no_force) {
+    const float xx = ux * gx, yy = uy * gy, zz = uz * gz;
+    MG[1] = 2.f * (xx + yy + zz);
+    MG[3] = gx;
+    MG[5] = gy;
+    MG[7] = gz;
+    MG[9] = 4.f * xx - 2.f * yy - 2.f * zz;
+    MG[11] = 2.f * yy - 2.f * zz;
+    MG[13] = ux * gy + uy * gx;
+    MG[14] = uy * gz + uz * gy;
+    MG[15] = ux * gz + uz * gx;
   }
 
   // equilibrium moments with the surface-tension perturbation (CG3:2836-2851)
@@ -171,18 +176,16 @@ __global__ void __launch_bounds__(256, 3) cg_collide_fast_kernel(CgArgs a) {
   for (int k = 0; k < kQ; k++) {
     const bool odd = (k >= 3 && k <= 8) || k >= 16;
     float m = odd ? 0.f : (float)cg::mcoef(k, 0) * f0;
-    float fh = odd ? 0.f : (float)cg::mcoef(k, 0) * G0;
 #pragma unroll
     for (int i = 1; i <= 9; i++) {
       const int c = cg::mcoef(k, 2 * i - 1);
       if (c == 0) continue;
       m += (float)c * (odd ? dp[i] : sp[i]);
-      fh += (float)c * (odd ? gd[i] : gs[i]);
     }
     const bool cons = (k == 0 || k == 3 || k == 5 || k == 7);
     const bool visc = (k == 1 || k == 2 || (k >= 9 && k <= 15));
     const float S = cons ? 0.f : (visc ? s_v : s_o);
-    ml[k] = m - S * (m - meq[k]) + (1.f - 0.5f * S) * fh;
+    ml[k] = m - S * (m - meq[k]) + (1.f - 0.5f * S) * MG[k];
   }
 
   // back-transform by parity blocks
