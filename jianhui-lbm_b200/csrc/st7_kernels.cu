@@ -65,17 +65,20 @@ __global__ void st7_conc_kernel(St7Args a, double* __restrict__ out) {
 }
 
 // Initial state g = C0/6 (1 + 3 e.u), written through the inverse pull.
+// Initial populations g_k = C/6 (1 + 3 e_k.u) of `init` (ST7:1249-1327),
+// which the reference evaluates before it reads the velocity file (ST7:472-
+// 473), with the velocity array still zero: g_k = C/6.  Stored through the
+// inverse pull so that the first step pulls exactly these values.
 template <typename T>
 __global__ void st7_init_kernel(St7Args a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= a.n) return;
-  const T* __restrict__ u = static_cast<const T*>(a.u);
   const T C = static_cast<const T*>(a.c_given)[x];
   const size_t npad = (size_t)a.npad;
   T* __restrict__ g = static_cast<T*>(a.dst);
+  const T eu = T(0);
 #pragma unroll
   for (int q = 1; q < 7; q++) {
-    const T eu = T(cx(q)) * u[x] + T(cy(q)) * u[npad + x] + T(cz(q)) * u[2 * npad + x];
     const size_t s = a.table[(size_t)(q - 1) * npad + x] - npad;
     g[s] = T(1.0 / 6.0) * C * (T(1) + T(3) * eu);
   }

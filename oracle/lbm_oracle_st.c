@@ -4,18 +4,19 @@
  *
  * Restates Single_Phase_3D/Solute_Transport_MPI_Software_Spars_6V.cpp
  * ("ST7") for a fully periodic domain: `init` (ST7:1249-1327) sets
- * g_k = C/6 (1 + 3 e_k.u) for the six axis velocities e2 (ST7:130), and each
- * step is `collision` (ST7:1345-1617: BGK g -> g - (g - C/6 (1 + 3 e.u))/tau_s,
- * push streaming with halfway bounce-back LR, ST7:1475-1528) followed by
- * `comput_macro_variables` (ST7:1619-1633: C = sum_k g_k, k = 1..6).
+ * g_k = C/6 (1 + 3 e_k.u) for the six axis velocities e2 (ST7:130) with the
+ * velocity array as it is before the velocity file is read (main calls init
+ * at ST7:472 and Backup_input_v at :473), i.e. zero: g_k = C/6; each step is
+ * `collision` (ST7:1345-1617: BGK g -> g - (g - C/6 (1 + 3 e.u))/tau_s with
+ * the file's velocity, push streaming with halfway bounce-back LR,
+ * ST7:1475-1528) followed by `comput_macro_variables` (ST7:1619-1633:
+ * C = sum_k g_k, k = 1..6).
  *
- * The reference is decomposed in x-slabs and needs at least two MPI ranks
- * (rank 0 exchanges with rank+1), so it cannot run under a one-rank MPI
- * stand-in; this restatement is therefore pinned by the physics instead
- * (mass conservation, pure diffusion with variance 2 D t where
- * D = (tau_s - 1/2)/3, advection of the centroid at u), and the GPU kernel is
- * compared with it bit for bit.  Parity with the reference's own binary is
- * unpinned.
+ * Pinned bit for bit against the reference program itself, run as two ranks
+ * of its x-slab decomposition under the multi-process MPI stand-in
+ * (oracle/mpishim, oracle/_ref/ref_st7_slab; fixture tests/golden/st7_slab.npz),
+ * and by the physics (mass conservation, pure diffusion with variance 2 D t
+ * where D = (tau_s - 1/2)/3, advection of the centroid at u).
  *
  * Layout: ids 1..count in SP3 compaction order, g AoS [(count+1)*7] (slot 0
  * unused, as in the reference), u AoS [(count+1)*3], C [(count+1)].
@@ -34,14 +35,14 @@ double orc_st7_tau(double diffusivity) {
   return diffusivity / (c_s2 * dt) + 0.5;
 }
 
-void orc_st7_init(int count, const double* u, const double* c0, double* g, double* C) {
+void orc_st7_init(int count, const double* c0, double* g, double* C) {
   memset(g, 0, sizeof(double) * 7);
   C[0] = 0;
   for (int i = 1; i <= count; i++) {
     C[i] = c0[i];
     g[(long)i * 7 + 0] = 0.0;
     for (int lm = 1; lm < 7; lm++) {
-      const double eu = E7[lm][0] * u[(long)i * 3 + 0] + E7[lm][1] * u[(long)i * 3 + 1] + E7[lm][2] * u[(long)i * 3 + 2];
+      const double eu = 0.0;  /* the velocity array before the velocity file is read */
       g[(long)i * 7 + lm] = 1.0 / 6.0 * C[i] * (1 + 3 * eu);
     }
   }

@@ -24,6 +24,8 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# where the fixture generators read the reference's own sample files
+REFERENCE_ROOT = os.environ.get("LBM_REFERENCE_ROOT", "/root/reference")
 _I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _U8P = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
@@ -43,6 +45,45 @@ def _load(name):
     if not os.path.exists(path):
         build()
     return C.CDLL(path)
+
+
+def run_ranks(program, args, nranks, cwd, timeout=300.0):
+    """Runs a reference program compiled against the multi-process MPI
+    stand-in (mpishim/mpi.h) as `nranks` processes in `cwd`; returns their
+    exit codes.  Messages go through a fresh directory (under /dev/shm when it
+    exists); a rank still running after `timeout` seconds is killed by its pid."""
+    import shutil
+    import subprocess
+
+    base = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    msgdir = tempfile.mkdtemp(prefix="mpishim_", dir=base)
+    procs = []
+    try:
+        for r in range(nranks):
+            env = dict(os.environ, MPISHIM_RANK=str(r), MPISHIM_SIZE=str(nranks), MPISHIM_DIR=msgdir,
+                       MPISHIM_TIMEOUT=str(int(timeout)))
+            log = open(os.path.join(cwd, f"rank{r}.log"), "w")
+            procs.append(subprocess.Popen([program, *args], cwd=cwd, env=env, stdout=log, stderr=subprocess.STDOUT))
+        codes = []
+        for p in procs:
+            try:
+                codes.append(p.wait(timeout=timeout))
+            except subprocess.TimeoutExpired:
+                p.kill()
+                codes.append(p.wait())
+        return codes
+    finally:
+        for p in procs:
+            if p.poll() is None:
+                p.kill()
+        shutil.rmtree(msgdir, ignore_errors=True)
+
+
+def slab_program(name):
+    """Path of a slab-decomposed reference program in _ref/ (ref_sp_slab,
+    ref_st7_slab), or None when it was not built."""
+    path = os.path.join(HERE, "_ref", name)
+    return path if os.path.exists(path) else None
 
 
 def reference_available():
@@ -287,7 +328,7 @@ class SoluteRun:
         self.L = L
         L.orc_st7_tau.argtypes = [C.c_double]
         L.orc_st7_tau.restype = C.c_double
-        L.orc_st7_init.argtypes = [C.c_int, _F64P, _F64P, _F64P, _F64P]
+        L.orc_st7_init.argtypes = [C.c_int, _F64P, _F64P, _F64P]
         L.orc_st7_step.argtypes = [C.c_int, _I32P, _F64P, C.c_double, _F64P, _F64P, _F64P]
         R = Restatement()
         self.mask = np.ascontiguousarray(mask, dtype=np.uint8)
@@ -299,7 +340,7 @@ class SoluteRun:
         c0 = np.zeros(n + 1)
         c0[1:] = np.ascontiguousarray(c0_cells, dtype=np.float64).reshape(-1)[self.mask.reshape(-1) == 0]
         self.g, self.G, self.C = np.zeros((n + 1) * 7), np.zeros((n + 1) * 7), np.zeros(n + 1)
-        L.orc_st7_init(n, self.u, c0, self.g, self.C)
+        L.orc_st7_init(n, c0, self.g, self.C)
 
     def step(self, k=1):
         for _ in range(k):

@@ -2,7 +2,7 @@
 solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
 compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
 
-    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --bc]
+    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --bc | --st7]
 
 Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
@@ -11,6 +11,7 @@ random generator at test time):
   sp_outputs_bc.npz  the same with pressure faces on x (Sub_BC 2, in_BC 1)  (--outputs)
   cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
   sp_bc.npz     pressure/velocity boundaries, Sub_BC 0..3, see bc_fixture()  (--bc)
+  st7_slab.npz  the solute program at two ranks, see st7_fixture()  (--st7)
   sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
                 M^-1, f/u/rho after 20 steps, Error and Comput_Perm outputs
   sp_24.npz     24^3 spheres, 200 steps: compaction digest, u, rho, f digest,
@@ -247,9 +248,62 @@ def bc_fixture():
     print("sp_bc", len(bc_cases()), "cases")
 
 
+ST7_SHAPE, ST7_SEED, ST7_D, ST7_NRANKS = (16, 10, 8), 41, 0.005, 2
+
+
+def solute_input(**kv):
+    """INPUT file of the solute program: the reference's sample
+    Single_Phase_3D/INPUT_SOLUTE.dat (its first 51 lines, read at run time)
+    with some values replaced; keys are the 0-based line numbers."""
+    lines = open(os.path.join(oracle.REFERENCE_ROOT, "Single_Phase_3D", "INPUT_SOLUTE.dat")).read().splitlines()[:51]
+    for i, v in kv.items():
+        lines[int(i[1:])] = f"{v}\t\t:{lines[int(i[1:])].split(':', 1)[1]}"
+    return "\n".join(lines) + "\n"
+
+
+def st7_fixture(out=None):
+    """The reference's own slab programs at two ranks (multi-process MPI
+    stand-in): the slab single-phase program makes the flow of a 16x10x8
+    sphere pack and writes Velocity_for_solute_100.<rank>.bin; the solute
+    program (D = 0.005, initial concentration uniform in [0, 1) as float)
+    advects and diffuses for 61 steps and backs up the concentration every 20
+    steps.  Stored: mask, initial concentration, the velocity records (slab
+    order, ranks concatenated), rank sizes, and the concentration at steps
+    20, 40, 60 (slab order)."""
+    import tempfile
+
+    sp, st = oracle.slab_program("ref_sp_slab"), oracle.slab_program("ref_st7_slab")
+    if not (sp and st):
+        raise SystemExit("oracle/_ref/ref_sp_slab and ref_st7_slab are needed (make -C oracle ref)")
+    mask = G.overlapping_spheres(ST7_SHAPE, 0.6, 2.5, seed=ST7_SEED)
+    nx, ny, nz = ST7_SHAPE
+    c0 = np.random.default_rng(5).uniform(0, 1, mask.shape).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        G.write_ascii(os.path.join(d, "mask.dat"), mask)
+        flow = input_text(L1="mask.dat", L2=f"{nx} {ny} {nz}", L3=100, L18=50, L20=-1, L21=-1, L24="./", L32=-1,
+                          L34=100)
+        open(os.path.join(d, "INPUT.dat"), "w").write(flow)
+        assert oracle.run_ranks(sp, ["INPUT.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
+        with open(os.path.join(d, "phase.dat"), "w") as fh:
+            fh.write("\n".join(repr(float(v)) for v in c0.reshape(-1)) + "\n")
+        text = solute_input(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=60, L23=ST7_D, L28=20,
+                            L33="0 1000", L36="./st_", L45=20, L47=100)
+        open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
+        assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
+        vel = [np.fromfile(os.path.join(d, f"Velocity_for_solute_100.{r}.bin")) for r in range(ST7_NRANKS)]
+        conc = {m: np.concatenate([np.fromfile(os.path.join(d, f"st_LBM_checkpoint_psi_{m}.{r}.bin_input"))[1:]
+                                   for r in range(ST7_NRANKS)]) for m in (20, 40, 60)}
+    np.savez_compressed(out or os.path.join(HERE, "st7_slab.npz"), mask=pack(mask), shape=np.array(mask.shape), c0=c0,
+                        diffusivity=ST7_D, nranks=ST7_NRANKS, u_slab=np.concatenate(vel),
+                        rank_nodes=np.array([v.size // 3 for v in vel]), steps=np.array([20, 40, 60]),
+                        c20=conc[20], c40=conc[40], c60=conc[60], input_solute=np.frombuffer(text.encode(), np.uint8))
+    print("st7_slab", mask.shape, [v.size // 3 for v in vel])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--bc", action="store_true")
+    ap.add_argument("--st7", action="store_true")
     ap.add_argument("--cfg1", action="store_true")
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
@@ -263,6 +317,9 @@ def main():
         return
     if a.bc:
         bc_fixture()
+        return
+    if a.st7:
+        st7_fixture()
         return
     ref = oracle.ReferenceSP3()
     if a.cfg1:

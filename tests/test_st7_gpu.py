@@ -71,3 +71,30 @@ def test_velocity_file_round_trip_and_coupling(L, flow_case, tmp_path):
             a.step(40)
             b.step(40)
             assert np.array_equal(a.concentration(), b.concentration())
+
+
+def test_st7_gpu_matches_the_reference_program(L, tmp_path):
+    """FP64 against the solute program itself (two slab ranks, fixture
+    st7_slab.npz): the velocity is read from the slab-order record file the
+    reference reads, the concentration compared bit for bit at the reference's
+    backups (steps 20, 40, 60: 21, 41, 61 updates)."""
+    import os
+
+    from helpers import GOLDEN, unpack_mask
+
+    z = np.load(os.path.join(GOLDEN, "st7_slab.npz"))
+    mask = unpack_mask(z["mask"], z["shape"])
+    path = str(tmp_path / "Velocity_for_solute_100.bin")
+    z["u_slab"].tofile(path)  # the two ranks' records, concatenated: the one-rank slab file
+    u = L.read_velocity_for_solute(path, mask, order="slab")
+    k, j, i = np.nonzero(mask == 0)
+    nz, ny, nx = mask.shape
+    order = np.argsort(i * ny * nz + j * nz + k, kind="stable")
+    with L.Solute(mask, z["c0"].astype(np.float64), float(z["diffusivity"]), u_nodes=u, precision="f64") as s:
+        done = -1
+        for m in (20, 40, 60):
+            s.step(m - done)
+            done = m
+            want = np.zeros(s.count + 1)
+            want[1 + order] = z[f"c{m}"]
+            assert np.array_equal(s.concentration()[1:], want[1:]), m
