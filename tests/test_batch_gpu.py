@@ -81,11 +81,14 @@ def test_batch_reset_and_autotune_reproduce(L, masks):
         t = b.autotune(trial_steps=5)
         assert t["block"] in (128, 256, 512) and t["ordering"] in (0, 2) and t["mlups"] > 0
         r2 = b.run(tol=1e-4, check_every=50, max_steps=5000)
+        # the tuned layout may order the nodes differently: the per-node
+        # arithmetic is the same, the flux sums run in another order
         for a, c in zip(r1, r2):
-            assert a["steps"] == c["steps"] and a["perm"][0] == c["perm"][0]
+            assert a["steps"] == c["steps"]
+            np.testing.assert_allclose(c["perm"][0], a["perm"][0], rtol=1e-6)
         b.reset()
         r3 = b.run(tol=1e-4, check_every=50, max_steps=5000)
-        assert [x["perm"][0] for x in r3] == [x["perm"][0] for x in r1]
+        assert [x["perm"][0] for x in r3] == [x["perm"][0] for x in r2]
         info = b.info()
         assert info["node_steps"] == sum(x["steps"] * x["count"] for x in r3) and info["last_run_ms"] > 0
 
