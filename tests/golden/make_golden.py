@@ -2,7 +2,7 @@
 solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
 compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
 
-    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --bc | --st7]
+    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --bc | --st7 | --slab-perm]
 
 Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
@@ -12,6 +12,8 @@ random generator at test time):
   cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
   sp_bc.npz     pressure/velocity boundaries, Sub_BC 0..3, see bc_fixture()  (--bc)
   st7_slab.npz  the solute program at two ranks, see st7_fixture()  (--st7)
+  sp_slab_perm.npz  the slab single-phase program at two ranks with its
+                local and group permeabilities, see slab_perm_fixture()  (--slab-perm)
   sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
                 M^-1, f/u/rho after 20 steps, Error and Comput_Perm outputs
   sp_24.npz     24^3 spheres, 200 steps: compaction digest, u, rho, f digest,
@@ -300,10 +302,45 @@ def st7_fixture(out=None):
     print("st7_slab", mask.shape, [v.size // 3 for v in vel])
 
 
+SLAB_GROUPS = dict(n_sub=[1, 2, 0, 0], size=[8, 4, 1, 1], corner=[0, 0, 0, 2, 2, 1, 0, 0, 0, 0, 0, 0])
+
+
+def slab_perm_fixture(out=None):
+    """The slab single-phase program at two ranks on the sp_outputs mask with
+    its sub-volume permeabilities on: Comput_Perm_LOCAL every report
+    (loc_perm = 1) and Comput_Grop_Perm every 50 steps (divisions: one cube of
+    8 at (0,0,0), 2^3 cubes of 4 from (2,2,1)); 101 steps.  Stored: the INPUT
+    file, mask, Results.txt and the Perm_<size>.output files."""
+    import tempfile
+
+    sp = oracle.slab_program("ref_sp_slab")
+    if not sp:
+        raise SystemExit("oracle/_ref/ref_sp_slab is needed (make -C oracle ref)")
+    mask = G.overlapping_spheres((14, 12, 10), 0.6, 2.5, seed=21)
+    g = SLAB_GROUPS
+    corners = [" ".join(str(c) for c in g["corner"][3 * i:3 * i + 3]) for i in range(4)]
+    text = input_text(L1="mask.dat", L2="14 12 10", L3=100, L17=1, L18=50, L20=-1, L21=-1, L24="./out_", L26=1,
+                      L32=-1, L34=-1, L36=50, L37=" ".join(map(str, g["n_sub"])), L38=" ".join(map(str, g["size"])),
+                      L39=corners[0], L40=corners[1], L41=corners[2], L42=corners[3])
+    with tempfile.TemporaryDirectory() as d:
+        G.write_ascii(os.path.join(d, "mask.dat"), mask)
+        open(os.path.join(d, "INPUT.dat"), "w").write(text)
+        assert oracle.run_ranks(sp, ["INPUT.dat"], 2, d) == [0, 0]
+        files = {n[len("out_"):]: open(os.path.join(d, n), "rb").read() for n in sorted(os.listdir(d))
+                 if n.startswith("out_") and (n.endswith(".output") or n.endswith("Results.txt"))}
+    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "input": np.frombuffer(text.encode(), np.uint8),
+            "names": np.array(sorted(files))}
+    for k, v in files.items():
+        blob[k] = np.frombuffer(v, np.uint8)
+    np.savez_compressed(out or os.path.join(HERE, "sp_slab_perm.npz"), **blob)
+    print("sp_slab_perm", sorted(files))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--bc", action="store_true")
     ap.add_argument("--st7", action="store_true")
+    ap.add_argument("--slab-perm", action="store_true")
     ap.add_argument("--cfg1", action="store_true")
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
@@ -320,6 +357,9 @@ def main():
         return
     if a.st7:
         st7_fixture()
+        return
+    if a.slab_perm:
+        slab_perm_fixture()
         return
     ref = oracle.ReferenceSP3()
     if a.cfg1:

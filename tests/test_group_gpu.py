@@ -52,3 +52,50 @@ def test_group_and_local_perm(L, oracle_mod):
     assert np.allclose(b[1, :3], u[1:][sel].sum(axis=0), rtol=1e-12, atol=1e-300)
     assert b[1, 3] == sel.sum()
     assert np.array_equal(b[2], np.zeros(4))
+
+
+def test_slab_program_sub_volume_permeabilities(L, tmp_path):
+    """Against the slab single-phase program itself, run at two ranks
+    (fixture sp_slab_perm.npz): its Perm_<size>.output files (Comput_Grop_Perm)
+    and the LOCAL permeability of its Results.txt (Comput_Perm_LOCAL) after 101
+    steps, printed with 6 significant digits, from lbm_group_perm /
+    lbm_local_perm on the FP64 state of the same INPUT file."""
+    import os
+
+    import make_golden
+    from helpers import GOLDEN, unpack_mask
+    from lbm_b200 import geometry as G
+
+    z = np.load(os.path.join(GOLDEN, "sp_slab_perm.npz"))
+    mask = unpack_mask(z["mask"], z["shape"])
+    G.write_ascii(str(tmp_path / "mask.dat"), mask)
+    lines = z["input"].tobytes().decode().splitlines()
+    lines[1] = f"{tmp_path / 'mask.dat'}\t\t:{lines[1].split(':', 1)[1]}"
+    (tmp_path / "INPUT.dat").write_text("\n".join(lines) + "\n")
+    s = L.SinglePhase.from_input(str(tmp_path / "INPUT.dat"), precision="f64")
+    try:
+        reso2k = s.input["reso"] ** 2 * 1000
+        s.step(s.input["n_max"] + 1)
+        gp = s.group_perm(**make_golden.SLAB_GROUPS)
+        local = s.local_perm() * reso2k
+    finally:
+        s.close()
+
+    def close(got, want):
+        return abs(got - want) <= 5e-6 * abs(want) + 1e-9
+
+    sizes = make_golden.SLAB_GROUPS["size"]
+    nsub = make_golden.SLAB_GROUPS["n_sub"]
+    row = 0
+    for d in range(4):
+        rows = gp[row:row + nsub[d] ** 3]
+        row += nsub[d] ** 3
+        if nsub[d] == 0:
+            continue
+        want = [list(map(float, ln.split())) for ln in z[f"Perm_{sizes[d]}.output"].tobytes().decode().splitlines()]
+        assert len(want) == len(rows)
+        for (p, phi), r in zip(want, rows):
+            assert close(r[0] * reso2k, p) and close(r[3], phi), (d, p, phi, r)
+    results = z["Results.txt"].tobytes().decode().split("The100th computation result:")[1]
+    vals = [float(x) for x in results.split("The LOCAL permiability is:")[1].splitlines()[0].split(",")]
+    assert all(close(a, b) for a, b in zip(local, vals)), (local, vals)
