@@ -310,7 +310,7 @@ def run_batch(a):
     import lbm_b200
     from lbm_b200 import workloads as W
 
-    inst_all = W.config4_instances(64)
+    inst_all = W.config4_instances(a.instances)
     mine = shard(inst_all, world, rank, lambda x: float((x[0] == 0).sum()))
     inst = [inst_all[i] for i in mine]
     tol, every, cap = 1e-6, 100, 400000
@@ -336,7 +336,7 @@ def run_batch(a):
     dk = max(abs(r["perm"][0] - s["perm"][0]) / abs(s["perm"][0]) for r, s in zip(res, singles))
     line = {"metric": "perm solves/s (batched)", "value": len(inst_all) / t_batch, "unit": "solves/s",
             "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 sphere packs, edge log-U[48,160], porosity U[0.25,0.5], r=5, tau=0.8, "
+            "config": {"workload": f"{len(inst_all)} sphere packs, edge log-U[48,160], porosity U[0.25,0.5], r=5, tau=0.8, "
                                    "gx=1e-6, stop test 1e-6 per 100 steps", "seed": 404,
                        "ordering": tune["ordering"], "block": tune["block"]},
             "one_at_a_time": {"value": len(inst_all) / t_single, "unit": "solves/s", "wall_s": t_single},
@@ -511,6 +511,7 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve", "cg", "solute"],
                     help="cfg2 = the headline single-domain bench; batch / serve = configs 4 / 5")
     ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--instances", type=int, default=64, help="batch: number of config-4 solves")
     ap.add_argument("--rate", type=float, default=8.0)
     ap.add_argument("--pool-nodes", type=int, default=96 * 1024 * 1024)
     ap.add_argument("--fp64-sample", type=int, default=6)
