@@ -446,8 +446,9 @@ def run_cg(a):
         return 0
     (d32, ms32, n), (d64, ms64, _) = out["f32"], out["f64"]
     peak, peak_src = measured_peak()
-    # colour pass 2*19*4 + 18*4 + 3*4, collide pass 19*4 + 18*4 + 3*4 + 3*19*4 (FP32)
-    cg_bytes = (2 * 19 * 4 + 72 + 12) + (19 * 4 + 72 + 12 + 3 * 19 * 4)
+    # FP32: colour pass 18*4 (table) + 8*4 (colour record) + 3*4 (rho_r, rho_b, psi);
+    # collide pass 19*4 (f) + 18*4 (table) + 3*4 (psi, rho_r, rho_b) + 19*4 (f*) + 8*4 (record)
+    cg_bytes = (72 + 32 + 12) + (19 * 4 + 72 + 12 + 19 * 4 + 32)
     achieved = n * cg_bytes / (ms32 * 1e-3) / 1e9
     line = {"metric": "colour-gradient fluid MLUPS (FP32)", "value": n / (ms32 * 1e-3) / 1e6, "unit": "MLUPS",
             "n_gpus": world, "higher_is_better": True, "dtype": "f32", "data": "synthetic",

@@ -47,7 +47,7 @@ struct lbm_cg_handle {
   Geometry geo;
   double MI[kQ][kQ];
   CgParams cp{};
-  Dev f[2], gr, gb, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
+  Dev f[2], gr, gb, rec, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
   int cur = 0;
   int given = 1;
   long long step = 0;
@@ -72,6 +72,7 @@ CgArgs cg_args(lbm_cg_handle* h, int c, int given) {
   a.f_dst = h->f[1 - c].p;
   a.gr = h->gr.p;
   a.gb = h->gb.p;
+  a.rec = h->rec.p;
   a.table = h->table.as<int32_t>();
   a.corder = h->f64 ? h->corder.as<uint8_t>() : nullptr;
   a.n = h->geo.count;
@@ -235,8 +236,12 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
   const int n = g.count, npad = g.npad;
   const size_t s = h->s();
   for (auto& b : h->f) LBM_CUDA_TRY(b.alloc((size_t)kQ * npad * s));
-  LBM_CUDA_TRY(h->gr.alloc((size_t)kQ * npad * s));
-  LBM_CUDA_TRY(h->gb.alloc((size_t)kQ * npad * s));
+  if (h->f64) {
+    LBM_CUDA_TRY(h->gr.alloc((size_t)kQ * npad * s));
+    LBM_CUDA_TRY(h->gb.alloc((size_t)kQ * npad * s));
+  } else {
+    LBM_CUDA_TRY(h->rec.alloc((size_t)8 * npad * sizeof(float)));
+  }
   LBM_CUDA_TRY(h->table.alloc((size_t)18 * npad * sizeof(int32_t)));
   LBM_CUDA_TRY(h->psi.alloc((size_t)npad * s));
   LBM_CUDA_TRY(h->rho_r.alloc((size_t)npad * s));
@@ -285,8 +290,9 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
     LBM_CUDA_TRY(cudaMemcpyAsync(h->rho_b.p, c.data(), sizeof(float) * npad, cudaMemcpyHostToDevice, h->stream));
     LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   }
-  LBM_CUDA_TRY(cudaMemsetAsync(h->gr.p, 0, h->gr.bytes, h->stream));
-  LBM_CUDA_TRY(cudaMemsetAsync(h->gb.p, 0, h->gb.bytes, h->stream));
+  if (h->gr.p) LBM_CUDA_TRY(cudaMemsetAsync(h->gr.p, 0, h->gr.bytes, h->stream));
+  if (h->gb.p) LBM_CUDA_TRY(cudaMemsetAsync(h->gb.p, 0, h->gb.bytes, h->stream));
+  if (h->rec.p) LBM_CUDA_TRY(cudaMemsetAsync(h->rec.p, 0, h->rec.bytes, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   *out = h.release();
   return LBM_OK;

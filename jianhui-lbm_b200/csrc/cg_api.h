@@ -17,8 +17,9 @@ struct CgParams {
 struct CgArgs {
   const void* f_src;  // [19][npad] post-collision f of the previous step
   void* f_dst;
-  void* gr;           // [19][npad] recoloured red distributions (at their source node)
+  void* gr;           // [19][npad] recoloured red distributions (at their source node), FP64
   void* gb;
+  void* rec;          // FP32: [npad][8] per-node colour record (rho_r, rho_b, u, unit colour gradient)
   const int32_t* table;
   const uint8_t* corder;  // [19][npad] colour summation order (FP64), or null
   int n, npad;

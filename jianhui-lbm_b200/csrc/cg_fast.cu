@@ -40,7 +40,7 @@ cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st) {
   return cudaStreamSynchronize(st);  // the arrays are host temporaries
 }
 
-// FP32 collide pass: the operator of the FP64 kernel (CG3:2684-3505) with
+// FP32 collide pass: the operator of the FP64 kernel (CG3:2684-3351) with
 // the arithmetic arranged for the GPU: the 18 table entries are read once and
 // serve both the population pull and the neighbour psi of the colour
 // gradient; moments and the back-transform use the opposite-pair split, the
@@ -206,40 +206,70 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
     fd[(size_t)cg::row(2 * i) * npad + x] = h - g;
   }
 
-  // equilibrium colour distributions and recolouring (CG3:3472-3505)
-  const float uu = ux * ux + uy * uy + uz * uz;
-  const float base = 1.f - 1.5f * uu;
-  float* __restrict__ grp = static_cast<float*>(a.gr);
-  float* __restrict__ gbp = static_cast<float*>(a.gb);
+  // colour record of this node: the recoloured distributions it emits
+  // (CG3:3472-3505) are a function of these eight values, and the next
+  // colour pass recomputes each one where it is pulled instead of storing
+  // 2 x 19 of them
+  float4* __restrict__ rec = reinterpret_cast<float4*>(a.rec) + 2 * (size_t)x;
+  rec[0] = make_float4(rr, rb, ux, uy);
+  rec[1] = make_float4(uz, nx, ny, nz);
+}
+
+// FP32 colour pass (CG3:3472-3570 restated as a pull): rho_r(x), rho_b(x) =
+// sums of the recoloured distributions arriving at x, each recomputed from
+// the colour record of the node that emitted it.  Direction k of a node with
+// record (r, b, u, n), k in the opposite pair (a, a+1) with a odd:
+//   E_a = 1 + 3 e_a.u + 4.5 (e_a.u)^2 - 1.5 u.u,  E_{a+1} likewise with -e_a,
+//   cp  = min(w r E_a, w r E_{a+1}, w b E_a, w b E_{a+1}) (e_a.n),
+//   g_r,a = w r E_a + cp, g_r,a+1 = w r E_{a+1} - cp,
+//   g_b,a = w b E_a - cp, g_b,a+1 = w b E_{a+1} + cp
+// (n is the unit colour gradient, zero where the reference skips the
+// recolouring).  The pull reads storage row q of x from node m = x - e_q, or,
+// behind a wall, from x itself in the opposite direction (the other member
+// of the same pair).
+__global__ void __launch_bounds__(256) cg_colour_fast_kernel(CgArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  const float4* __restrict__ rec = reinterpret_cast<const float4*>(a.rec);
+  const int npad = a.npad;
+  float sr, sb;
   {
-    const float w0 = (float)weight(0);
-    grp[x] = w0 * rr * base;
-    gbp[x] = w0 * rb * base;
+    const float4 r0 = __ldg(rec + 2 * (size_t)x), r1 = __ldg(rec + 2 * (size_t)x + 1);
+    const float uu = r0.z * r0.z + r0.w * r0.w + r1.x * r1.x;
+    const float e0 = (float)weight(0) * (1.f - 1.5f * uu);
+    sr = r0.x * e0;
+    sb = r0.y * e0;
   }
 #pragma unroll
-  for (int i = 1; i <= 9; i++) {
-    const int ka = 2 * i - 1, kb = 2 * i;
+  for (int q = 1; q < kQ; q++) {
+    const int k = cg::of_row(q);
+    const int ka = (k % 2) ? k : k - 1;  // first member of the pair
+    const int32_t s = __ldg(a.table + (size_t)(q - 1) * npad + x);
+    const int32_t lo = q * npad;
+    const bool streamed = s >= lo && s < lo + npad;
+    const int m = streamed ? s - lo : x;
+    // member of the pair actually pulled: k itself when streamed, its opposite behind a wall
+    const bool first = ((k % 2) != 0) == streamed;
+    const float4 r0 = __ldg(rec + 2 * (size_t)m), r1 = __ldg(rec + 2 * (size_t)m + 1);
+    const float ux = r0.z, uy = r0.w, uz = r1.x;
     const float eu = (float)cg::ex(ka) * ux + (float)cg::ey(ka) * uy + (float)cg::ez(ka) * uz;
+    const float base = 1.f - 1.5f * (ux * ux + uy * uy + uz * uz) + 4.5f * eu * eu;
+    const float Ea = base + 3.f * eu, Eb = base - 3.f * eu;
     const float w = (float)weight(ka);
-    const float Ea = base + 3.f * eu + 4.5f * eu * eu, Eb = base - 3.f * eu + 4.5f * eu * eu;
-    float ra = w * rr * Ea, rbb = w * rr * Eb, ba = w * rb * Ea, bb = w * rb * Eb;
-    if (cc > 0.f) {
-      const float ef = (float)cg::ex(ka) * C0 + (float)cg::ey(ka) * C1 + (float)cg::ez(ka) * C2;
-      const float cp = fminf(fminf(ra, rbb), fminf(ba, bb)) * (ef * icc);
-      ra += cp;
-      rbb -= cp;
-      ba -= cp;
-      bb += cp;
-    }
-    grp[(size_t)cg::row(ka) * npad + x] = ra;
-    grp[(size_t)cg::row(kb) * npad + x] = rbb;
-    gbp[(size_t)cg::row(ka) * npad + x] = ba;
-    gbp[(size_t)cg::row(kb) * npad + x] = bb;
+    const float wr = w * r0.x, wb = w * r0.y;
+    const float ra = wr * Ea, rb_ = wr * Eb, ba = wb * Ea, bb = wb * Eb;
+    const float en = (float)cg::ex(ka) * r1.y + (float)cg::ey(ka) * r1.z + (float)cg::ez(ka) * r1.w;
+    const float cp = fminf(fminf(ra, rb_), fminf(ba, bb)) * en;
+    sr += first ? ra + cp : rb_ - cp;
+    sb += first ? ba - cp : bb + cp;
   }
+  static_cast<float*>(a.rho_r)[x] = sr;
+  static_cast<float*>(a.rho_b)[x] = sb;
+  static_cast<float*>(a.psi)[x] = (sr - sb) / (sr + sb);
 }
 
 cudaError_t cg_colour_f32(const CgArgs& a, cudaStream_t st) {
-  if (a.n > 0) cg_colour_kernel<false><<<(a.n + 255) / 256, 256, 0, st>>>(a);
+  if (a.n > 0) cg_colour_fast_kernel<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
