@@ -315,7 +315,7 @@ def run_batch(a):
     inst = [inst_all[i] for i in mine]
     tol, every, cap = 1e-6, 100, 400000
     with lbm_b200.Batch(inst, precision="f32", ordering="auto", block=0, device=local) as b:
-        tune = b.autotune(trial_steps=10)
+        tune = b.autotune(trial_steps=30)
         b.reset()
         barrier(pg)
         t0 = time.perf_counter()
