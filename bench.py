@@ -314,8 +314,10 @@ def run_batch(a):
     mine = shard(inst_all, world, rank, lambda x: float((x[0] == 0).sum()))
     inst = [inst_all[i] for i in mine]
     tol, every, cap = 1e-6, 100, 400000
-    with lbm_b200.Batch(inst, precision="f32", ordering="auto", block=0, device=local) as b:
-        tune = b.autotune(trial_steps=30)
+    fixed = a.batch_block > 0
+    with lbm_b200.Batch(inst, precision="f32", ordering="reference" if fixed else "auto",
+                        block=a.batch_block if fixed else 0, device=local) as b:
+        tune = {"ordering": 0, "block": a.batch_block} if fixed else b.autotune(trial_steps=30)
         b.reset()
         barrier(pg)
         t0 = time.perf_counter()
@@ -513,6 +515,7 @@ def main():
                     help="cfg2 = the headline single-domain bench; batch / serve = configs 4 / 5")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--instances", type=int, default=64, help="batch: number of config-4 solves")
+    ap.add_argument("--batch-block", type=int, default=0, help="batch: fixed block size, reference order (0 = autotune)")
     ap.add_argument("--rate", type=float, default=8.0)
     ap.add_argument("--pool-nodes", type=int, default=96 * 1024 * 1024)
     ap.add_argument("--fp64-sample", type=int, default=6)

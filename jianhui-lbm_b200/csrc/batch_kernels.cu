@@ -20,7 +20,7 @@
 namespace lbm {
 
 template <Store K, int BS>
-__global__ void __launch_bounds__(BS, 1024 / BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
+__global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
   using T = typename Traits<K>::T;
   using A = typename Traits<K>::A;
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
