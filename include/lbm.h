@@ -299,6 +299,7 @@ typedef struct lbm_cg_params {
   double flux_umax;        /* rel_perm_psi2: fluxes count nodes with |u| below this */
   int precision;           /* LBM_PREC_F64 (bit-exact) or LBM_PREC_F32 */
   int device;
+  int perdir;              /* PerDir 1..3: direction of the permeability change and of sd_l/sd_g */
 } lbm_cg_params;
 
 /* Comput_Perm (CG3:5116-5284) and Comput_Saturation (CG3:5286-5370). */
@@ -307,10 +308,17 @@ typedef struct lbm_cg_diag {
   double saturation;       /* share of pore nodes with psi >= 0 */
   double q_l[3], q_g[3];   /* phase fluxes (sum of u per phase) */
   double perm_l[3], perm_g[3];
-  double perm_rel_change;  /* liquid permeability along x, relative change */
+  double perm_rel_change;  /* liquid permeability along perdir, relative change */
   double u_ave;            /* |Q_l + Q_g| / (V * porosity) */
   double capillary;        /* u_ave * nu_l / cap_a */
   double mass;             /* sum rho */
+  /* Error (CG3:4683-4750) over all nodes, against u one step earlier */
+  double u_max;            /* max |u| */
+  double u_rel_change;     /* ||u - u_prev|| / (||u|| + 1e-30) */
+  double u_mean_speed;     /* sum |u| / (nx ny nz) */
+  /* Comput_Saturation's position sums (CG3:5300-5345): sum of psi * (coordinate
+   * along perdir) over nodes with psi >= 0 (sd_l) and psi < 0 (sd_g) */
+  double sd_l, sd_g;
 } lbm_cg_diag;
 
 typedef struct lbm_cg_handle lbm_cg_handle;

@@ -48,6 +48,9 @@ struct lbm_cg_handle {
   double MI[kQ][kQ];
   CgParams cp{};
   Dev f[2], gr, gb, rec, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
+  Dev u_prev, axis, partials2, result2;  // Error's u0 and the saturation position sums
+  bool uprev_valid = false;
+  int perdir = 1;
   int cur = 0;
   int given = 1;
   long long step = 0;
@@ -66,8 +69,9 @@ struct lbm_cg_handle {
 
 namespace {
 
-CgArgs cg_args(lbm_cg_handle* h, int c, int given) {
+CgArgs cg_args(lbm_cg_handle* h, int c, int given, bool write_u = false) {
   CgArgs a{};
+  a.u_out = write_u ? h->u_prev.p : nullptr;
   a.f_src = h->f[c].p;
   a.f_dst = h->f[1 - c].p;
   a.gr = h->gr.p;
@@ -85,8 +89,8 @@ CgArgs cg_args(lbm_cg_handle* h, int c, int given) {
   return a;
 }
 
-cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given) {
-  const CgArgs a = cg_args(h, c, given);
+cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u = false) {
+  const CgArgs a = cg_args(h, c, given, write_u);
   cudaError_t e = cudaSuccess;
   if (!given) e = h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream);
   if (e != cudaSuccess) return e;
@@ -155,7 +159,7 @@ lbm_status cg_check(lbm_cg_handle* h) {
 
 // Runs the colour pass (when the state is not the initial one) and the
 // diagnostics reduction; optional macro fields in internal order.
-lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double* u_out) {
+lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double* u_out, double* r2 = nullptr) {
   if (!h->given) {
     const CgArgs a = cg_args(h, h->cur, 0);
     LBM_CUDA_TRY(h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream));
@@ -176,9 +180,14 @@ lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double*
   ra.u_out = u_out;
   ra.partials = h->partials.as<double>();
   ra.result = h->result.as<double>();
+  ra.u_prev = (!h->given && h->uprev_valid) ? h->u_prev.p : nullptr;
+  ra.axis = h->axis.as<int32_t>();
+  ra.partials2 = h->partials2.as<double>();
+  ra.result2 = h->result2.as<double>();
   const int nb = reduce_blocks(h->geo.count);
   LBM_CUDA_TRY(h->f64 ? cg_reduce_f64(ra, nb, h->stream) : cg_reduce_f32(ra, nb, h->stream));
   LBM_CUDA_TRY(cudaMemcpyAsync(r, ra.result, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (r2) LBM_CUDA_TRY(cudaMemcpyAsync(r2, ra.result2, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return LBM_OK;
 }
@@ -249,6 +258,22 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
   LBM_CUDA_TRY(h->ref_of.alloc((size_t)n * sizeof(int32_t)));
   LBM_CUDA_TRY(h->partials.alloc((size_t)reduce_blocks(n) * 8 * sizeof(double)));
   LBM_CUDA_TRY(h->result.alloc(8 * sizeof(double)));
+  LBM_CUDA_TRY(h->partials2.alloc((size_t)reduce_blocks(n) * 8 * sizeof(double)));
+  LBM_CUDA_TRY(h->result2.alloc(8 * sizeof(double)));
+  LBM_CUDA_TRY(h->u_prev.alloc((size_t)3 * npad * s));
+  {
+    // coordinate of every node along perdir, for the saturation position sums
+    h->perdir = (p->perdir >= 1 && p->perdir <= 3) ? p->perdir : 1;
+    std::vector<int32_t> ax(npad, 0);
+    for (int x = 0; x < n; x++) {
+      const int c = g.coor[g.ref_of[x]];  // i*ny*nz + j*nz + k
+      const int i = c / (ny * nz), j = (c % (ny * nz)) / nz, k = c % nz;
+      ax[x] = h->perdir == 1 ? i : (h->perdir == 2 ? j : k);
+    }
+    LBM_CUDA_TRY(h->axis.alloc((size_t)npad * sizeof(int32_t)));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->axis.p, ax.data(), sizeof(int32_t) * npad, cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
   LBM_CUDA_TRY(cudaMemcpyAsync(h->table.p, g.src.data(), sizeof(int32_t) * 18 * (size_t)npad,
                                cudaMemcpyHostToDevice, h->stream));
   LBM_CUDA_TRY(cudaMemcpyAsync(h->ref_of.p, g.ref_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice,
@@ -304,7 +329,7 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   if (nsteps < 0) return fail(LBM_ERR_ARG, "lbm_cg_step: negative step count");
   if (nsteps == 0) return LBM_OK;
   int left = nsteps;
-  if (left - (h->given ? 1 : 0) >= kCgGraphSteps) {
+  if (left - (h->given ? 1 : 0) - 1 >= kCgGraphSteps) {
     const int c0 = h->cur;
     for (int c = 0; c < 2; c++)
       if ((st = cg_graph(h, c)) != LBM_OK) return st;
@@ -312,20 +337,22 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   }
   LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
   if (h->given) {
-    LBM_CUDA_TRY(one_cg_step(h, h->cur, 1));
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, 1, left == 1));
     h->cur = 1 - h->cur;
     h->given = 0;
     left--;
   }
-  while (left >= kCgGraphSteps) {
+  while (left - 1 >= kCgGraphSteps) {
     LBM_CUDA_TRY(cudaGraphLaunch(h->graph[h->cur], h->stream));
     left -= kCgGraphSteps;  // even chain: parity unchanged
   }
+  // the last step also writes its pre-collision u (Error's u0 of the next report)
   while (left > 0) {
-    LBM_CUDA_TRY(one_cg_step(h, h->cur, 0));
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, 0, left == 1));
     h->cur = 1 - h->cur;
     left--;
   }
+  h->uprev_valid = true;
   LBM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
   LBM_CUDA_TRY(cudaEventSynchronize(h->ev1));
   float ms = 0;
@@ -339,8 +366,8 @@ lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out) {
   lbm_status st = cg_check(h);
   if (st != LBM_OK) return st;
   if (!out) return fail(LBM_ERR_ARG, "lbm_cg_reduce: null output");
-  double r[8];
-  if ((st = cg_reduce_raw(h, r, nullptr, nullptr)) != LBM_OK) return st;
+  double r[8], r2[8];
+  if ((st = cg_reduce_raw(h, r, nullptr, nullptr, r2)) != LBM_OK) return st;
   const Geometry& g = h->geo;
   const double V = (double)g.nx * g.ny * g.nz, phi = g.porosity, dp = 0.0;
   const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
@@ -357,8 +384,14 @@ lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out) {
   out->capillary = std::sqrt(vx * vx + vy * vy + vz * vz) / phi * h->prm.nu_l / h->prm.cap_a;
   out->saturation = r[3] / (V * phi);  // CG3:5361
   out->mass = r[7];
-  out->perm_rel_change = (out->perm_l[0] - h->perm_prev) / h->perm_prev;
-  h->perm_prev = out->perm_l[0];
+  const int dir = h->perdir - 1;
+  out->perm_rel_change = (out->perm_l[dir] - h->perm_prev) / h->perm_prev;  // CG3:5235-5246
+  h->perm_prev = out->perm_l[dir];
+  out->u_max = std::sqrt(r2[3]);                                         // CG3:4709-4745
+  out->u_rel_change = std::sqrt(r2[0]) / (std::sqrt(r2[1]) + 1e-30);
+  out->u_mean_speed = r2[2] / V;
+  out->sd_l = r2[4];
+  out->sd_g = r2[5];
   return LBM_OK;
 }
 

@@ -28,6 +28,7 @@ struct CgArgs {
   void* rho_b;
   int given;          // first step after init: rho = 1, u = 0
   CgParams p;
+  void* u_out;        // [3][npad] this step's pre-collision u, or null (Error's u0)
 };
 
 struct CgReduceArgs {
@@ -42,6 +43,11 @@ struct CgReduceArgs {
   double* u_out;    // optional [3][npad]
   double* partials;
   double* result;   // Ql(3), count(psi >= 0), Qg(3), mass
+  // Error and the saturation position sums: null u_prev -> no change
+  const void* u_prev;      // [3][npad]
+  const int32_t* axis;     // [npad] coordinate along perdir, or null
+  double* partials2;
+  double* result2;         // |du|^2, |u|^2, |u|, max |u|^2, sd_l, sd_g, 0, 0
 };
 
 cudaError_t cg_set_mi_f64(const double* mi, cudaStream_t st);

@@ -30,6 +30,7 @@ cudaError_t cg_collide_f64(const CgArgs& a, cudaStream_t st) {
 cudaError_t cg_reduce_f64(const CgReduceArgs& a, int nblocks, cudaStream_t st) {
   cg_reduce_kernel<true><<<nblocks, 256, 0, st>>>(a);
   cg_reduce_final_kernel<<<1, 1024, 0, st>>>(a.partials, nblocks, a.result);
+  if (a.partials2) reduce_final_kernel<<<1, 1024, 0, st>>>(a.partials2, nblocks, a.result2);
   return cudaGetLastError();
 }
 

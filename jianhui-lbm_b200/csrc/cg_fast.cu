@@ -114,6 +114,12 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
     uy = (jy + 0.5f * gy) * ir;
     uz = (jz + 0.5f * gz) * ir;
   }
+  if (a.u_out) {
+    float* uo = static_cast<float*>(a.u_out);
+    uo[x] = ux;
+    uo[(size_t)npad + x] = uy;
+    uo[2 * (size_t)npad + x] = uz;
+  }
 
   const float* __restrict__ rrp = static_cast<const float*>(a.rho_r);
   const float* __restrict__ rbp = static_cast<const float*>(a.rho_b);
@@ -305,6 +311,7 @@ cudaError_t cg_export_f(bool f64, const void* f, const int32_t* table, const int
 cudaError_t cg_reduce_f32(const CgReduceArgs& a, int nblocks, cudaStream_t st) {
   cg_reduce_kernel<false><<<nblocks, 256, 0, st>>>(a);
   cg_reduce_final_kernel<<<1, 1024, 0, st>>>(a.partials, nblocks, a.result);
+  if (a.partials2) reduce_final_kernel<<<1, 1024, 0, st>>>(a.partials2, nblocks, a.result2);
   return cudaGetLastError();
 }
 

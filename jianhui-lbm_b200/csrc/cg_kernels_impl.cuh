@@ -91,6 +91,12 @@ __global__ void __launch_bounds__(256) cg_collide_kernel(CgArgs a) {
     uz = (sz + T(1.0 * a.p.g[2]) / T(2)) / rho;
   }
   if (!FAITHFUL && a.given) drho = T(0);
+  if (a.u_out) {
+    T* uo = static_cast<T*>(a.u_out);
+    uo[x] = ux;
+    uo[(size_t)a.npad + x] = uy;
+    uo[2 * (size_t)a.npad + x] = uz;
+  }
 
   // colour gradient over x + e_t, solid neighbours at psi_solid (CG3:2684-2712)
   const T psi_x = psi[x];
@@ -254,8 +260,10 @@ __global__ void __launch_bounds__(256) cg_reduce_kernel(CgReduceArgs a) {
   using T = typename CgT<FAITHFUL>::T;
   __shared__ double smem[8 * 32];
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc2[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Error (CG3:4683-4750) and saturation position sums
   const T* __restrict__ fs = static_cast<const T*>(a.f);
   const T* __restrict__ psi = static_cast<const T*>(a.psi);
+  const T* __restrict__ up = static_cast<const T*>(a.u_prev);
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.n; x += gridDim.x * blockDim.x) {
     T rho, ux, uy, uz;
     if (a.given) {
@@ -305,8 +313,32 @@ __global__ void __launch_bounds__(256) cg_reduce_kernel(CgReduceArgs a) {
     }
     if (ps >= 0) acc[3] += 1.0;  // Comput_Saturation counts psi >= 0 (CG3:5319)
     acc[7] += (double)rho;
+    if (a.partials2) {
+      double px = dx, py = dy, pz = dz;
+      if (up) {
+        px = up[x];
+        py = up[(size_t)a.npad + x];
+        pz = up[2 * (size_t)a.npad + x];
+      }
+      const double u2 = dx * dx + dy * dy + dz * dz;
+      acc2[0] += (dx - px) * (dx - px) + (dy - py) * (dy - py) + (dz - pz) * (dz - pz);
+      acc2[1] += u2;
+      acc2[2] += sqrt(u2);
+      acc2[3] = fmax(acc2[3], u2);
+      if (a.axis) {
+        const double sdir = (double)a.axis[x];
+        if (ps >= 0)
+          acc2[4] += ps * sdir;
+        else
+          acc2[5] += ps * sdir;
+      }
+    }
   }
   block_reduce8<-1>(acc, a.partials + (size_t)blockIdx.x * 8, smem);
+  if (a.partials2) {
+    __syncthreads();  // smem is reused
+    block_reduce8<3>(acc2, a.partials2 + (size_t)blockIdx.x * 8, smem);
+  }
 }
 
 // Fixed-order sum of the per-block partials (all slots are sums).

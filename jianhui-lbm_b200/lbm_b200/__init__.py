@@ -143,14 +143,16 @@ class ServerResult(C.Structure):
 class CGParams(C.Structure):
     _fields_ = [("nu_l", C.c_double), ("nu_g", C.c_double), ("psi_solid", C.c_double), ("cap_a", C.c_double),
                 ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double), ("body_force_phase", C.c_int),
-                ("flux_psi", C.c_double), ("flux_umax", C.c_double), ("precision", C.c_int), ("device", C.c_int)]
+                ("flux_psi", C.c_double), ("flux_umax", C.c_double), ("precision", C.c_int), ("device", C.c_int),
+                ("perdir", C.c_int)]
 
 
 class CGDiag(C.Structure):
     _fields_ = [("step", C.c_longlong), ("saturation", C.c_double), ("q_l", C.c_double * 3),
                 ("q_g", C.c_double * 3), ("perm_l", C.c_double * 3), ("perm_g", C.c_double * 3),
                 ("perm_rel_change", C.c_double), ("u_ave", C.c_double), ("capillary", C.c_double),
-                ("mass", C.c_double)]
+                ("mass", C.c_double), ("u_max", C.c_double), ("u_rel_change", C.c_double),
+                ("u_mean_speed", C.c_double), ("sd_l", C.c_double), ("sd_g", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -347,12 +349,12 @@ class ColourGradient:
     ``psi`` holds the initial phase per cell, (nz, ny, nx), +1 = component r."""
 
     def __init__(self, mask, psi, nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0),
-                 body_force_phase=-1, flux_psi=0.99, flux_umax=0.01, precision="f32", device=0):
+                 body_force_phase=-1, flux_psi=0.99, flux_umax=0.01, precision="f32", device=0, perdir=1):
         m = np.ascontiguousarray(mask, dtype=np.uint8)
         nz, ny, nx = m.shape
         p = CGParams(float(nu_l), float(nu_g), float(psi_solid), float(cap_a), float(g[0]), float(g[1]), float(g[2]),
                      int(body_force_phase), float(flux_psi), float(flux_umax),
-                     PRECISIONS[precision] if isinstance(precision, str) else int(precision), int(device))
+                     PRECISIONS[precision] if isinstance(precision, str) else int(precision), int(device), int(perdir))
         h = C.c_void_p()
         _check(lib().lbm_cg_create(C.byref(p), m.reshape(-1), np.ascontiguousarray(psi, dtype=np.float64).reshape(-1),
                                    nx, ny, nz, C.byref(h)))
