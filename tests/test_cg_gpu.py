@@ -88,3 +88,35 @@ def test_cg_fp64_matches_oracle_over_longer_run(L, oracle_mod):
     assert np.array_equal(f, rd["f"])
     for k in ("u", "psi", "rho_r", "rho_b"):
         assert np.array_equal(d[k], rd[k]), k
+
+
+def test_cg_diag_error_and_position_sums(L, oracle_mod):
+    """Error's u_max / relative change / mean speed (CG3:4683-4750) and the saturation
+    position sums Sd_l, Sd_g (CG3:5286-5400) from the FP64 kernels against the
+    oracle's u (this step) and u0 (the step before), summed in double on the host."""
+    from lbm_b200 import geometry as G
+
+    mask = G.random_cylinders((20, 18, 16), 0.6, 2.0, seed=61)
+    psi = G.blob_phase_field(mask, seed=62, saturation=0.5)
+    kw = dict(nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(0.0, 1e-5, 0.0), body_force_phase=-1,
+              flux_psi=0.99, flux_umax=0.01)
+    ref = oracle_mod.ColourGradientRun(mask, psi, **kw)
+    ref.step(40)
+    u = ref.u.reshape(-1, 3)[1:]
+    u0 = ref.u0.reshape(-1, 3)[1:]
+    ps = ref.psi[1:]
+    zyx = np.nonzero(mask.reshape(mask.shape) == 0)
+    V = mask.size
+    for perdir in (1, 2, 3):
+        coord = zyx[3 - perdir]
+        with L.ColourGradient(mask, psi, precision="f64", perdir=perdir, **kw) as s:
+            s.step(25)
+            s.step(15)
+            r = s.reduce()
+        u2 = (u * u).sum(axis=1)
+        np.testing.assert_allclose(r["u_max"], np.sqrt(u2.max()), rtol=1e-13)
+        np.testing.assert_allclose(r["u_rel_change"],
+                                   np.sqrt(((u - u0) ** 2).sum()) / (np.sqrt(u2.sum()) + 1e-30), rtol=1e-9)
+        np.testing.assert_allclose(r["u_mean_speed"], np.sqrt(u2).sum() / V, rtol=1e-12)
+        np.testing.assert_allclose(r["sd_l"], (ps * coord)[ps >= 0].sum(), rtol=1e-12)
+        np.testing.assert_allclose(r["sd_g"], (ps * coord)[ps < 0].sum(), rtol=1e-12)
