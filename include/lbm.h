@@ -339,6 +339,110 @@ LBM_API lbm_status lbm_cg_info(lbm_cg_handle* h, int* count, double* porosity, l
                                double* last_step_ms);
 LBM_API void lbm_cg_destroy(lbm_cg_handle* h);
 
+/* Parameter changes between steps (the reference's gxs / CapA updates).
+ * timing LBM_CG_FORCE_BEFORE_MACRO: the new force also enters the macro step
+ * of the last step taken (pressure_bodyforce_change, CG3:1252-1370, runs
+ * between collision and comput_macro_variables); LBM_CG_FORCE_BEFORE_COLLISION:
+ * the last step's macro keeps the old force and the next collision uses the
+ * new one (the stabiliser's switch at stab_time, CG3:851-852). */
+#define LBM_CG_FORCE_BEFORE_MACRO 0
+#define LBM_CG_FORCE_BEFORE_COLLISION 1
+LBM_API lbm_status lbm_cg_set_body_force(lbm_cg_handle* h, double gx, double gy, double gz, int timing);
+/* rel_perm_ift's surface-tension change (CG3:892-893) */
+LBM_API lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a);
+/* Comput_Perm / Comput_Saturation window (CG3:5156-5227, 5307-5361):
+ * window = per_xn, per_xp, per_yn, per_yp, per_zn, per_zp; the fluxes and the
+ * saturation count are divided by its volume, and the porosity (lbm_cg_info,
+ * u_ave, capillary number, saturation) becomes the window's pore fraction
+ * (CG3:1835-1851).  restrict_nodes = 1 also limits
+ * the sums to the nodes inside it (the reference does so when one of
+ * par_per_x/y/z equals 1).  All -1 = whole box. */
+LBM_API lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict_nodes);
+/* Restores a state like Backup_init (CG3:5438-5690): f [(count+1)*19] in the
+ * CG velocity order, psi, rho_r, rho_b [(count+1)], reference id order (row 0
+ * ignored).  The next step takes psi / rho_r / rho_b as given and rho, u from f. */
+LBM_API lbm_status lbm_cg_set_state(lbm_cg_handle* h, const double* f, const double* psi, const double* rho_r,
+                                    const double* rho_b);
+
+/* INPUT file of the colour-gradient program (CG3:372-474, field order and
+ * types kept; nx, ny, nz as written in the file = NX+1, ...). */
+typedef struct lbm_cg_input {
+  char geometry_file[256];
+  char phase_file[256];
+  int nx, ny, nz;
+  int n_max;
+  double reso;
+  int in_bc;
+  int in_psi_bc;
+  double gx, gy, gz;
+  int pre_xp; double p_xp; int pre_xn; double p_xn;
+  int pre_yp; double p_yp; int pre_yn; double p_yn;
+  int pre_zp; double p_zp; int pre_zn; double p_zn;
+  int vel_xp; double v_xp; int vel_xn; double v_xn;
+  int vel_yp; double v_yp; int vel_yn; double v_yn;
+  int vel_zp; double v_zp; int vel_zn; double v_zn;
+  int psi_xp, psi_xn, psi_yp, psi_yn, psi_zp, psi_zn;
+  double nu_l, nu_g;
+  double contact_angle;          /* ContactAngle_parameter = psi_solid */
+  double cap_a;
+  double inivx, inivy, inivz;
+  double permeability;           /* single-phase permeability (mD) for relative values */
+  int wr_per, perdir, fre_re, out_mode, fre_ve, fre_de, fre_psi;
+  int lattice_v; double dx_input, dt_input;
+  char output_path[256];
+  int sub_bc;
+  int stab, stab_time;
+  double ini_sat;
+  int ini_buf;
+  double rel_perm_psi, rel_perm_psi2;
+  int par_per_x, par_per_y, par_per_z;
+  int per_xp, per_xn, per_yp, per_yn, per_zp, per_zn;
+  int fre_backup, mode_backup_ini;
+  int decbin;
+  int pressure_change, pre_chan_pb;
+  int pre_chan[5];
+  double pre_chan_pn[5], pre_chan_pp[5], pre_chan_f[5];
+  int bodyforce_apply;
+  int pressure_change2, pre_chan_pb2, interval_pre;
+  double pre_chan_pns, pre_chan_pps, pre_chan_fs;
+  int chan_no, sat_cri;
+  double sat_cri_d;
+  int least_square, num_least_square;
+  int rel_perm_id_dir, rel_perm_chan_num;
+  int rel_perm_ift; double vary_ift;
+  int input_dynamic, update_fre;
+  int mix_psi_thickness; double protion_w; int zero_sigma_thickness;
+} lbm_cg_input;
+
+LBM_API lbm_status lbm_read_cg_input(const char* path, lbm_cg_input* out);
+/* Phase file (CG3:2130-2150): nx*ny*nz whitespace-separated numbers, x
+ * fastest, each read as float; out [nz][ny][nx]. */
+LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, double* out);
+/* Reads the INPUT file, the geometry and the phase file and creates the
+ * solver with the file's physics: psi_solid = ContactAngle_parameter, the
+ * force off until stab_time when the stabiliser is on, the flux thresholds
+ * rel_perm_psi / rel_perm_psi2, PerDir and the permeability window.  Options
+ * outside a fully periodic run with the phase read from file (pressure or
+ * velocity faces, psi faces, random or mixture initialisation, a
+ * self-defined lattice velocity, a non-zero initial velocity, drainage /
+ * imbibition control, capillary-pressure stepping, dynamic input) are
+ * rejected with LBM_ERR_ARG naming the field. */
+LBM_API lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
+                                            lbm_cg_input* parsed_out);
+
+/* Output writers of the colour-gradient program: velocity and density VTK
+ * (output_velocity CG3:4840-4931, output_density CG3:4933-5020; the
+ * single-phase formats), the phase VTK (output_psi CG3:5022-5114: title lines
+ * given by the caller, values at 2 significant digits, 0 on solids) and the
+ * checkpoint <prefix>LBM_checkpoint_{velocity,rho,psi,f,rhor,rhob}_<m>.0.bin_input
+ * (Backup CG3:5693-5745; Backup_init CG3:5438-5690 reads it back). */
+LBM_API lbm_status lbm_cg_write_vtk_velocity(lbm_cg_handle* h, const char* path);
+LBM_API lbm_status lbm_cg_write_vtk_density(lbm_cg_handle* h, const char* path);
+LBM_API lbm_status lbm_cg_write_vtk_psi(lbm_cg_handle* h, const char* path, const char* version_suffix,
+                                        const char* title);
+LBM_API lbm_status lbm_cg_write_checkpoint(lbm_cg_handle* h, const char* prefix, long long m);
+LBM_API lbm_status lbm_cg_read_checkpoint(lbm_cg_handle* h, const char* prefix, long long m);
+
 /* --------------------------------------------- D3Q7 solute (passive scalar) */
 
 typedef struct lbm_st7_params {

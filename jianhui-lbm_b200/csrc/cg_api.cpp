@@ -10,6 +10,11 @@
 #include "cg_basis.h"
 
 namespace lbm {
+
+lbm_status read_cg_input_file(const char* path, lbm_cg_input* o);
+lbm_status read_phase_file(const char* path, int nx, int ny, int nz, double* out);
+lbm_status read_mask_file(const char* path, int nx, int ny, int nz, int decbin, uint8_t* mask);
+
 namespace {
 
 struct Dev {
@@ -49,14 +54,20 @@ struct lbm_cg_handle {
   CgParams cp{};
   Dev f[2], gr, gb, rec, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
   Dev u_prev, axis, partials2, result2;  // Error's u0 and the saturation position sums
+  Dev win;                                // permeability window flags, or none
+  long long window_volume = 0;            // divisor of the fluxes and the saturation
   bool uprev_valid = false;
   int perdir = 1;
   int cur = 0;
+  // 1: initial state (rho = 1, u = 0, psi / rho_r / rho_b given);
+  // 2: restored state (psi / rho_r / rho_b given, rho and u from f);
+  // 0: running (the colour pass recomputes psi / rho_r / rho_b)
   int given = 1;
   long long step = 0;
   double perm_prev = 0.0;
   double last_ms = 0.0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  CgParams graph_cp{};  // parameters the graphs were captured with
   ~lbm_cg_handle() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
@@ -84,7 +95,7 @@ CgArgs cg_args(lbm_cg_handle* h, int c, int given, bool write_u = false) {
   a.psi = h->psi.p;
   a.rho_r = h->rho_r.p;
   a.rho_b = h->rho_b.p;
-  a.given = given;
+  a.given = given == 1;
   a.p = h->cp;
   return a;
 }
@@ -97,8 +108,31 @@ cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u = false
   return h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
 }
 
+bool same_params(const CgParams& a, const CgParams& b) {
+  bool same = a.psi_solid == b.psi_solid && a.cap_a == b.cap_a && a.body_force_phase == b.body_force_phase &&
+              a.flux_psi == b.flux_psi;
+  for (int d = 0; d < 3; d++) same = same && a.g[d] == b.g[d] && a.gm[d] == b.gm[d];
+  return same;
+}
+
+void drop_graphs(lbm_cg_handle* h) {
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// Chains of kCgGraphSteps running steps, captured with the steady parameters
+// (gm = g); a parameter change drops them.
 lbm_status cg_graph(lbm_cg_handle* h, int c0) {
+  CgParams steady = h->cp;
+  for (int d = 0; d < 3; d++) steady.gm[d] = steady.g[d];
+  if (!same_params(steady, h->graph_cp)) drop_graphs(h);
   if (h->graph[c0]) return LBM_OK;
+  h->graph_cp = steady;
+  const CgParams saved = h->cp;
+  h->cp = steady;
   cudaGraph_t g = nullptr;
   LBM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t err = cudaSuccess;
@@ -107,6 +141,7 @@ lbm_status cg_graph(lbm_cg_handle* h, int c0) {
     err = one_cg_step(h, c, 0);
     c = 1 - c;
   }
+  h->cp = saved;
   const cudaError_t end = cudaStreamEndCapture(h->stream, &g);
   if (err != cudaSuccess || end != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
@@ -170,10 +205,8 @@ lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double*
   ra.psi = h->psi.p;
   ra.n = h->geo.count;
   ra.npad = h->geo.npad;
-  ra.given = h->given;
-  ra.g[0] = h->prm.gx;
-  ra.g[1] = h->prm.gy;
-  ra.g[2] = h->prm.gz;
+  ra.given = h->given == 1;
+  for (int d = 0; d < 3; d++) ra.g[d] = h->cp.gm[d];  // the pending macro step's force
   ra.flux_psi = h->prm.flux_psi;
   ra.flux_umax = h->prm.flux_umax;
   ra.rho_out = rho_out;
@@ -184,6 +217,7 @@ lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double*
   ra.axis = h->axis.as<int32_t>();
   ra.partials2 = h->partials2.as<double>();
   ra.result2 = h->result2.as<double>();
+  ra.win = h->win.as<uint8_t>();
   const int nb = reduce_blocks(h->geo.count);
   LBM_CUDA_TRY(h->f64 ? cg_reduce_f64(ra, nb, h->stream) : cg_reduce_f32(ra, nb, h->stream));
   LBM_CUDA_TRY(cudaMemcpyAsync(r, ra.result, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -227,9 +261,10 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
   CgParams& cp = h->cp;
   cp.psi_solid = p->psi_solid;
   cp.cap_a = p->cap_a;
-  cp.g[0] = p->gx;
-  cp.g[1] = p->gy;
-  cp.g[2] = p->gz;
+  cp.g[0] = cp.gm[0] = p->gx;
+  cp.g[1] = cp.gm[1] = p->gy;
+  cp.g[2] = cp.gm[2] = p->gz;
+  h->window_volume = (long long)nx * ny * nz;
   cp.body_force_phase = p->body_force_phase;
   cp.flux_psi = p->flux_psi;
   const double c_s2 = 1.0 * 1.0 / 3, dt = 1.0;
@@ -329,17 +364,22 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   if (nsteps < 0) return fail(LBM_ERR_ARG, "lbm_cg_step: negative step count");
   if (nsteps == 0) return LBM_OK;
   int left = nsteps;
-  if (left - (h->given ? 1 : 0) - 1 >= kCgGraphSteps) {
+  // the first step runs alone after init or restore, and when a force change
+  // falls between the pending macro step and the next collision
+  bool special = h->given != 0;
+  for (int d = 0; d < 3; d++) special = special || h->cp.gm[d] != h->cp.g[d];
+  if (left - (special ? 1 : 0) - 1 >= kCgGraphSteps) {
     const int c0 = h->cur;
     for (int c = 0; c < 2; c++)
       if ((st = cg_graph(h, c)) != LBM_OK) return st;
     h->cur = c0;
   }
   LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
-  if (h->given) {
-    LBM_CUDA_TRY(one_cg_step(h, h->cur, 1, left == 1));
+  if (special) {
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, h->given, left == 1));
     h->cur = 1 - h->cur;
     h->given = 0;
+    for (int d = 0; d < 3; d++) h->cp.gm[d] = h->cp.g[d];
     left--;
   }
   while (left - 1 >= kCgGraphSteps) {
@@ -369,20 +409,22 @@ lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out) {
   double r[8], r2[8];
   if ((st = cg_reduce_raw(h, r, nullptr, nullptr, r2)) != LBM_OK) return st;
   const Geometry& g = h->geo;
-  const double V = (double)g.nx * g.ny * g.nz, phi = g.porosity, dp = 0.0;
-  const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
+  // fluxes and saturation over the window volume, Error over the box; the
+  // porosity is the window's pore fraction (CG3:1851, 5217-5227, 5361)
+  const double V = (double)g.nx * g.ny * g.nz, Vw = (double)h->window_volume, phi = g.porosity, dp = 0.0;
+  const double* gg = h->cp.gm;  // gxs when the macro step ran
   std::memset(out, 0, sizeof(*out));
   out->step = h->step;
   for (int d = 0; d < 3; d++) {
     out->q_l[d] = r[d];
     out->q_g[d] = r[4 + d];
-    out->perm_l[d] = r[d] / V * h->prm.nu_l / (gg[d] + dp);      // CG3:5217-5222
-    out->perm_g[d] = r[4 + d] / V * h->prm.nu_g / (gg[d] + dp);
+    out->perm_l[d] = r[d] / Vw * h->prm.nu_l / (gg[d] + dp);      // CG3:5217-5222
+    out->perm_g[d] = r[4 + d] / Vw * h->prm.nu_g / (gg[d] + dp);
   }
-  const double vx = (r[0] + r[4]) / V, vy = (r[1] + r[5]) / V, vz = (r[2] + r[6]) / V;
+  const double vx = (r[0] + r[4]) / Vw, vy = (r[1] + r[5]) / Vw, vz = (r[2] + r[6]) / Vw;
   out->u_ave = std::sqrt((vx / phi) * (vx / phi) + (vy / phi) * (vy / phi) + (vz / phi) * (vz / phi));
-  out->capillary = std::sqrt(vx * vx + vy * vy + vz * vz) / phi * h->prm.nu_l / h->prm.cap_a;
-  out->saturation = r[3] / (V * phi);  // CG3:5361
+  out->capillary = std::sqrt(vx * vx + vy * vy + vz * vz) / phi * h->prm.nu_l / h->cp.cap_a;
+  out->saturation = r[3] / (Vw * phi);  // CG3:5361
   out->mass = r[7];
   const int dir = h->perdir - 1;
   out->perm_rel_change = (out->perm_l[dir] - h->perm_prev) / h->perm_prev;  // CG3:5235-5246
@@ -447,6 +489,174 @@ lbm_status lbm_cg_get_populations(lbm_cg_handle* h, double* f) {
   LBM_CUDA_TRY(cudaMemcpyAsync(f, o.p, o.bytes, cudaMemcpyDeviceToHost, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return LBM_OK;
+}
+
+lbm_status lbm_cg_set_body_force(lbm_cg_handle* h, double gx, double gy, double gz, int timing) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (timing != LBM_CG_FORCE_BEFORE_MACRO && timing != LBM_CG_FORCE_BEFORE_COLLISION)
+    return fail(LBM_ERR_ARG, "lbm_cg_set_body_force: unknown timing");
+  const double g[3] = {gx, gy, gz};
+  for (int d = 0; d < 3; d++) {
+    h->cp.g[d] = g[d];
+    if (timing == LBM_CG_FORCE_BEFORE_MACRO) h->cp.gm[d] = g[d];
+  }
+  h->prm.gx = gx;
+  h->prm.gy = gy;
+  h->prm.gz = gz;
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  h->cp.cap_a = cap_a;
+  h->prm.cap_a = cap_a;
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict_nodes) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!window) return fail(LBM_ERR_ARG, "lbm_cg_set_window: null window");
+  Geometry& g = h->geo;
+  bool whole = true;
+  for (int i = 0; i < 6; i++) whole = whole && window[i] < 0;
+  if (whole) {
+    h->window_volume = (long long)g.nx * g.ny * g.nz;
+    g.porosity = (double)g.count / (double)h->window_volume;
+    h->win.alloc(0);
+    return LBM_OK;
+  }
+  h->window_volume = (long long)(window[1] - window[0] + 1) * (window[3] - window[2] + 1) * (window[5] - window[4] + 1);
+  // the porosity becomes the window's pore fraction (CG3:1835-1851)
+  std::vector<uint8_t> in((size_t)g.npad, 0);
+  long long pores = 0;
+  for (int x = 0; x < g.count; x++) {
+    const int c = g.coor[g.ref_of[x]];  // i*ny*nz + j*nz + k
+    const int i = c / (g.ny * g.nz), j = (c % (g.ny * g.nz)) / g.nz, k = c % g.nz;
+    in[x] = i >= window[0] && i <= window[1] && j >= window[2] && j <= window[3] && k >= window[4] && k <= window[5];
+    pores += in[x];
+  }
+  g.porosity = h->window_volume > 0 ? (double)pores / (double)h->window_volume : 0.0;
+  if (!restrict_nodes) {
+    h->win.alloc(0);
+    return LBM_OK;
+  }
+  LBM_CUDA_TRY(h->win.alloc(in.size()));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->win.p, in.data(), in.size(), cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_set_state(lbm_cg_handle* h, const double* f, const double* psi, const double* rho_r,
+                            const double* rho_b) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!f || !psi || !rho_r || !rho_b) return fail(LBM_ERR_ARG, "lbm_cg_set_state: null argument");
+  const int n = h->geo.count, npad = h->geo.npad;
+  Dev in;
+  const size_t fbytes = (size_t)(n + 1) * kQ * sizeof(double);
+  LBM_CUDA_TRY(in.alloc(fbytes));
+  LBM_CUDA_TRY(cudaMemcpyAsync(in.p, f, fbytes, cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(cg_import_f(h->f64, h->f[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n, npad,
+                           in.as<double>(), h->stream));
+  // scalar fields: internal order equals reference order - 1 for this solver
+  const double* srcs[3] = {psi, rho_r, rho_b};
+  Dev* dsts[3] = {&h->psi, &h->rho_r, &h->rho_b};
+  std::vector<double> d(npad, 0.0);
+  std::vector<float> fl(npad, 0.f);
+  for (int i = 0; i < 3; i++) {
+    for (int x = 0; x < n; x++) d[x] = srcs[i][h->geo.ref_of[x]];
+    if (h->f64) {
+      LBM_CUDA_TRY(cudaMemcpyAsync(dsts[i]->p, d.data(), sizeof(double) * npad, cudaMemcpyHostToDevice, h->stream));
+    } else {
+      for (int x = 0; x < npad; x++) fl[x] = (float)d[x];
+      LBM_CUDA_TRY(cudaMemcpyAsync(dsts[i]->p, fl.data(), sizeof(float) * npad, cudaMemcpyHostToDevice, h->stream));
+    }
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  h->given = 2;
+  h->uprev_valid = false;
+  return LBM_OK;
+}
+
+lbm_status lbm_read_cg_input(const char* path, lbm_cg_input* out) { return read_cg_input_file(path, out); }
+
+lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, double* out) {
+  return read_phase_file(path, nx, ny, nz, out);
+}
+
+lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
+                                    lbm_cg_input* parsed_out) {
+  if (!out) return fail(LBM_ERR_ARG, "lbm_cg_create_from_input: null output");
+  *out = nullptr;
+  lbm_cg_input in;
+  lbm_status st = read_cg_input_file(input_path, &in);
+  if (st != LBM_OK) return st;
+  if (parsed_out) *parsed_out = in;
+  // a fully periodic run with the phase read from file (CG3:2355-2380)
+  if (in.in_bc != 0) return fail(LBM_ERR_ARG, "in_BC: pressure / velocity faces are not supported by lbm_cg");
+  if (in.in_psi_bc != 0 && (in.psi_xp || in.psi_xn || in.psi_yp || in.psi_yn || in.psi_zp || in.psi_zn))
+    return fail(LBM_ERR_ARG, "psi_xp..psi_zn: constant-phase faces are not supported by lbm_cg");
+  if (in.ini_sat >= 0)
+    return fail(LBM_ERR_ARG, "ini_Sat: random initial phase (seeded from the clock) is not supported; use -1");
+  if (in.mix_psi_thickness > 0) return fail(LBM_ERR_ARG, "mix_psi_thickness: mixture injection is not supported");
+  if (in.lattice_v != 0) return fail(LBM_ERR_ARG, "lattice_v: self-defined lattice velocity is not supported");
+  if (in.inivx != 0 || in.inivy != 0 || in.inivz != 0)
+    return fail(LBM_ERR_ARG, "initial velocity: only a fluid at rest is supported");
+  if (in.rel_perm_id_dir != 0) return fail(LBM_ERR_ARG, "rel_perm_id_dir: imbibition / drainage control is not supported");
+  if (in.pressure_change2 != 0) return fail(LBM_ERR_ARG, "pressure_change2: capillary-pressure stepping is not supported");
+  if (in.input_dynamic != 0) return fail(LBM_ERR_ARG, "input_dynamic: dynamic input update is not supported");
+  if (in.fre_re <= 0) return fail(LBM_ERR_ARG, "freRe must be positive");
+  if (in.fre_psi == 0) return fail(LBM_ERR_ARG, "frePsi = 0: the reference takes n % 0; use -1 or a positive interval");
+  if (in.least_square > 0 && in.num_least_square < 2)
+    return fail(LBM_ERR_ARG, "num_least_square must be at least 2 for the least-squares fit");
+  const size_t cells = (size_t)in.nx * in.ny * in.nz;
+  std::vector<uint8_t> mask(cells);
+  std::vector<double> psi(cells);
+  // file paths are relative to the working directory, as in the reference
+  if ((st = read_mask_file(in.geometry_file, in.nx, in.ny, in.nz, in.decbin, mask.data())) != LBM_OK) return st;
+  if ((st = read_phase_file(in.phase_file, in.nx, in.ny, in.nz, psi.data())) != LBM_OK) return st;
+  lbm_cg_params p{};
+  p.nu_l = in.nu_l;
+  p.nu_g = in.nu_g;
+  p.psi_solid = in.contact_angle;  // CG3:2355
+  p.cap_a = in.cap_a;
+  const bool stab = in.stab == 1;  // gxs = 0 until stab_time (CG3:2375-2378)
+  p.gx = stab ? 0.0 : in.gx;
+  p.gy = stab ? 0.0 : in.gy;
+  p.gz = stab ? 0.0 : in.gz;
+  p.body_force_phase = in.bodyforce_apply;
+  p.flux_psi = in.rel_perm_psi;
+  p.flux_umax = in.rel_perm_psi2;
+  p.precision = precision;
+  p.device = 0;
+  p.perdir = in.perdir;
+  lbm_cg_handle* h = nullptr;
+  if ((st = lbm_cg_create(&p, mask.data(), psi.data(), in.nx, in.ny, in.nz, &h)) != LBM_OK) return st;
+  if (in.par_per_x || in.par_per_y || in.par_per_z) {
+    // an axis without a partial window spans the whole box (CG3:1707-1712);
+    // the sums are limited to the window when one of par_per_* is 1
+    // (CG3:5156, 5307)
+    const int w[6] = {in.par_per_x ? in.per_xn : 0, in.par_per_x ? in.per_xp : in.nx - 1,
+                      in.par_per_y ? in.per_yn : 0, in.par_per_y ? in.per_yp : in.ny - 1,
+                      in.par_per_z ? in.per_zn : 0, in.par_per_z ? in.per_zp : in.nz - 1};
+    const int restrict_nodes = (in.par_per_x - 1) * (in.par_per_y - 1) * (in.par_per_z - 1) == 0;
+    if ((st = lbm_cg_set_window(h, w, restrict_nodes)) != LBM_OK) {
+      lbm_cg_destroy(h);
+      return st;
+    }
+  }
+  *out = h;
+  return LBM_OK;
+}
+
+const uint8_t* lbm_cg_internal_mask(lbm_cg_handle* h, int* nx, int* ny, int* nz) {
+  *nx = h->geo.nx;
+  *ny = h->geo.ny;
+  *nz = h->geo.nz;
+  return h->mask.data();
 }
 
 lbm_status lbm_cg_info(lbm_cg_handle* h, int* count, double* porosity, long long* step, double* last_step_ms) {

@@ -7,7 +7,10 @@ namespace lbm {
 
 struct CgParams {
   double psi_solid, cap_a;
-  double g[3];
+  double g[3];   // body force of this step's collision (Guo forcing)
+  double gm[3];  // body force of the macro step folded into this step's collide
+                 // (u = (j + gm/2)/rho of the previous step; equals g except
+                 // right after a force change that precedes a collision)
   int body_force_phase;
   double flux_psi;
   // viscosity interpolation (CG3 init, delta = 0.1)
@@ -48,6 +51,7 @@ struct CgReduceArgs {
   const int32_t* axis;     // [npad] coordinate along perdir, or null
   double* partials2;
   double* result2;         // |du|^2, |u|^2, |u|, max |u|^2, sd_l, sd_g, 0, 0
+  const uint8_t* win;      // [npad] 1 = node inside the permeability window, or null (all)
 };
 
 cudaError_t cg_set_mi_f64(const double* mi, cudaStream_t st);
@@ -62,5 +66,7 @@ bool build_cg_inverse(double MI[kQ][kQ]);
 // f in the CG direction order, reference layout [(count+1)*19]
 cudaError_t cg_export_f(bool f64, const void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,
                         double* out, cudaStream_t st);
+cudaError_t cg_import_f(bool f64, void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,
+                        const double* in, cudaStream_t st);
 
 }  // namespace lbm

@@ -110,9 +110,9 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
     drho = r;
     rho = 1.f + r;
     const float ir = 1.f / rho;
-    ux = (jx + 0.5f * gx) * ir;
-    uy = (jy + 0.5f * gy) * ir;
-    uz = (jz + 0.5f * gz) * ir;
+    ux = (jx + 0.5f * (float)a.p.gm[0]) * ir;
+    uy = (jy + 0.5f * (float)a.p.gm[1]) * ir;
+    uz = (jz + 0.5f * (float)a.p.gm[2]) * ir;
   }
   if (a.u_out) {
     float* uo = static_cast<float*>(a.u_out);
@@ -305,6 +305,28 @@ cudaError_t cg_export_f(bool f64, const void* f, const int32_t* table, const int
     cg_export_kernel<double, false><<<g, 256, 0, st>>>((const double*)f, table, ref_of, n, npad, out);
   else
     cg_export_kernel<float, true><<<g, 256, 0, st>>>((const float*)f, table, ref_of, n, npad, out);
+  return cudaGetLastError();
+}
+
+// Inverse of cg_export_kernel: each (node, direction) owns one pulled slot.
+template <typename T, bool DEV>
+__global__ void cg_import_kernel(T* __restrict__ f, const int32_t* __restrict__ table,
+                                 const int32_t* __restrict__ ref_of, int n, int npad, const double* __restrict__ in) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  const double* row = in + (size_t)ref_of[x] * kQ;
+#pragma unroll
+  for (int k = 0; k < kQ; k++) f[cg_slot(table, npad, x, cg::row(k))] = (T)(DEV ? row[k] - weight(k) : row[k]);
+}
+
+cudaError_t cg_import_f(bool f64, void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,
+                        const double* in, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int g = (n + 255) / 256;
+  if (f64)
+    cg_import_kernel<double, false><<<g, 256, 0, st>>>((double*)f, table, ref_of, n, npad, in);
+  else
+    cg_import_kernel<float, true><<<g, 256, 0, st>>>((float*)f, table, ref_of, n, npad, in);
   return cudaGetLastError();
 }
 

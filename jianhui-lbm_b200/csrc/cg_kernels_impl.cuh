@@ -86,9 +86,9 @@ __global__ void __launch_bounds__(256) cg_collide_kernel(CgArgs a) {
       drho = r;
       rho = T(1) + r;
     }
-    ux = (sx + T(1.0 * a.p.g[0]) / T(2)) / rho;
-    uy = (sy + T(1.0 * a.p.g[1]) / T(2)) / rho;
-    uz = (sz + T(1.0 * a.p.g[2]) / T(2)) / rho;
+    ux = (sx + T(1.0 * a.p.gm[0]) / T(2)) / rho;
+    uy = (sy + T(1.0 * a.p.gm[1]) / T(2)) / rho;
+    uz = (sz + T(1.0 * a.p.gm[2]) / T(2)) / rho;
   }
   if (!FAITHFUL && a.given) drho = T(0);
   if (a.u_out) {
@@ -299,7 +299,8 @@ __global__ void __launch_bounds__(256) cg_reduce_kernel(CgReduceArgs a) {
     }
     const double ps = psi[x];
     const double dx = ux, dy = uy, dz = uz;
-    if (sqrt(dx * dx + dy * dy + dz * dz) < a.flux_umax) {
+    const bool in_win = a.win == nullptr || a.win[x] != 0;  // Comput_Perm's window (CG3:5156-5180)
+    if (in_win && sqrt(dx * dx + dy * dy + dz * dz) < a.flux_umax) {
       if (ps >= a.flux_psi) {
         acc[0] += dx;
         acc[1] += dy;
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(256) cg_reduce_kernel(CgReduceArgs a) {
         acc[6] += dz;
       }
     }
-    if (ps >= 0) acc[3] += 1.0;  // Comput_Saturation counts psi >= 0 (CG3:5319)
+    if (in_win && ps >= 0) acc[3] += 1.0;  // Comput_Saturation counts psi >= 0 (CG3:5319)
     acc[7] += (double)rho;
     if (a.partials2) {
       double px = dx, py = dy, pz = dz;
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(256) cg_reduce_kernel(CgReduceArgs a) {
       acc2[1] += u2;
       acc2[2] += sqrt(u2);
       acc2[3] = fmax(acc2[3], u2);
-      if (a.axis) {
+      if (a.axis && in_win) {
         const double sdir = (double)a.axis[x];
         if (ps >= 0)
           acc2[4] += ps * sdir;

@@ -105,6 +105,104 @@ lbm_status read_input_file(const char* path, lbm_input* o) {
   return LBM_OK;
 }
 
+// Field order of the colour-gradient program's INPUT file (CG3:372-474).
+lbm_status read_cg_input_file(const char* path, lbm_cg_input* o) {
+  if (!path || !o) return fail(LBM_ERR_ARG, "lbm_read_cg_input: null argument");
+  std::ifstream fin(path);
+  if (!fin) return fail(LBM_ERR_IO, std::string("cannot open input file ") + path);
+  std::memset(o, 0, sizeof(*o));
+  LineReader r(fin);
+  bool ok = true;
+  r.skip();
+  ok &= r.word(o->geometry_file, sizeof(o->geometry_file));
+  ok &= r.word(o->phase_file, sizeof(o->phase_file));
+  ok &= r.line(o->nx, o->ny, o->nz);
+  ok &= r.line(o->n_max);
+  ok &= r.line(o->reso);
+  ok &= r.line(o->in_bc);
+  ok &= r.line(o->in_psi_bc);
+  ok &= r.line(o->gx, o->gy, o->gz);
+  ok &= r.line(o->pre_xp, o->p_xp, o->pre_xn, o->p_xn);
+  ok &= r.line(o->pre_yp, o->p_yp, o->pre_yn, o->p_yn);
+  ok &= r.line(o->pre_zp, o->p_zp, o->pre_zn, o->p_zn);
+  ok &= r.line(o->vel_xp, o->v_xp, o->vel_xn, o->v_xn);
+  ok &= r.line(o->vel_yp, o->v_yp, o->vel_yn, o->v_yn);
+  ok &= r.line(o->vel_zp, o->v_zp, o->vel_zn, o->v_zn);
+  ok &= r.line(o->psi_xp, o->psi_xn);
+  ok &= r.line(o->psi_yp, o->psi_yn);
+  ok &= r.line(o->psi_zp, o->psi_zn);
+  ok &= r.line(o->nu_l);
+  ok &= r.line(o->nu_g);
+  ok &= r.line(o->contact_angle);
+  ok &= r.line(o->cap_a);
+  ok &= r.line(o->inivx, o->inivy, o->inivz);
+  ok &= r.line(o->permeability);
+  r.skip();
+  ok &= r.line(o->wr_per);
+  ok &= r.line(o->perdir);
+  ok &= r.line(o->fre_re);
+  ok &= r.line(o->out_mode);
+  ok &= r.line(o->fre_ve);
+  ok &= r.line(o->fre_de);
+  ok &= r.line(o->fre_psi);
+  r.skip();
+  ok &= r.line(o->lattice_v, o->dx_input, o->dt_input);
+  ok &= r.word(o->output_path, sizeof(o->output_path));
+  ok &= r.line(o->sub_bc);
+  ok &= r.line(o->stab, o->stab_time);
+  ok &= r.line(o->ini_sat);
+  ok &= r.line(o->ini_buf);
+  ok &= r.line(o->rel_perm_psi, o->rel_perm_psi2);
+  ok &= r.line(o->par_per_x, o->par_per_y, o->par_per_z);
+  ok &= r.line(o->per_xp, o->per_xn);
+  ok &= r.line(o->per_yp, o->per_yn);
+  ok &= r.line(o->per_zp, o->per_zn);
+  r.skip();
+  ok &= r.line(o->fre_backup);
+  ok &= r.line(o->mode_backup_ini);
+  r.skip();
+  ok &= r.line(o->decbin);
+  r.skip();
+  ok &= r.line(o->pressure_change, o->pre_chan_pb);
+  for (int i = 0; i < 5; i++) ok &= r.line(o->pre_chan[i], o->pre_chan_pn[i], o->pre_chan_pp[i], o->pre_chan_f[i]);
+  ok &= r.line(o->bodyforce_apply);
+  r.skip();
+  ok &= r.line(o->pressure_change2, o->pre_chan_pb2, o->interval_pre);
+  ok &= r.line(o->pre_chan_pns, o->pre_chan_pps, o->pre_chan_fs, o->chan_no, o->sat_cri);
+  ok &= r.line(o->sat_cri_d);
+  r.skip();
+  ok &= r.line(o->least_square, o->num_least_square);
+  r.skip();
+  ok &= r.line(o->rel_perm_id_dir, o->rel_perm_chan_num);
+  ok &= r.line(o->rel_perm_ift, o->vary_ift);
+  ok &= r.line(o->input_dynamic, o->update_fre);
+  r.skip();
+  ok &= r.line(o->mix_psi_thickness);
+  ok &= r.line(o->protion_w);
+  ok &= r.line(o->zero_sigma_thickness);
+  if (!ok) return fail(LBM_ERR_FORMAT, std::string("malformed input file ") + path);
+  if (o->nx <= 0 || o->ny <= 0 || o->nz <= 0)
+    return fail(LBM_ERR_FORMAT, "input file: non-positive grid size");
+  return LBM_OK;
+}
+
+// Phase file (CG3:2144-2150): nx*ny*nz numbers, k outer / j / i inner, each
+// stored as float.
+lbm_status read_phase_file(const char* path, int nx, int ny, int nz, double* out) {
+  if (!path || !out || nx <= 0 || ny <= 0 || nz <= 0) return fail(LBM_ERR_ARG, "lbm_read_phase: bad argument");
+  std::ifstream fin(path);
+  if (!fin) return fail(LBM_ERR_IO, std::string("the concentration file (") + path + ") does not exist");
+  const size_t cells = (size_t)nx * ny * nz;
+  for (size_t c = 0; c < cells; c++) {
+    float v;
+    if (!(fin >> v))
+      return fail(LBM_ERR_FORMAT, std::string("phase file ") + path + ": " + std::to_string(c) + " values, expected " +
+                                      std::to_string(cells));
+    out[c] = (double)v;
+  }
+  return LBM_OK;
+}
+
 // decbin 0: whitespace-separated integer tokens, k outer / j / i inner; any
 // non-zero token is solid (SP3:929-943 reads into Solid, Partition_Solid
 // SP3:3818-3819 treats Solid == 0 as pore).  decbin 1: raw int32 C-order

@@ -155,6 +155,7 @@ void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPl
 
 // Mask and box of a single-phase handle (for solvers coupled to it).
 const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz);
+extern "C" const uint8_t* lbm_cg_internal_mask(lbm_cg_handle* h, int* nx, int* ny, int* nz);
 
 // ---------------------------------------------------------------- errors
 void set_error(const std::string& msg);

@@ -147,6 +147,42 @@ class CGParams(C.Structure):
                 ("perdir", C.c_int)]
 
 
+class CGInput(C.Structure):
+    _fields_ = [
+        ("geometry_file", C.c_char * 256), ("phase_file", C.c_char * 256),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("n_max", C.c_int), ("reso", C.c_double),
+        ("in_bc", C.c_int), ("in_psi_bc", C.c_int), ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+        ("pre_xp", C.c_int), ("p_xp", C.c_double), ("pre_xn", C.c_int), ("p_xn", C.c_double),
+        ("pre_yp", C.c_int), ("p_yp", C.c_double), ("pre_yn", C.c_int), ("p_yn", C.c_double),
+        ("pre_zp", C.c_int), ("p_zp", C.c_double), ("pre_zn", C.c_int), ("p_zn", C.c_double),
+        ("vel_xp", C.c_int), ("v_xp", C.c_double), ("vel_xn", C.c_int), ("v_xn", C.c_double),
+        ("vel_yp", C.c_int), ("v_yp", C.c_double), ("vel_yn", C.c_int), ("v_yn", C.c_double),
+        ("vel_zp", C.c_int), ("v_zp", C.c_double), ("vel_zn", C.c_int), ("v_zn", C.c_double),
+        ("psi_xp", C.c_int), ("psi_xn", C.c_int), ("psi_yp", C.c_int), ("psi_yn", C.c_int), ("psi_zp", C.c_int),
+        ("psi_zn", C.c_int), ("nu_l", C.c_double), ("nu_g", C.c_double), ("contact_angle", C.c_double),
+        ("cap_a", C.c_double), ("inivx", C.c_double), ("inivy", C.c_double), ("inivz", C.c_double),
+        ("permeability", C.c_double), ("wr_per", C.c_int), ("perdir", C.c_int), ("fre_re", C.c_int),
+        ("out_mode", C.c_int), ("fre_ve", C.c_int), ("fre_de", C.c_int), ("fre_psi", C.c_int),
+        ("lattice_v", C.c_int), ("dx_input", C.c_double), ("dt_input", C.c_double),
+        ("output_path", C.c_char * 256), ("sub_bc", C.c_int), ("stab", C.c_int), ("stab_time", C.c_int),
+        ("ini_sat", C.c_double), ("ini_buf", C.c_int), ("rel_perm_psi", C.c_double), ("rel_perm_psi2", C.c_double),
+        ("par_per_x", C.c_int), ("par_per_y", C.c_int), ("par_per_z", C.c_int),
+        ("per_xp", C.c_int), ("per_xn", C.c_int), ("per_yp", C.c_int), ("per_yn", C.c_int),
+        ("per_zp", C.c_int), ("per_zn", C.c_int), ("fre_backup", C.c_int), ("mode_backup_ini", C.c_int),
+        ("decbin", C.c_int), ("pressure_change", C.c_int), ("pre_chan_pb", C.c_int), ("pre_chan", C.c_int * 5),
+        ("pre_chan_pn", C.c_double * 5), ("pre_chan_pp", C.c_double * 5), ("pre_chan_f", C.c_double * 5),
+        ("bodyforce_apply", C.c_int), ("pressure_change2", C.c_int), ("pre_chan_pb2", C.c_int),
+        ("interval_pre", C.c_int), ("pre_chan_pns", C.c_double), ("pre_chan_pps", C.c_double),
+        ("pre_chan_fs", C.c_double), ("chan_no", C.c_int), ("sat_cri", C.c_int), ("sat_cri_d", C.c_double),
+        ("least_square", C.c_int), ("num_least_square", C.c_int), ("rel_perm_id_dir", C.c_int),
+        ("rel_perm_chan_num", C.c_int), ("rel_perm_ift", C.c_int), ("vary_ift", C.c_double),
+        ("input_dynamic", C.c_int), ("update_fre", C.c_int), ("mix_psi_thickness", C.c_int),
+        ("protion_w", C.c_double), ("zero_sigma_thickness", C.c_int),
+    ]
+
+    as_dict = Input.as_dict
+
+
 class CGDiag(C.Structure):
     _fields_ = [("step", C.c_longlong), ("saturation", C.c_double), ("q_l", C.c_double * 3),
                 ("q_g", C.c_double * 3), ("perm_l", C.c_double * 3), ("perm_g", C.c_double * 3),
@@ -215,6 +251,18 @@ _SIGNATURES = {
     "lbm_cg_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                      C.POINTER(C.c_double)], C.c_int),
     "lbm_cg_destroy": ([C.c_void_p], None),
+    "lbm_cg_set_body_force": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int], C.c_int),
+    "lbm_cg_set_cap_a": ([C.c_void_p, C.c_double], C.c_int),
+    "lbm_cg_set_window": ([C.c_void_p, _I32P, C.c_int], C.c_int),
+    "lbm_cg_set_state": ([C.c_void_p, _F64P, _F64P, _F64P, _F64P], C.c_int),
+    "lbm_read_cg_input": ([C.c_char_p, C.POINTER(CGInput)], C.c_int),
+    "lbm_read_phase": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
+    "lbm_cg_create_from_input": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(CGInput)], C.c_int),
+    "lbm_cg_write_vtk_velocity": ([C.c_void_p, C.c_char_p], C.c_int),
+    "lbm_cg_write_vtk_density": ([C.c_void_p, C.c_char_p], C.c_int),
+    "lbm_cg_write_vtk_psi": ([C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p], C.c_int),
+    "lbm_cg_write_checkpoint": ([C.c_void_p, C.c_char_p, C.c_longlong], C.c_int),
+    "lbm_cg_read_checkpoint": ([C.c_void_p, C.c_char_p, C.c_longlong], C.c_int),
     "lbm_st7_create": ([C.c_void_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P, _F64P, C.POINTER(C.c_void_p)], C.c_int),
     "lbm_st7_create_from_flow": ([C.c_void_p, C.c_void_p, _F64P, C.POINTER(C.c_void_p)], C.c_int),
     "lbm_st7_step": ([C.c_void_p, C.c_int], C.c_int),
@@ -260,9 +308,12 @@ def read_checkpoint(flow, prefix, m):
     _check(lib().lbm_read_checkpoint(flow._h, os.fsencode(prefix), int(m)))
 
 
-def driver_path():
-    """Path of the lbm_sp command-line driver built beside liblbm.so."""
-    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "lbm_sp")
+def driver_path(name="lbm_sp"):
+    """Path of a command-line driver built beside liblbm.so: ``lbm_sp``
+    (single phase) or ``lbm_cg`` (colour gradient)."""
+    if name not in ("lbm_sp", "lbm_cg"):
+        raise ValueError(f"unknown driver {name!r}")
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), name)
 
 
 class ST7Params(C.Structure):
@@ -362,6 +413,56 @@ class ColourGradient:
         c, ph, st, ms = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
         _check(lib().lbm_cg_info(h, C.byref(c), C.byref(ph), C.byref(st), C.byref(ms)))
         self.count, self.porosity = c.value, ph.value
+
+    @classmethod
+    def from_input(cls, input_path, precision="f64"):
+        """Solver of the colour-gradient program's INPUT file (geometry and
+        phase file read from the paths it names); returns (solver, input dict)."""
+        self = cls.__new__(cls)
+        h, inp = C.c_void_p(), CGInput()
+        _check(lib().lbm_cg_create_from_input(os.fsencode(input_path),
+                                              PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                                              C.byref(h), C.byref(inp)))
+        self._h = h
+        c, ph, st, ms = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
+        _check(lib().lbm_cg_info(h, C.byref(c), C.byref(ph), C.byref(st), C.byref(ms)))
+        self.count, self.porosity = c.value, ph.value
+        return self, inp.as_dict()
+
+    def set_body_force(self, g, before_collision=False):
+        """New body force; with before_collision the last step's macro values
+        keep the old one (the stabiliser's switch), else they take the new one
+        (the force ramps)."""
+        _check(lib().lbm_cg_set_body_force(self._h, float(g[0]), float(g[1]), float(g[2]), int(bool(before_collision))))
+
+    def set_cap_a(self, cap_a):
+        _check(lib().lbm_cg_set_cap_a(self._h, float(cap_a)))
+
+    def set_window(self, window, restrict_nodes=True):
+        """window = (xn, xp, yn, yp, zn, zp) inclusive, or None for the whole box."""
+        w = np.full(6, -1, dtype=np.int32) if window is None else np.ascontiguousarray(window, dtype=np.int32)
+        _check(lib().lbm_cg_set_window(self._h, w, int(bool(restrict_nodes))))
+
+    def set_state(self, f, psi, rho_r, rho_b):
+        """Restores f [(count+1), 19] (CG velocity order) and psi / rho_r /
+        rho_b [(count+1)], reference id order."""
+        arr = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        _check(lib().lbm_cg_set_state(self._h, arr(f), arr(psi), arr(rho_r), arr(rho_b)))
+
+    def write_vtk_velocity(self, path):
+        _check(lib().lbm_cg_write_vtk_velocity(self._h, os.fsencode(path)))
+
+    def write_vtk_density(self, path):
+        _check(lib().lbm_cg_write_vtk_density(self._h, os.fsencode(path)))
+
+    def write_vtk_psi(self, path, version_suffix="", title=""):
+        _check(lib().lbm_cg_write_vtk_psi(self._h, os.fsencode(path), version_suffix.encode(), title.encode()))
+
+    def write_checkpoint(self, prefix, m):
+        _check(lib().lbm_cg_write_checkpoint(self._h, os.fsencode(prefix), int(m)))
+
+    def read_checkpoint(self, prefix, m):
+        _check(lib().lbm_cg_read_checkpoint(self._h, os.fsencode(prefix), int(m)))
 
     def step(self, n=1):
         _check(lib().lbm_cg_step(self._h, int(n)))
@@ -574,6 +675,21 @@ def read_input(path):
     out = Input()
     _check(lib().lbm_read_input(os.fsencode(path), C.byref(out)))
     return out.as_dict()
+
+
+def read_cg_input(path):
+    """INPUT file of the colour-gradient program as a dict (field order CG3:372-474)."""
+    out = CGInput()
+    _check(lib().lbm_read_cg_input(os.fsencode(path), C.byref(out)))
+    return out.as_dict()
+
+
+def read_phase(path, shape):
+    """Phase file (x fastest, each value read as float) as [nz, ny, nx] float64."""
+    nx, ny, nz = shape
+    out = np.zeros(nx * ny * nz)
+    _check(lib().lbm_read_phase(os.fsencode(path), nx, ny, nz, out))
+    return out.reshape(nz, ny, nx)
 
 
 def read_mask(path, shape, decbin):

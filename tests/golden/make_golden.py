@@ -2,7 +2,7 @@
 solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
 compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
 
-    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --bc | --st7 | --slab-perm]
+    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --cg-outputs | --bc | --st7 | --slab-perm]
 
 Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
@@ -10,6 +10,9 @@ random generator at test time):
                 run on an INPUT.dat: every file it writes  (--outputs)
   sp_outputs_bc.npz  the same with pressure faces on x (Sub_BC 2, in_BC 1)  (--outputs)
   cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
+  cg_outputs*.npz  the colour-gradient program (oracle/_ref/ref_cg3_main) on
+                INPUT_cg.dat variants: every file it writes, and a restart from
+                its checkpoint, see cg_program_outputs()  (--cg-outputs)
   sp_bc.npz     pressure/velocity boundaries, Sub_BC 0..3, see bc_fixture()  (--bc)
   st7_slab.npz  the solute program at two ranks, see st7_fixture()  (--st7)
   sp_slab_perm.npz  the slab single-phase program at two ranks with its
@@ -205,6 +208,102 @@ def save_program_outputs(fname, mask, input_txt):
     print(fname, sorted(a))
 
 
+def cg_input_text(**kv):
+    """INPUT file of the colour-gradient program: INPUT_cg.dat with some
+    values replaced; keys are the 0-based line numbers of the file."""
+    lines = open(os.path.join(HERE, "INPUT_cg.dat")).read().splitlines()
+    for i, v in kv.items():
+        lines[int(i[1:])] = f"{v}\t\t:{lines[int(i[1:])].split(':', 1)[1]}"
+    return "\n".join(lines) + "\n"
+
+
+def cg_geometry():
+    """14x12x10 spheres (porosity 0.6) with a blob phase field at S_w = 0.5."""
+    mask = G.overlapping_spheres((14, 12, 10), 0.6, 2.5, seed=21)
+    psi = G.blob_phase_field(mask, seed=22, saturation=0.5)
+    return mask, psi
+
+
+def phase_text(psi):
+    return " ".join(str(int(v)) for v in psi.reshape(-1)) + "\n"
+
+
+# The colour-gradient program's runs (the reference program compiled from its
+# source, oracle/_ref/ref_cg3_main), name -> INPUT line overrides.
+CG_RUNS = {
+    # reports every 50 steps to n_max = 150, VTK of density / velocity at 100,
+    # phase VTK every 50, mesh VTK, checkpoints at 100 and at the end
+    "cg_outputs.npz": dict(L45=100),
+    # stabiliser (force from step 30), permeability window 3..10 on x limiting
+    # the sums, least-squares fit over 4 reports, surface tension changed at
+    # step 100, y the permeability direction, the force on both phases, a
+    # second force component; reports every 25 steps
+    "cg_outputs_sched.npz": dict(L8="1.0e-5 4.0e-6 0.0", L26=2, L27=25, L28=0, L29=-1, L30=-1, L31=75, L36="1 30",
+                                 L40="1 0 0", L41="10 3", L56=0, L62="1 4", L65="100 2.0e-3"),
+    # body-force ramp along y through three points (the first segment starts
+    # from gx, as the reference writes it), z the permeability direction
+    "cg_outputs_ramp.npz": dict(L8="1.0e-5 2.0e-6 -1.0e-6", L26=3, L27=25, L28=0, L29=-1, L30=-1, L31=-1,
+                                L50="2 2", L51="40 1.0 1.0 8.0e-6", L52="90 1.0 1.0 3.0e-6",
+                                L53="120 1.0 1.0 5.0e-6"),
+}
+
+
+def run_cg_program(workdir, input_txt, mask, psi, args=()):
+    import subprocess
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cg3_main")
+    G.write_ascii(os.path.join(workdir, "mask.dat"), mask)
+    with open(os.path.join(workdir, "phase.dat"), "w") as f:
+        f.write(phase_text(psi))
+    with open(os.path.join(workdir, "INPUT.dat"), "w") as f:
+        f.write(input_txt)
+    subprocess.run([exe, "INPUT.dat", *args], cwd=workdir, check=True, capture_output=True)
+
+
+def collect_cg(workdir, prefix):
+    out = {}
+    for name in sorted(os.listdir(workdir)):
+        if not name.startswith(prefix):
+            continue
+        key = name[len(prefix):]
+        data = open(os.path.join(workdir, name), "rb").read()
+        if key.startswith("LBM_checkpoint_"):
+            width = {"rho": 1, "velocity": 3, "f": 19, "psi": 1, "rhor": 1, "rhob": 1}[key.split("_")[2]]
+            out[key] = digest(np.frombuffer(data, dtype=np.float64).reshape(-1, width)[1:])
+        else:
+            out[key] = data
+    return out
+
+
+def save_cg(fname, mask, psi, input_txt, files):
+    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "phase": np.frombuffer(phase_text(psi).encode(), np.uint8),
+            "input": np.frombuffer(input_txt.encode(), np.uint8), "names": np.array(sorted(files))}
+    for k, v in files.items():
+        blob[k] = np.frombuffer(v, np.uint8) if isinstance(v, bytes) else np.array(v)
+    np.savez_compressed(os.path.join(HERE, fname), **blob)
+    print(fname, sorted(files))
+
+
+def cg_program_outputs():
+    """Every file the colour-gradient program writes for the runs of CG_RUNS,
+    and a restart: the first run's step-100 checkpoint read back
+    (mode_backup_ini = 100, prefix ./out_) and run for 60 more steps
+    (cg_outputs_restart.npz, files prefixed rst_)."""
+    import tempfile
+
+    mask, psi = cg_geometry()
+    for fname, kv in CG_RUNS.items():
+        text = cg_input_text(**kv)
+        with tempfile.TemporaryDirectory() as d:
+            run_cg_program(d, text, mask, psi)
+            files = collect_cg(d, "out_")
+            if fname == "cg_outputs.npz":
+                rst = cg_input_text(L4=59, L27=20, L29=-1, L30=-1, L31=40, L34="./rst_", L45=0, L46=100)
+                run_cg_program(d, rst, mask, psi, ("./out_",))
+                save_cg("cg_outputs_restart.npz", mask, psi, rst, collect_cg(d, "rst_"))
+        save_cg(fname, mask, psi, text, files)
+
+
 def bc_cases():
     """(name, Boundaries, g, perdir) of the boundary-condition fixture: for
     each Sub_BC 0..3, pressure on the two x faces, pressure on all six faces
@@ -344,8 +443,12 @@ def main():
     ap.add_argument("--cfg1", action="store_true")
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
+    ap.add_argument("--cg-outputs", action="store_true")
     a = ap.parse_args()
     oracle.build()
+    if a.cg_outputs:
+        cg_program_outputs()
+        return
     if a.cg:
         cg_small()
         return

@@ -1,0 +1,93 @@
+"""The colour-gradient program's INPUT file, phase file and the options the
+drop-in driver refuses, on the CPU (no device calls: the checks run before
+the solver is created)."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN
+
+
+@pytest.fixture(scope="module")
+def L():
+    import __graft_entry__
+
+    __graft_entry__.build_library()
+    import lbm_b200
+
+    return lbm_b200
+
+
+def set_lines(text, **kv):
+    lines = text.splitlines()
+    for k, v in kv.items():
+        i = int(k[1:])
+        lines[i] = f"{v}\t\t:{lines[i].split(':', 1)[1]}"
+    return "\n".join(lines) + "\n"
+
+
+def test_cg_input_field_order(L):
+    d = L.read_cg_input(os.path.join(GOLDEN, "INPUT_cg.dat"))
+    assert (d["geometry_file"], d["phase_file"]) == ("mask.dat", "phase.dat")
+    assert (d["nx"], d["ny"], d["nz"], d["n_max"], d["reso"]) == (14, 12, 10, 150, 7.0)
+    assert (d["in_bc"], d["in_psi_bc"], d["gx"], d["gy"], d["gz"]) == (0, 0, 1e-5, 0.0, 0.0)
+    assert (d["nu_l"], d["nu_g"], d["contact_angle"], d["cap_a"], d["permeability"]) == (0.1, 0.1, 0.70711, 1e-3,
+                                                                                        2500.0)
+    assert (d["wr_per"], d["perdir"], d["fre_re"], d["out_mode"], d["fre_ve"], d["fre_de"], d["fre_psi"]) == (
+        1, 1, 50, 1, 100, 100, 50)
+    assert d["output_path"] == "./out_"
+    assert (d["stab"], d["stab_time"], d["ini_sat"], d["ini_buf"]) == (0, 500, -1.0, 0)
+    assert (d["rel_perm_psi"], d["rel_perm_psi2"]) == (0.99, 0.01)
+    assert (d["per_xp"], d["per_xn"], d["per_yp"], d["per_yn"], d["per_zp"], d["per_zn"]) == (10, 3, 11, 0, 9, 0)
+    assert (d["fre_backup"], d["mode_backup_ini"], d["decbin"]) == (-1, 0, 0)
+    assert (d["pressure_change"], d["pre_chan_pb"], d["pre_chan"]) == (0, 2, [-1] * 5)
+    assert d["bodyforce_apply"] == -1
+    assert (d["pressure_change2"], d["pre_chan_pb2"], d["interval_pre"], d["chan_no"], d["sat_cri"]) == (0, 1, 2000, 6,
+                                                                                                        10)
+    assert (d["least_square"], d["num_least_square"], d["rel_perm_id_dir"], d["rel_perm_chan_num"]) == (0, 4, 0, 5)
+    assert (d["rel_perm_ift"], d["vary_ift"], d["input_dynamic"], d["update_fre"]) == (0, 0.7e-2, 0, 1000)
+    assert (d["mix_psi_thickness"], d["protion_w"], d["zero_sigma_thickness"]) == (0, 0.5, 6)
+
+
+def test_cg_fixture_inputs_parse(L, tmp_path):
+    for name in ("cg_outputs.npz", "cg_outputs_sched.npz", "cg_outputs_ramp.npz", "cg_outputs_restart.npz"):
+        g = np.load(os.path.join(GOLDEN, name))
+        p = tmp_path / "INPUT.dat"
+        p.write_bytes(g["input"].tobytes())
+        d = L.read_cg_input(str(p))
+        assert (d["nx"], d["ny"], d["nz"]) == tuple(int(s) for s in g["shape"][::-1])
+        assert "Results.txt" in [str(n) for n in g["names"]]
+    d = L.read_cg_input(str(p))
+    assert (d["mode_backup_ini"], d["output_path"]) == (100, "./rst_")
+
+
+def test_phase_file_reads_as_float(L, tmp_path):
+    vals = np.array([1, -1, 0.3, 0.1234567891234, -2.5e-3, 0], dtype=np.float64)
+    p = tmp_path / "phase.dat"
+    p.write_text(" ".join(repr(float(v)) for v in vals[:3]) + "\n" + "\t".join(repr(float(v)) for v in vals[3:]) + "\n")
+    got = L.read_phase(str(p), (3, 2, 1))
+    assert got.shape == (1, 2, 3)
+    assert np.array_equal(got.reshape(-1), vals.astype(np.float32).astype(np.float64))
+    with pytest.raises(L.LbmError):
+        L.read_phase(str(p), (7, 1, 1))
+
+
+@pytest.mark.parametrize("lines,field", [
+    (dict(L6=1), "in_BC"),
+    (dict(L7=1, L15="1 1"), "psi_xp"),
+    (dict(L37=0.5), "ini_Sat"),
+    (dict(L68=3), "mix_psi_thickness"),
+    (dict(L33="1 1.0 2.0"), "lattice_v"),
+    (dict(L22="1e-3 0 0"), "initial velocity"),
+    (dict(L64="1 5"), "rel_perm_id_dir"),
+    (dict(L58="1 1 2000"), "pressure_change2"),
+    (dict(L66="1 1000"), "input_dynamic"),
+    (dict(L31=0), "frePsi"),
+])
+def test_cg_driver_refuses_options_outside_its_scope(L, tmp_path, lines, field):
+    text = set_lines(open(os.path.join(GOLDEN, "INPUT_cg.dat")).read(), **lines)
+    (tmp_path / "INPUT.dat").write_text(text)
+    with pytest.raises(L.LbmError) as e:
+        L.ColourGradient.from_input(str(tmp_path / "INPUT.dat"))
+    assert e.value.status == -1 and field in str(e.value), str(e.value)
