@@ -468,6 +468,58 @@ LBM_API lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps);
 /* C per fluid node [(count+1)], reference id order, row 0 zero */
 LBM_API lbm_status lbm_st7_get_concentration(lbm_st7_handle* h, double* c);
 LBM_API lbm_status lbm_st7_info(lbm_st7_handle* h, int* count, long long* step, double* last_step_ms);
+/* g as the next step reads it (the reference's fg after comput_macro_variables,
+ * ST7:1619-1633): [(count+1)*7] in reference id order, column 0 and row 0 zero */
+LBM_API lbm_status lbm_st7_get_populations(lbm_st7_handle* h, double* g);
+/* Restores g [(count+1)*7] and C [(count+1)] like Backup_init (ST7:3716-3802);
+ * the next step takes C as given */
+LBM_API lbm_status lbm_st7_set_state(lbm_st7_handle* h, const double* g, const double* c);
+
+/* INPUT file of the solute program (ST7:219-280, field order and types kept;
+ * nx, ny, nz as written in the file). */
+typedef struct lbm_st7_input {
+  char geometry_file[256];
+  char conc_file[256];        /* initial concentration, x fastest, read as float */
+  int nx, ny, nz;
+  int n_max;
+  double reso;
+  int in_bc;
+  double buoyancy, ref_psi;   /* ref_psi: value written on solid cells */
+  double gravity;
+  double gx, gy, gz;
+  int pre_xp; double p_xp; int pre_xn; double p_xn;
+  int pre_yp; double p_yp; int pre_yn; double p_yn;
+  int pre_zp; double p_zp; int pre_zn; double p_zn;
+  int vel_xp; double v_xp; int vel_xn; double v_xn;
+  int vel_yp; double v_yp; int vel_yn; double v_yn;
+  int vel_zp; double v_zp; int vel_zn; double v_zn;
+  int sol_c_xp; double c_xp; int sol_c_xn; double c_xn;
+  int sol_c_yp; double c_yp; int sol_c_yn; double c_yn;
+  int sol_c_zp; double c_zp; int sol_c_zn; double c_zn;
+  int sol_zf_xp; double zf_xp; int sol_zf_xn; double zf_xn;
+  int sol_zf_yp; double zf_yp; int sol_zf_yn; double zf_yn;
+  int sol_zf_zp; double zf_zp; int sol_zf_zn; double zf_zn;
+  double nu;                  /* flow viscosity (for the Reynolds number) */
+  double nu_s;                /* solute diffusivity */
+  double inivx, inivy, inivz;
+  int wr_per, perdir, fre_re, out_mode, fre_ve, fre_de, fre_psi;
+  int sub_dis, fre_dis;
+  int lattice_v; double dx_input, dt_input;
+  char output_path[256];
+  int sub_bc, sub_bc_psi, ini_psi;
+  int par_per_x, par_per_y, par_per_z;
+  int per_xp, per_xn, per_yp, per_yn, per_zp, per_zn;
+  int fre_backup, mode_backup_ini;
+  int sol_ini_n;              /* step tag of the Velocity_for_solute files read */
+  int decbin;
+} lbm_st7_input;
+
+LBM_API lbm_status lbm_read_st7_input(const char* path, lbm_st7_input* out);
+
+/* x-slab decomposition of the slab programs (ST7:951-975): rank r holds the
+ * x-planes [first_x[r], first_x[r+1]), first_x [nranks+1].  The per-rank
+ * Velocity_for_solute and checkpoint files of an N-rank run follow it. */
+LBM_API lbm_status lbm_slab_partition(const uint8_t* mask, int nx, int ny, int nz, int nranks, int* first_x);
 LBM_API void lbm_st7_destroy(lbm_st7_handle* h);
 
 /* Velocity_for_solute_<n>.<rank>.bin (SP:5093-5120): Count*3 raw doubles in

@@ -41,7 +41,7 @@ CUDA_SOURCES = [
 ]
 CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp", "output.cpp"]
 # Command-line drivers linked against liblbm.so: (source, executable name).
-EXECUTABLES = [("lbm_sp_main.cpp", "lbm_sp"), ("lbm_cg_main.cpp", "lbm_cg")]
+EXECUTABLES = [("lbm_sp_main.cpp", "lbm_sp"), ("lbm_cg_main.cpp", "lbm_cg"), ("lbm_st7_main.cpp", "lbm_st7")]
 BIN = os.path.join(HERE, "lbm_b200")
 
 

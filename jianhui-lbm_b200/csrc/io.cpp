@@ -186,6 +186,71 @@ lbm_status read_cg_input_file(const char* path, lbm_cg_input* o) {
   return LBM_OK;
 }
 
+// Field order of the solute program's INPUT file (ST7:219-280).
+lbm_status read_st7_input_file(const char* path, lbm_st7_input* o) {
+  if (!path || !o) return fail(LBM_ERR_ARG, "lbm_read_st7_input: null argument");
+  std::ifstream fin(path);
+  if (!fin) return fail(LBM_ERR_IO, std::string("cannot open input file ") + path);
+  std::memset(o, 0, sizeof(*o));
+  LineReader r(fin);
+  bool ok = true;
+  r.skip();
+  ok &= r.word(o->geometry_file, sizeof(o->geometry_file));
+  ok &= r.word(o->conc_file, sizeof(o->conc_file));
+  ok &= r.line(o->nx, o->ny, o->nz);
+  ok &= r.line(o->n_max);
+  ok &= r.line(o->reso);
+  ok &= r.line(o->in_bc);
+  ok &= r.line(o->buoyancy, o->ref_psi);
+  ok &= r.line(o->gravity);
+  ok &= r.line(o->gx, o->gy, o->gz);
+  ok &= r.line(o->pre_xp, o->p_xp, o->pre_xn, o->p_xn);
+  ok &= r.line(o->pre_yp, o->p_yp, o->pre_yn, o->p_yn);
+  ok &= r.line(o->pre_zp, o->p_zp, o->pre_zn, o->p_zn);
+  ok &= r.line(o->vel_xp, o->v_xp, o->vel_xn, o->v_xn);
+  ok &= r.line(o->vel_yp, o->v_yp, o->vel_yn, o->v_yn);
+  ok &= r.line(o->vel_zp, o->v_zp, o->vel_zn, o->v_zn);
+  ok &= r.line(o->sol_c_xp, o->c_xp, o->sol_c_xn, o->c_xn);
+  ok &= r.line(o->sol_c_yp, o->c_yp, o->sol_c_yn, o->c_yn);
+  ok &= r.line(o->sol_c_zp, o->c_zp, o->sol_c_zn, o->c_zn);
+  ok &= r.line(o->sol_zf_xp, o->zf_xp, o->sol_zf_xn, o->zf_xn);
+  ok &= r.line(o->sol_zf_yp, o->zf_yp, o->sol_zf_yn, o->zf_yn);
+  ok &= r.line(o->sol_zf_zp, o->zf_zp, o->sol_zf_zn, o->zf_zn);
+  ok &= r.line(o->nu);
+  ok &= r.line(o->nu_s);
+  ok &= r.line(o->inivx, o->inivy, o->inivz);
+  r.skip();
+  ok &= r.line(o->wr_per);
+  ok &= r.line(o->perdir);
+  ok &= r.line(o->fre_re);
+  ok &= r.line(o->out_mode);
+  ok &= r.line(o->fre_ve);
+  ok &= r.line(o->fre_de);
+  ok &= r.line(o->fre_psi);
+  ok &= r.line(o->sub_dis, o->fre_dis);
+  r.skip();
+  ok &= r.line(o->lattice_v, o->dx_input, o->dt_input);
+  ok &= r.word(o->output_path, sizeof(o->output_path));
+  ok &= r.line(o->sub_bc);
+  ok &= r.line(o->sub_bc_psi);
+  ok &= r.line(o->ini_psi);
+  ok &= r.line(o->par_per_x, o->par_per_y, o->par_per_z);
+  ok &= r.line(o->per_xp, o->per_xn);
+  ok &= r.line(o->per_yp, o->per_yn);
+  ok &= r.line(o->per_zp, o->per_zn);
+  r.skip();
+  ok &= r.line(o->fre_backup);
+  ok &= r.line(o->mode_backup_ini);
+  ok &= r.line(o->sol_ini_n);
+  r.skip();
+  r.skip();
+  ok &= r.line(o->decbin);
+  if (!ok) return fail(LBM_ERR_FORMAT, std::string("malformed input file ") + path);
+  if (o->nx <= 0 || o->ny <= 0 || o->nz <= 0)
+    return fail(LBM_ERR_FORMAT, "input file: non-positive grid size");
+  return LBM_OK;
+}
+
 // Phase file (CG3:2144-2150): nx*ny*nz numbers, k outer / j / i inner, each
 // stored as float.
 lbm_status read_phase_file(const char* path, int nx, int ny, int nz, double* out) {

@@ -38,6 +38,9 @@ std::vector<int32_t> slab_to_reference(const Geometry& g) {
 }
 
 }  // namespace
+
+lbm_status read_st7_input_file(const char* path, lbm_st7_input* o);
+
 }  // namespace lbm
 
 using namespace lbm;
@@ -201,6 +204,42 @@ lbm_status lbm_st7_get_concentration(lbm_st7_handle* h, double* c) {
   return LBM_OK;
 }
 
+lbm_status lbm_st7_get_populations(lbm_st7_handle* h, double* g) {
+  if (!h || !g) return fail(LBM_ERR_ARG, "lbm_st7_get_populations: bad argument");
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  const int n = h->geo.count;
+  Mem out;
+  const size_t bytes = sizeof(double) * (size_t)(n + 1) * 7;
+  LBM_CUDA_TRY(out.alloc(bytes));
+  LBM_CUDA_TRY(cudaMemsetAsync(out.p, 0, bytes, h->stream));
+  LBM_CUDA_TRY(st7_launch_export(h->f64, st7_args(h, false), static_cast<const int32_t*>(h->ref_of.p),
+                                 static_cast<double*>(out.p), h->stream));
+  LBM_CUDA_TRY(cudaMemcpyAsync(g, out.p, bytes, cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+lbm_status lbm_st7_set_state(lbm_st7_handle* h, const double* g, const double* c) {
+  if (!h || !g || !c) return fail(LBM_ERR_ARG, "lbm_st7_set_state: bad argument");
+  LBM_CUDA_TRY(cudaSetDevice(h->device));
+  const int n = h->geo.count, npad = h->geo.npad;
+  Mem in;
+  const size_t bytes = sizeof(double) * (size_t)(n + 1) * 7;
+  LBM_CUDA_TRY(in.alloc(bytes));
+  LBM_CUDA_TRY(cudaMemcpyAsync(in.p, g, bytes, cudaMemcpyHostToDevice, h->stream));
+  St7Args a = st7_args(h, true);
+  a.dst = h->g[h->cur].p;  // the buffer the next step pulls from
+  LBM_CUDA_TRY(st7_launch_import(h->f64, a, static_cast<const int32_t*>(h->ref_of.p), static_cast<const double*>(in.p),
+                                 h->stream));
+  // the first step takes C as given, like the restored rho_r of the reference
+  std::vector<double> cc((size_t)npad, 0.0);
+  for (int x = 0; x < n; x++) cc[x] = c[h->geo.ref_of[x]];
+  lbm_status st = upload_as(h, h->c0, cc);
+  if (st != LBM_OK) return st;
+  h->given = true;
+  return LBM_OK;
+}
+
 lbm_status lbm_st7_info(lbm_st7_handle* h, int* count, long long* step, double* last_step_ms) {
   if (!h) return fail(LBM_ERR_ARG, "null st7 handle");
   if (count) *count = h->geo.count;
@@ -273,6 +312,44 @@ lbm_status lbm_read_velocity_for_solute_ordered(const char* path, const uint8_t*
   const std::vector<int32_t> slab = slab_to_reference(g);
   for (int s = 0; s < g.count; s++)
     for (int d = 0; d < 3; d++) u_nodes[(size_t)slab[s] * 3 + d] = in[(size_t)s * 3 + d];
+  return LBM_OK;
+}
+
+lbm_status lbm_read_st7_input(const char* path, lbm_st7_input* out) { return read_st7_input_file(path, out); }
+
+// x-slab decomposition of the slab programs (ST7:951-975, the same steps in
+// the single-phase slab program): rank r takes the x-planes
+// [first_x[r], first_x[r+1]); the cut after rank r is the plane boundary
+// whose cumulative pore count is nearest to (r+1)/nranks of all pores, the
+// later plane on a tie.
+lbm_status lbm_slab_partition(const uint8_t* mask, int nx, int ny, int nz, int nranks, int* first_x) {
+  if (!mask || !first_x || nx <= 0 || ny <= 0 || nz <= 0 || nranks <= 0)
+    return fail(LBM_ERR_ARG, "lbm_slab_partition: bad argument");
+  std::vector<long long> plane(nx, 0);
+  long long sum = 0;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        if (mask[i + (size_t)nx * (j + (size_t)ny * k)] == 0) {
+          plane[i]++;
+          sum++;
+        }
+  const double ave = (double)sum / nranks;
+  first_x[0] = 0;
+  for (int r = 0; r < nranks - 1; r++) {
+    long long pre = 0, aft = 0;
+    int ni = 0;
+    while (aft < ave * (r + 1)) {
+      if (ni >= nx) return fail(LBM_ERR_ARG, "lbm_slab_partition: more ranks than x-planes with pores");
+      pre = aft;
+      aft += plane[ni];
+      ni++;
+    }
+    first_x[r + 1] = ((double)(aft - ave * (r + 1)) > (double)(ave * (r + 1) - pre)) ? ni - 1 : ni;
+  }
+  first_x[nranks] = nx;
+  for (int r = 0; r < nranks; r++)
+    if (first_x[r + 1] < first_x[r]) return fail(LBM_ERR_ARG, "lbm_slab_partition: empty slab");
   return LBM_OK;
 }
 

@@ -19,5 +19,8 @@ struct St7Args {
 cudaError_t st7_launch_step(bool f64, const St7Args& a, cudaStream_t st);
 cudaError_t st7_launch_conc(bool f64, const St7Args& a, double* out, cudaStream_t st);
 cudaError_t st7_launch_init(bool f64, const St7Args& a, cudaStream_t st);
+// a.src: the state to export; a.dst: the buffer the next step pulls from
+cudaError_t st7_launch_export(bool f64, const St7Args& a, const int32_t* ref_of, double* out, cudaStream_t st);
+cudaError_t st7_launch_import(bool f64, const St7Args& a, const int32_t* ref_of, const double* in, cudaStream_t st);
 
 }  // namespace lbm

@@ -84,7 +84,52 @@ __global__ void st7_init_kernel(St7Args a) {
   }
 }
 
+// g as the next step pulls it, [(count+1)*7] in reference id order
+// (column 0 unused), and its inverse.
+template <typename T>
+__global__ void st7_export_kernel(St7Args a, const int32_t* __restrict__ ref_of, double* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  const T* __restrict__ src = static_cast<const T*>(a.src);
+  const size_t npad = (size_t)a.npad;
+  double* row = out + (size_t)ref_of[x] * 7;
+  row[0] = 0.0;
+#pragma unroll
+  for (int q = 1; q < 7; q++) row[q] = (double)src[a.table[(size_t)(q - 1) * npad + x] - npad];
+}
+
+template <typename T>
+__global__ void st7_import_kernel(St7Args a, const int32_t* __restrict__ ref_of, const double* __restrict__ in) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  T* __restrict__ dst = static_cast<T*>(a.dst);
+  const size_t npad = (size_t)a.npad;
+  const double* row = in + (size_t)ref_of[x] * 7;
+#pragma unroll
+  for (int q = 1; q < 7; q++) dst[a.table[(size_t)(q - 1) * npad + x] - npad] = (T)row[q];
+}
+
 }  // namespace
+
+cudaError_t st7_launch_export(bool f64, const St7Args& a, const int32_t* ref_of, double* out, cudaStream_t st) {
+  if (a.n == 0) return cudaSuccess;
+  const int g = (a.n + 255) / 256;
+  if (f64)
+    st7_export_kernel<double><<<g, 256, 0, st>>>(a, ref_of, out);
+  else
+    st7_export_kernel<float><<<g, 256, 0, st>>>(a, ref_of, out);
+  return cudaGetLastError();
+}
+
+cudaError_t st7_launch_import(bool f64, const St7Args& a, const int32_t* ref_of, const double* in, cudaStream_t st) {
+  if (a.n == 0) return cudaSuccess;
+  const int g = (a.n + 255) / 256;
+  if (f64)
+    st7_import_kernel<double><<<g, 256, 0, st>>>(a, ref_of, in);
+  else
+    st7_import_kernel<float><<<g, 256, 0, st>>>(a, ref_of, in);
+  return cudaGetLastError();
+}
 
 cudaError_t st7_launch_step(bool f64, const St7Args& a, cudaStream_t st) {
   if (a.n == 0) return cudaSuccess;

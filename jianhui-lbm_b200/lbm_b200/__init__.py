@@ -183,6 +183,33 @@ class CGInput(C.Structure):
     as_dict = Input.as_dict
 
 
+class ST7Input(C.Structure):
+    _fields_ = [
+        ("geometry_file", C.c_char * 256), ("conc_file", C.c_char * 256),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("n_max", C.c_int), ("reso", C.c_double),
+        ("in_bc", C.c_int), ("buoyancy", C.c_double), ("ref_psi", C.c_double), ("gravity", C.c_double),
+        ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+    ] + [item for ax in "xyz" for item in ((f"pre_{ax}p", C.c_int), (f"p_{ax}p", C.c_double),
+                                          (f"pre_{ax}n", C.c_int), (f"p_{ax}n", C.c_double))] \
+      + [item for ax in "xyz" for item in ((f"vel_{ax}p", C.c_int), (f"v_{ax}p", C.c_double),
+                                          (f"vel_{ax}n", C.c_int), (f"v_{ax}n", C.c_double))] \
+      + [item for ax in "xyz" for item in ((f"sol_c_{ax}p", C.c_int), (f"c_{ax}p", C.c_double),
+                                          (f"sol_c_{ax}n", C.c_int), (f"c_{ax}n", C.c_double))] \
+      + [item for ax in "xyz" for item in ((f"sol_zf_{ax}p", C.c_int), (f"zf_{ax}p", C.c_double),
+                                          (f"sol_zf_{ax}n", C.c_int), (f"zf_{ax}n", C.c_double))] \
+      + [("nu", C.c_double), ("nu_s", C.c_double), ("inivx", C.c_double), ("inivy", C.c_double),
+         ("inivz", C.c_double), ("wr_per", C.c_int), ("perdir", C.c_int), ("fre_re", C.c_int),
+         ("out_mode", C.c_int), ("fre_ve", C.c_int), ("fre_de", C.c_int), ("fre_psi", C.c_int),
+         ("sub_dis", C.c_int), ("fre_dis", C.c_int), ("lattice_v", C.c_int), ("dx_input", C.c_double),
+         ("dt_input", C.c_double), ("output_path", C.c_char * 256), ("sub_bc", C.c_int), ("sub_bc_psi", C.c_int),
+         ("ini_psi", C.c_int), ("par_per_x", C.c_int), ("par_per_y", C.c_int), ("par_per_z", C.c_int),
+         ("per_xp", C.c_int), ("per_xn", C.c_int), ("per_yp", C.c_int), ("per_yn", C.c_int),
+         ("per_zp", C.c_int), ("per_zn", C.c_int), ("fre_backup", C.c_int), ("mode_backup_ini", C.c_int),
+         ("sol_ini_n", C.c_int), ("decbin", C.c_int)]
+
+    as_dict = Input.as_dict
+
+
 class CGDiag(C.Structure):
     _fields_ = [("step", C.c_longlong), ("saturation", C.c_double), ("q_l", C.c_double * 3),
                 ("q_g", C.c_double * 3), ("perm_l", C.c_double * 3), ("perm_g", C.c_double * 3),
@@ -269,6 +296,10 @@ _SIGNATURES = {
     "lbm_st7_get_concentration": ([C.c_void_p, _F64P], C.c_int),
     "lbm_st7_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_double)], C.c_int),
     "lbm_st7_destroy": ([C.c_void_p], None),
+    "lbm_st7_get_populations": ([C.c_void_p, _F64P], C.c_int),
+    "lbm_st7_set_state": ([C.c_void_p, _F64P, _F64P], C.c_int),
+    "lbm_read_st7_input": ([C.c_char_p, C.POINTER(ST7Input)], C.c_int),
+    "lbm_slab_partition": ([_U8P, C.c_int, C.c_int, C.c_int, C.c_int, _I32P], C.c_int),
     "lbm_write_velocity_for_solute": ([C.c_void_p, C.c_char_p], C.c_int),
     "lbm_read_velocity_for_solute": ([C.c_char_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
     "lbm_write_velocity_for_solute_ordered": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
@@ -310,8 +341,8 @@ def read_checkpoint(flow, prefix, m):
 
 def driver_path(name="lbm_sp"):
     """Path of a command-line driver built beside liblbm.so: ``lbm_sp``
-    (single phase) or ``lbm_cg`` (colour gradient)."""
-    if name not in ("lbm_sp", "lbm_cg"):
+    (single phase), ``lbm_cg`` (colour gradient) or ``lbm_st7`` (solute)."""
+    if name not in ("lbm_sp", "lbm_cg", "lbm_st7"):
         raise ValueError(f"unknown driver {name!r}")
     return os.path.join(os.path.dirname(os.path.abspath(__file__)), name)
 
@@ -350,6 +381,17 @@ class Solute:
         c = np.zeros(self.count + 1)
         _check(lib().lbm_st7_get_concentration(self._h, c))
         return c
+
+    def populations(self):
+        """g as the next step reads it, [(count+1), 7] (column 0 unused)."""
+        g = np.zeros((self.count + 1) * 7)
+        _check(lib().lbm_st7_get_populations(self._h, g))
+        return g.reshape(-1, 7)
+
+    def set_state(self, g, c):
+        """Restores g [(count+1), 7] and C [(count+1)]; the next step takes C as given."""
+        arr = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        _check(lib().lbm_st7_set_state(self._h, arr(g), arr(c)))
 
     def last_step_ms(self):
         """Device time of the last step() call in ms (CUDA events on the solver's stream)."""
@@ -682,6 +724,23 @@ def read_cg_input(path):
     out = CGInput()
     _check(lib().lbm_read_cg_input(os.fsencode(path), C.byref(out)))
     return out.as_dict()
+
+
+def read_st7_input(path):
+    """INPUT file of the solute program as a dict (field order ST7:219-280)."""
+    out = ST7Input()
+    _check(lib().lbm_read_st7_input(os.fsencode(path), C.byref(out)))
+    return out.as_dict()
+
+
+def slab_partition(mask, nranks):
+    """x-slab split of the slab programs (ST7:951-975) of a [nz, ny, nx] mask:
+    rank r holds the x-planes first[r] .. first[r+1]-1."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    nz, ny, nx = m.shape
+    first = np.zeros(int(nranks) + 1, dtype=np.int32)
+    _check(lib().lbm_slab_partition(m.reshape(-1), nx, ny, nz, int(nranks), first))
+    return first
 
 
 def read_phase(path, shape):

@@ -2,7 +2,8 @@
 solver itself: Single_Phase_3D/SINGLE_PHASE_MPI_Software_Spars_3DPartition.cpp
 compiled from its own source (oracle/Makefile -> oracle/_ref/libref_sp3.so).
 
-    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --cg-outputs | --bc | --st7 | --slab-perm]
+    python tests/golden/make_golden.py [--cfg1 | --cg | --outputs | --cg-outputs | --bc | --st7 | --st7-outputs |
+                                        --slab-perm]
 
 Fixtures (all inputs are stored with the outputs, so nothing depends on a
 random generator at test time):
@@ -15,6 +16,9 @@ random generator at test time):
                 its checkpoint, see cg_program_outputs()  (--cg-outputs)
   sp_bc.npz     pressure/velocity boundaries, Sub_BC 0..3, see bc_fixture()  (--bc)
   st7_slab.npz  the solute program at two ranks, see st7_fixture()  (--st7)
+  st7_outputs*.npz  every file the solute program writes at two ranks (both
+                output layouts, and a restart), see st7_program_outputs()
+                (--st7-outputs)
   sp_slab_perm.npz  the slab single-phase program at two ranks with its
                 local and group permeabilities, see slab_perm_fixture()  (--slab-perm)
   sp_small.npz  12x10x8 overlapping spheres, 20 steps: compaction, nei_loc,
@@ -268,7 +272,7 @@ def collect_cg(workdir, prefix):
         key = name[len(prefix):]
         data = open(os.path.join(workdir, name), "rb").read()
         if key.startswith("LBM_checkpoint_"):
-            width = {"rho": 1, "velocity": 3, "f": 19, "psi": 1, "rhor": 1, "rhob": 1}[key.split("_")[2]]
+            width = {"rho": 1, "velocity": 3, "f": 19, "psi": 1, "rhor": 1, "rhob": 1, "fg": 7}[key.split("_")[2]]
             out[key] = digest(np.frombuffer(data, dtype=np.float64).reshape(-1, width)[1:])
         else:
             out[key] = data
@@ -401,6 +405,66 @@ def st7_fixture(out=None):
     print("st7_slab", mask.shape, [v.size // 3 for v in vel])
 
 
+def st7_program_outputs():
+    """The solute program itself at two ranks (multi-process MPI stand-in):
+    every file it writes, for the drop-in driver's byte-for-byte test.  The
+    slab single-phase program first makes the flow of the st7_slab geometry
+    (Velocity_for_solute_100.<rank>.bin, stored verbatim); then the solute
+    program runs 61 steps with reports every 20, velocity VTK every 40,
+    concentration VTK every 20, checkpoints every 40, solids written as 0.5,
+    in both output layouts (Out_Mode 1: st7_outputs.npz, Out_Mode 0:
+    st7_outputs_b.npz); and a restart from the step-40 checkpoint (copied to
+    the unprefixed names Backup_init reads) runs 31 more steps
+    (st7_outputs_restart.npz)."""
+    import shutil
+    import tempfile
+
+    sp, st = oracle.slab_program("ref_sp_slab"), oracle.slab_program("ref_st7_slab")
+    if not (sp and st):
+        raise SystemExit("oracle/_ref/ref_sp_slab and ref_st7_slab are needed (make -C oracle ref)")
+    mask = G.overlapping_spheres(ST7_SHAPE, 0.6, 2.5, seed=ST7_SEED)
+    nx, ny, nz = ST7_SHAPE
+    c0 = np.random.default_rng(5).uniform(0, 1, mask.shape).astype(np.float32)
+    phase = "\n".join(repr(float(v)) for v in c0.reshape(-1)) + "\n"
+    with tempfile.TemporaryDirectory() as d:
+        G.write_ascii(os.path.join(d, "mask.dat"), mask)
+        flow = input_text(L1="mask.dat", L2=f"{nx} {ny} {nz}", L3=100, L18=50, L20=-1, L21=-1, L24="./", L32=-1,
+                          L34=100)
+        open(os.path.join(d, "INPUT.dat"), "w").write(flow)
+        assert oracle.run_ranks(sp, ["INPUT.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
+        vel = {f"Velocity_for_solute_100.{r}.bin": open(os.path.join(d, f"Velocity_for_solute_100.{r}.bin"), "rb").read()
+               for r in range(ST7_NRANKS)}
+        open(os.path.join(d, "phase.dat"), "w").write(phase)
+        runs = {"st7_outputs.npz": ("./st_", dict(L29=1)), "st7_outputs_b.npz": ("./sb_", dict(L29=0))}
+        for fname, (prefix, kv) in runs.items():
+            text = solute_input(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=60, L7="0.0 0.5", L23=ST7_D,
+                                L28=20, L30=40, L32=20, L33="0 1000", L36=prefix, L45=40, L47=100, **kv)
+            open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
+            assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
+            save_st7(fname, mask, phase, text, vel, collect_cg(d, prefix[2:]))
+        for r in range(ST7_NRANKS):
+            for what in ("psi", "fg"):
+                shutil.copy(os.path.join(d, f"st_LBM_checkpoint_{what}_40.{r}.bin_input"),
+                            os.path.join(d, f"LBM_checkpoint_{what}_40.{r}.bin_input"))
+        text = solute_input(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=30, L7="0.0 0.5", L23=ST7_D,
+                            L28=10, L29=1, L30=-1, L32=30, L33="0 1000", L36="./rs_", L45=-1, L46=40, L47=100)
+        open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
+        assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
+        save_st7("st7_outputs_restart.npz", mask, phase, text, vel, collect_cg(d, "rs_"))
+
+
+def save_st7(fname, mask, phase, text, vel, files):
+    blob = {"mask": pack(mask), "shape": np.array(mask.shape), "phase": np.frombuffer(phase.encode(), np.uint8),
+            "input": np.frombuffer(text.encode(), np.uint8), "nranks": ST7_NRANKS,
+            "names": np.array(sorted(files)), "velocity_files": np.array(sorted(vel))}
+    for k, v in vel.items():
+        blob["file:" + k] = np.frombuffer(v, np.uint8)
+    for k, v in files.items():
+        blob[k] = np.frombuffer(v, np.uint8) if isinstance(v, bytes) else np.array(v)
+    np.savez_compressed(os.path.join(HERE, fname), **blob)
+    print(fname, sorted(files))
+
+
 SLAB_GROUPS = dict(n_sub=[1, 2, 0, 0], size=[8, 4, 1, 1], corner=[0, 0, 0, 2, 2, 1, 0, 0, 0, 0, 0, 0])
 
 
@@ -444,8 +508,12 @@ def main():
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
     ap.add_argument("--cg-outputs", action="store_true")
+    ap.add_argument("--st7-outputs", action="store_true")
     a = ap.parse_args()
     oracle.build()
+    if a.st7_outputs:
+        st7_program_outputs()
+        return
     if a.cg_outputs:
         cg_program_outputs()
         return

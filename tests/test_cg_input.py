@@ -91,3 +91,27 @@ def test_cg_driver_refuses_options_outside_its_scope(L, tmp_path, lines, field):
     with pytest.raises(L.LbmError) as e:
         L.ColourGradient.from_input(str(tmp_path / "INPUT.dat"))
     assert e.value.status == -1 and field in str(e.value), str(e.value)
+
+
+def test_st7_input_field_order_and_slab_partition(L, tmp_path):
+    """The solute program's INPUT file (ST7:219-280) and its x-slab split
+    (ST7:951-975) against the rank sizes the reference itself produced."""
+    g = np.load(os.path.join(GOLDEN, "st7_outputs.npz"))
+    p = tmp_path / "INPUT_st.dat"
+    p.write_bytes(g["input"].tobytes())
+    d = L.read_st7_input(str(p))
+    assert (d["geometry_file"], d["conc_file"], d["nx"], d["ny"], d["nz"], d["n_max"]) == (
+        "mask.dat", "phase.dat", 16, 10, 8, 60)
+    assert (d["buoyancy"], d["ref_psi"], d["nu"], d["nu_s"]) == (0.0, 0.5, 0.05, 0.005)
+    assert (d["fre_re"], d["out_mode"], d["fre_ve"], d["fre_psi"], d["sub_dis"], d["fre_dis"]) == (20, 1, 40, 20, 0,
+                                                                                                 1000)
+    assert (d["output_path"], d["fre_backup"], d["mode_backup_ini"], d["sol_ini_n"], d["decbin"]) == (
+        "./st_", 40, 0, 100, 0)
+    shape = tuple(int(s) for s in g["shape"])
+    mask = np.unpackbits(g["mask"])[: np.prod(shape)].reshape(shape)
+    first = L.slab_partition(mask, 2)
+    sizes = [(mask[:, :, first[r]:first[r + 1]] == 0).sum() for r in range(2)]
+    # the slab program wrote Count*3 velocities per rank
+    assert sizes == [g["file:Velocity_for_solute_100.%d.bin" % r].size // 24 for r in range(2)]
+    st = np.load(os.path.join(GOLDEN, "st7_slab.npz"))
+    assert sizes == [int(v) for v in st["rank_nodes"]]
