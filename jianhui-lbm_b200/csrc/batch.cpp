@@ -1,6 +1,7 @@
 // Node pool shared by lbm_batch (a fixed set of solves) and lbm_server
 // (continuous batching of a request stream).
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -100,7 +101,7 @@ struct Pool {
   int block = 256, grid = 0;
   int ordering = LBM_ORDER_REFERENCE;
   double fp16_scale = 1.0;
-  Buf pop[2], table, tile_inst, inst, state, partials, active_tiles, n_active;
+  Buf pop[2], table, tile_inst, inst, state, partials, active_tiles, n_active, work;
   SetupScratch setup;
   std::vector<InstParams> h_inst;
   InstState* h_state = nullptr;  // pinned
@@ -109,7 +110,9 @@ struct Pool {
   std::vector<std::unique_ptr<Job>> slot_job;
   std::vector<int> slot_parity;  // buffer holding a finished slot's state
   int cur = 0;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // chain graphs per step grid (the grid follows the stepping tile count,
+  // rounded up to a power of two, so a few graphs cover every pool state)
+  std::map<int, std::array<cudaGraphExec_t, 2>> graphs;
   int g_chain = 0;
   double g_tol = 0;
   long long g_max = 0;
@@ -123,11 +126,24 @@ struct Pool {
     if (stream) cudaStreamDestroy(stream);
   }
   void drop_graphs() {
-    for (auto& g : graph)
-      if (g) {
-        cudaGraphExecDestroy(g);
-        g = nullptr;
-      }
+    for (auto& kv : graphs)
+      for (auto& g : kv.second)
+        if (g) cudaGraphExecDestroy(g);
+    graphs.clear();
+  }
+
+  // Step grid of a chain: one block per work item (block nodes of a
+  // stepping tile), rounded up to a power of two, at most the pool's full
+  // grid.  Any grid is correct (the kernel strides); this one neither idles
+  // blocks on a small stepping set nor starves a large one.
+  int chain_grid() const {
+    long long tiles = 0;
+    for (int i = 0; i < nslots; i++)
+      if (slot_job[i] && h_state[i].active) tiles += h_inst[i].tile_end - h_inst[i].tile_begin;
+    const long long items = std::max(1LL, tiles * (kTile / block));
+    long long g = 1;
+    while (g < items) g <<= 1;
+    return (int)std::min<long long>(g, grid);
   }
 
   lbm_status init(Store k, long long cap_nodes, int slots, int blk, int dev, int order, double f16) {
@@ -154,6 +170,7 @@ struct Pool {
     LBM_CUDA_TRY(state.alloc((size_t)nslots * sizeof(InstState)));
     LBM_CUDA_TRY(partials.alloc((size_t)ntiles * 8 * sizeof(double)));
     LBM_CUDA_TRY(active_tiles.alloc((size_t)ntiles * sizeof(int)));
+    LBM_CUDA_TRY(work.alloc((size_t)ntiles * sizeof(TileWork)));
     LBM_CUDA_TRY(n_active.alloc(sizeof(int)));
     LBM_CUDA_TRY(cudaMemsetAsync(n_active.p, 0, sizeof(int), stream));
     LBM_CUDA_TRY(cudaMallocHost((void**)&h_state, (size_t)nslots * sizeof(InstState)));
@@ -168,7 +185,7 @@ struct Pool {
                                  cudaMemcpyHostToDevice, stream));
     LBM_CUDA_TRY(cudaMemcpyAsync(state.p, h_state, (size_t)nslots * sizeof(InstState), cudaMemcpyHostToDevice,
                                  stream));
-    grid = batch_step_grid(kind, block);
+    grid = batch_step_grid(ntiles, block);
     return LBM_OK;
   }
 
@@ -285,6 +302,7 @@ struct Pool {
     a.state = state.as<InstState>();
     a.active_tiles = active_tiles.as<int>();
     a.n_active = n_active.as<int>();
+    a.work = work.as<TileWork>();
     return a;
   }
   BatchReduceArgs reduce_args(int c) const {
@@ -300,10 +318,11 @@ struct Pool {
     r.tile_partials = partials.as<double>();
     r.active_tiles = active_tiles.as<int>();
     r.n_active = n_active.as<int>();
+    r.work = work.as<TileWork>();
     return r;
   }
 
-  lbm_status capture(int c0, int chain, double tol, long long max_steps) {
+  lbm_status capture(int c0, int chain, double tol, long long max_steps, int step_grid, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     LBM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     // the chain starts from the current set of stepping slots (admissions and
@@ -311,7 +330,7 @@ struct Pool {
     cudaError_t err = launch_batch_list(reduce_args(c0), stream);
     int c = c0;
     for (int s = 0; s < chain && err == cudaSuccess; s++) {
-      err = launch_batch_step(kind, step_args(c), block, grid, s, stream);
+      err = launch_batch_step(kind, step_args(c), block, step_grid, s, stream);
       c = 1 - c;
     }
     if (err == cudaSuccess) err = launch_batch_check(kind, reduce_args(c), chain, tol, max_steps, stream);
@@ -320,7 +339,7 @@ struct Pool {
       if (g) cudaGraphDestroy(g);
       return fail(LBM_ERR_CUDA, std::string("pool graph capture: ") + cudaGetErrorString(err ? err : end));
     }
-    const cudaError_t inst_e = cudaGraphInstantiate(&graph[c0], g, 0);
+    const cudaError_t inst_e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     LBM_CUDA_TRY(inst_e);
     return LBM_OK;
@@ -336,11 +355,15 @@ struct Pool {
       g_max = max_steps;
       g_block = block;
     }
-    if (!graph[cur]) {
-      lbm_status st = capture(cur, chain, tol, max_steps);
+    const int step_grid = chain_grid();
+    auto it = graphs.find(step_grid);
+    if (it == graphs.end()) it = graphs.emplace(step_grid, std::array<cudaGraphExec_t, 2>{nullptr, nullptr}).first;
+    cudaGraphExec_t& ge = it->second[cur];
+    if (!ge) {
+      lbm_status st = capture(cur, chain, tol, max_steps, step_grid, &ge);
       if (st != LBM_OK) return st;
     }
-    LBM_CUDA_TRY(cudaGraphLaunch(graph[cur], stream));
+    LBM_CUDA_TRY(cudaGraphLaunch(ge, stream));
     cur = (chain & 1) ? 1 - cur : cur;
     LBM_CUDA_TRY(cudaMemcpyAsync(h_state, state.p, (size_t)nslots * sizeof(InstState), cudaMemcpyDeviceToHost,
                                  stream));
@@ -601,7 +624,7 @@ lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* ordering_out, 
     if ((st = batch_layout(b)) != LBM_OK) return st;
     for (int bl : blocks) {
       P.block = bl;
-      P.grid = batch_step_grid(P.kind, bl);
+      P.grid = batch_step_grid(P.ntiles, bl);
       if ((st = batch_reset(b)) != LBM_OK) return st;
       LBM_CUDA_TRY(launch_batch_list(P.reduce_args(P.cur), P.stream));
       for (int s = 0; s < 2; s++) {  // warm-up
@@ -627,7 +650,7 @@ lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* ordering_out, 
   }
   P.ordering = best_o;
   P.block = best_b;
-  P.grid = batch_step_grid(P.kind, best_b);
+  P.grid = batch_step_grid(P.ntiles, best_b);
   if ((st = batch_layout(b)) != LBM_OK) return st;
   if ((st = batch_reset(b)) != LBM_OK) return st;
   P.drop_graphs();

@@ -31,6 +31,17 @@ struct InstState {
   int done;    // 0 running, 1 converged, 2 step cap, 3 non-finite
 };
 
+// One stepping tile of a chain, written by the list kernel so that a step
+// block needs one broadcast load before its population gathers.
+struct TileWork {
+  int p0, end;  // first node of the tile; end of its instance's node range
+  float g[3];
+  float s_v, s_o;
+  float fp16_scale;
+  float u0[3];
+  int fresh;    // first step of a newly admitted instance: rho = 1, u = u0
+};
+
 struct BatchStepArgs {
   const void* src_pop;
   void* dst_pop;
@@ -42,6 +53,7 @@ struct BatchStepArgs {
   const InstState* state;
   const int* active_tiles;  // tiles of stepping slots, ascending
   const int* n_active;      // its length (device scalar)
+  const TileWork* work;     // [n_active] per stepping tile
 };
 
 struct BatchReduceArgs {
@@ -56,6 +68,7 @@ struct BatchReduceArgs {
   double* tile_partials;  // [ntiles][8]
   int* active_tiles;
   int* n_active;
+  TileWork* work;
 };
 
 // Rebuilds the active tile list from tile ownership and slot states.
@@ -70,7 +83,9 @@ cudaError_t launch_batch_export_macro(Store kind, const void* pop, const int32_t
                                       cudaStream_t st);
 cudaError_t launch_batch_init(Store kind, void* pop, const int32_t* table, int cap, int begin, int n,
                               const InstParams& ip, cudaStream_t st);
-int batch_step_grid(Store kind, int block);
+// Largest step grid of a pool: eight waves of resident blocks, or fewer when
+// the pool holds fewer work items (block nodes of a tile).
+int batch_step_grid(int ntiles, int block);
 
 // The 18 table rows [18][g.count] of one instance placed at node `begin` of a
 // pool with row stride `cap` (flat pool indices q*cap + begin + m).

@@ -5,9 +5,11 @@
 // [18][cap] whose entries are flat indices q*cap + m into the same pool (an
 // instance only ever pulls from its own range).  The pool is cut into tiles
 // of kTile nodes; tile_inst[t] names the instance slot owning tile t (-1 =
-// free).  One persistent kernel walks the tiles of all instances each step
-// and skips tiles of free or finished slots, so the launch shape -- and the
-// captured CUDA graph -- never changes while instances come and go.
+// free).  At the start of every chain a list kernel compacts the tiles of
+// stepping slots into a work list (with each tile's constants); the step
+// kernel strides over that list, so any grid is correct and the captured
+// CUDA graph of a chain only depends on the grid the host picks for the
+// stepping tile count (one graph per power of two).
 //
 // Convergence is decided on the device: every chain of check_every steps ends
 // with a per-tile sum of u, a per-instance sum of its tiles in fixed order
@@ -19,52 +21,47 @@
 
 namespace lbm {
 
+// Work item = BS nodes of a stepping tile (the tiles in the active list
+// order, kTile / BS items per tile).  The grid strides over the items; tile
+// constants come from the list kernel's TileWork record, so the population
+// gathers of an item wait on a single broadcast load, as in the
+// single-domain step.  The host sizes the grid per chain to the stepping
+// tile count (at most eight waves of resident blocks), so idle pool capacity
+// launches no blocks.
 template <Store K, int BS>
 __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
   using T = typename Traits<K>::T;
   using A = typename Traits<K>::A;
+  constexpr int kSub = kTile / BS;
+  const int items = *a.n_active * kSub;
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
   const size_t cap = (size_t)a.cap;
-  const int na = *a.n_active;
-  // tile -> slot lookups of the next tile are issued before this tile's
-  // work, so their latency hides behind it instead of starting every tile
-  int i = blockIdx.x;
-  int t_next = i < na ? a.active_tiles[i] : 0;
-  int s_next = i < na ? a.tile_inst[t_next] : 0;
-  for (; i < na; i += gridDim.x) {
-    const int t = t_next, slot = s_next;
-    if (i + (int)gridDim.x < na) {
-      t_next = a.active_tiles[i + gridDim.x];
-      s_next = a.tile_inst[t_next];
-    }
-    const InstParams ip = a.inst[slot];
-    const bool given = (chain_step == 0) && a.state[slot].fresh;
-    const float scale = ip.fp16_scale, inv_scale = 1.0f / ip.fp16_scale;
-#pragma unroll 1
-    for (int k = threadIdx.x; k < kTile; k += BS) {
-      const int p = t * kTile + k;
-      if (p >= ip.end) break;
-      A f[kQ];
-      f[0] = load_pop<K>(src + p, inv_scale);
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const int i = it / kSub;
+    const TileWork w = a.work[i];
+    const int p = w.p0 + (it - i * kSub) * BS + threadIdx.x;
+    if (p >= w.end) continue;
+    const float scale = w.fp16_scale, inv_scale = 1.0f / w.fp16_scale;
+    A f[kQ];
+    f[0] = load_pop<K>(src + p, inv_scale);
 #pragma unroll
-      for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(src + __ldg(a.table + (size_t)(q - 1) * cap + p), inv_scale);
-      PairSplit<A> ps;
-      split_pairs(f, ps);
-      A drho, rho, ux, uy, uz;
-      if (given) {
-        rho = A(1);
-        drho = A(0);
-        ux = A(ip.u0[0]);
-        uy = A(ip.u0[1]);
-        uz = A(ip.u0[2]);
-      } else {
-        macro_dev<A>(f, ps, A(0.5f * ip.g[0]), A(0.5f * ip.g[1]), A(0.5f * ip.g[2]), drho, rho, ux, uy, uz);
-      }
-      mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(ip.g[0]), A(ip.g[1]), A(ip.g[2]), A(ip.s_v), A(ip.s_o));
-#pragma unroll
-      for (int q = 0; q < kQ; q++) store_pop<K>(dst + (size_t)q * cap + p, f[q], scale);
+    for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(src + __ldg(a.table + (size_t)(q - 1) * cap + p), inv_scale);
+    PairSplit<A> ps;
+    split_pairs(f, ps);
+    A drho, rho, ux, uy, uz;
+    if (chain_step == 0 && w.fresh) {
+      rho = A(1);
+      drho = A(0);
+      ux = A(w.u0[0]);
+      uy = A(w.u0[1]);
+      uz = A(w.u0[2]);
+    } else {
+      macro_dev<A>(f, ps, A(0.5f * w.g[0]), A(0.5f * w.g[1]), A(0.5f * w.g[2]), drho, rho, ux, uy, uz);
     }
+    mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(w.g[0]), A(w.g[1]), A(w.g[2]), A(w.s_v), A(w.s_o));
+#pragma unroll
+    for (int q = 0; q < kQ; q++) store_pop<K>(dst + (size_t)q * cap + p, f[q], scale);
   }
 }
 
@@ -90,7 +87,22 @@ __global__ void __launch_bounds__(1024) batch_list_kernel(BatchReduceArgs a) {
   int w = counts[threadIdx.x] - c;
   for (int t = lo; t < hi; t++) {
     const int s = a.tile_inst[t];
-    if (s >= 0 && a.state[s].active) a.active_tiles[w++] = t;
+    if (s >= 0 && a.state[s].active) {
+      const InstParams& ip = a.inst[s];
+      TileWork tw;
+      tw.p0 = t * kTile;
+      tw.end = ip.end;
+      for (int d = 0; d < 3; d++) {
+        tw.g[d] = ip.g[d];
+        tw.u0[d] = ip.u0[d];
+      }
+      tw.s_v = ip.s_v;
+      tw.s_o = ip.s_o;
+      tw.fp16_scale = ip.fp16_scale;
+      tw.fresh = a.state[s].fresh;
+      a.work[w] = tw;
+      a.active_tiles[w++] = t;
+    }
   }
   if (threadIdx.x == 1023) *a.n_active = counts[1023];
 }
@@ -242,23 +254,21 @@ static cudaError_t step_k(const BatchStepArgs& a, int block, int grid, int chain
   return cudaGetLastError();
 }
 
-// Persistent launch shape: as many resident blocks as the SMs hold.
-int batch_step_grid(Store kind, int block) {
+int batch_step_grid(int ntiles, int block) {
+  const int b = (block == 128 || block == 512) ? block : 256;
   int dev = 0, sms = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaErrorInvalidValue;
-  if (kind == Store::F16) {
-    if (block == 128) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F16, 128>, 128, 0);
-    else if (block == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F16, 512>, 512, 0);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F16, 256>, 256, 0);
-  } else {
-    if (block == 128) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 128>, 128, 0);
-    else if (block == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 512>, 512, 0);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 256>, 256, 0);
-  }
+  cudaError_t e;
+  if (b == 128)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 128>, 128, 0);
+  else if (b == 512)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 512>, 512, 0);
+  else
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 256>, 256, 0);
   if (e != cudaSuccess || per < 1) per = 1;
-  return sms * per;
+  const long long waves = 8LL * sms * per, items = (long long)ntiles * (kTile / b);
+  return (int)std::max(1LL, std::min(waves, items));
 }
 
 cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int grid, int chain_step,
