@@ -39,7 +39,7 @@ CUDA_SOURCES = [
     ("st7_kernels.cu", ["-fmad=false"]),
     ("box_sums.cu", []),
 ]
-CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp", "output.cpp"]
+CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp", "output.cpp", "transfer.cpp"]
 # Command-line drivers linked against liblbm.so: (source, executable name).
 EXECUTABLES = [("lbm_sp_main.cpp", "lbm_sp"), ("lbm_cg_main.cpp", "lbm_cg"), ("lbm_st7_main.cpp", "lbm_st7")]
 BIN = os.path.join(HERE, "lbm_b200")

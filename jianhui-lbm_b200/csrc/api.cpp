@@ -79,6 +79,9 @@ struct lbm_handle {
   // dense cell -> internal index map for box sums, built on first use
   DevBuf cell_idx;
   bool cell_idx_valid = false;
+  // field export: device buffers kept between calls, pinned staging
+  DevBuf x_rint, x_uint, x_rref, x_uref;
+  PinnedStage stage;
   int cur = 0;
   long long step = 0;
   bool given_macro = true;  // next step / reduce takes rho, u from rho_given / u_given
@@ -691,11 +694,11 @@ lbm_status lbm_get_fields(lbm_handle* h, double* rho, double* u) {
   lbm_status st = check_handle(h);
   if (st != LBM_OK) return st;
   const int n = h->geo.count, npad = h->geo.npad;
-  DevBuf rint, uint_, rref, uref;
-  LBM_CUDA_TRY(rint.alloc((size_t)npad * sizeof(double)));
-  LBM_CUDA_TRY(uint_.alloc((size_t)3 * npad * sizeof(double)));
-  LBM_CUDA_TRY(rref.alloc((size_t)(n + 1) * sizeof(double)));
-  LBM_CUDA_TRY(uref.alloc((size_t)(n + 1) * 3 * sizeof(double)));
+  DevBuf &rint = h->x_rint, &uint_ = h->x_uint, &rref = h->x_rref, &uref = h->x_uref;
+  if (!rint.p) LBM_CUDA_TRY(rint.alloc((size_t)npad * sizeof(double)));
+  if (!uint_.p) LBM_CUDA_TRY(uint_.alloc((size_t)3 * npad * sizeof(double)));
+  if (!rref.p) LBM_CUDA_TRY(rref.alloc((size_t)(n + 1) * sizeof(double)));
+  if (!uref.p) LBM_CUDA_TRY(uref.alloc((size_t)(n + 1) * 3 * sizeof(double)));
   double r[8];
   const double pp[3] = {h->perm_prev[0], h->perm_prev[1], h->perm_prev[2]};
   if ((st = reduce_raw(h, r, rint.as<double>(), uint_.as<double>())) != LBM_OK) return st;
@@ -704,8 +707,8 @@ lbm_status lbm_get_fields(lbm_handle* h, double* rho, double* u) {
   LBM_CUDA_TRY(cudaMemsetAsync(uref.p, 0, uref.bytes, h->stream));
   LBM_CUDA_TRY(launch_export_macro(rint.as<double>(), uint_.as<double>(), h->ref_of.as<int32_t>(), n, npad,
                                    rref.as<double>(), uref.as<double>(), h->stream));
-  if (rho) LBM_CUDA_TRY(cudaMemcpyAsync(rho, rref.p, rref.bytes, cudaMemcpyDeviceToHost, h->stream));
-  if (u) LBM_CUDA_TRY(cudaMemcpyAsync(u, uref.p, uref.bytes, cudaMemcpyDeviceToHost, h->stream));
+  if (rho) LBM_CUDA_TRY(d2h_staged(h->stage, rho, rref.p, rref.bytes, h->stream));
+  if (u) LBM_CUDA_TRY(d2h_staged(h->stage, u, uref.p, uref.bytes, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return LBM_OK;
 }
@@ -715,7 +718,7 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f) {
   if (st != LBM_OK) return st;
   if (!f) return fail(LBM_ERR_ARG, "lbm_get_populations: null output");
   const int n = h->geo.count;
-  DevBuf out;
+  DevBuf out;  // 152 B per node: not kept between calls
   LBM_CUDA_TRY(out.alloc((size_t)(n + 1) * kQ * sizeof(double)));
   LBM_CUDA_TRY(cudaMemsetAsync(out.p, 0, out.bytes, h->stream));
   int n_main;
@@ -723,8 +726,7 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f) {
   if ((st = finalize_faces(h, &n_main, &bnd_f)) != LBM_OK) return st;
   LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
                                  h->geo.npad, h->fp16_scale, out.as<double>(), h->stream, n_main, bnd_f));
-  LBM_CUDA_TRY(cudaMemcpyAsync(f, out.p, out.bytes, cudaMemcpyDeviceToHost, h->stream));
-  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  LBM_CUDA_TRY(d2h_staged(h->stage, f, out.p, out.bytes, h->stream));
   return LBM_OK;
 }
 

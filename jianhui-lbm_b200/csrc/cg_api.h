@@ -22,7 +22,7 @@ struct CgArgs {
   void* f_dst;
   void* gr;           // [19][npad] recoloured red distributions (at their source node), FP64
   void* gb;
-  void* rec;          // FP32: [npad][8] per-node colour record (rho_r, rho_b, u, unit colour gradient)
+  void* rec;          // FP32: [2][npad] float4 per-node colour record (rho_r, rho_b, ux, uy | uz, unit colour gradient)
   const int32_t* table;
   const uint8_t* corder;  // [19][npad] colour summation order (FP64), or null
   int n, npad;

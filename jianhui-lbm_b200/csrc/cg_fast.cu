@@ -46,7 +46,7 @@ cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st) {
 // gradient; moments and the back-transform use the opposite-pair split, the
 // Guo moments their closed forms; divisions by constants and repeated
 // divisions become reciprocal multiplies.
-__global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
+__global__ void __launch_bounds__(256, 4) cg_collide_fast_kernel(CgArgs a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= a.n) return;
   const float* __restrict__ fs = static_cast<const float*>(a.f_src);
@@ -216,9 +216,11 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
   // (CG3:3472-3505) are a function of these eight values, and the next
   // colour pass recomputes each one where it is pulled instead of storing
   // 2 x 19 of them
-  float4* __restrict__ rec = reinterpret_cast<float4*>(a.rec) + 2 * (size_t)x;
+  // two planes [2][npad] of float4: a warp's gathers of one plane read
+  // 16 contiguous-ish bytes per node instead of half of every 32-byte record
+  float4* __restrict__ rec = reinterpret_cast<float4*>(a.rec) + x;
   rec[0] = make_float4(rr, rb, ux, uy);
-  rec[1] = make_float4(uz, nx, ny, nz);
+  rec[npad] = make_float4(uz, nx, ny, nz);
 }
 
 // FP32 colour pass (CG3:3472-3570 restated as a pull): rho_r(x), rho_b(x) =
@@ -240,7 +242,7 @@ __global__ void __launch_bounds__(256) cg_colour_fast_kernel(CgArgs a) {
   const int npad = a.npad;
   float sr, sb;
   {
-    const float4 r0 = __ldg(rec + 2 * (size_t)x), r1 = __ldg(rec + 2 * (size_t)x + 1);
+    const float4 r0 = __ldg(rec + x), r1 = __ldg(rec + (size_t)npad + x);
     const float uu = r0.z * r0.z + r0.w * r0.w + r1.x * r1.x;
     const float e0 = (float)weight(0) * (1.f - 1.5f * uu);
     sr = r0.x * e0;
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(256) cg_colour_fast_kernel(CgArgs a) {
     const int m = streamed ? s - lo : x;
     // member of the pair actually pulled: k itself when streamed, its opposite behind a wall
     const bool first = ((k % 2) != 0) == streamed;
-    const float4 r0 = __ldg(rec + 2 * (size_t)m), r1 = __ldg(rec + 2 * (size_t)m + 1);
+    const float4 r0 = __ldg(rec + m), r1 = __ldg(rec + (size_t)npad + m);
     const float ux = r0.z, uy = r0.w, uz = r1.x;
     const float eu = (float)cg::ex(ka) * ux + (float)cg::ey(ka) * uy + (float)cg::ez(ka) * uz;
     const float base = 1.f - 1.5f * (ux * ux + uy * uy + uz * uz) + 4.5f * eu * eu;

@@ -153,6 +153,21 @@ bool bc_active(const lbm_boundary& bc);
 // within each class, and builds the per-node operation lists.
 void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPlan* plan);
 
+// Two pinned staging buffers for device -> pageable host copies (allocated
+// on first use, owned by a handle; one copy at a time).
+struct PinnedStage {
+  static constexpr size_t kChunk = size_t(8) << 20;
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  PinnedStage() = default;
+  PinnedStage(const PinnedStage&) = delete;
+  PinnedStage& operator=(const PinnedStage&) = delete;
+  ~PinnedStage();
+};
+// Copies `bytes` from device memory `src` to host memory `dst` in order on
+// `st` and returns when the host copy is complete.
+cudaError_t d2h_staged(PinnedStage& s, void* dst, const void* src, size_t bytes, cudaStream_t st);
+
 // Mask and box of a single-phase handle (for solvers coupled to it).
 const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz);
 extern "C" const uint8_t* lbm_cg_internal_mask(lbm_cg_handle* h, int* nx, int* ny, int* nz);
