@@ -46,7 +46,7 @@ cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st) {
 // gradient; moments and the back-transform use the opposite-pair split, the
 // Guo moments their closed forms; divisions by constants and repeated
 // divisions become reciprocal multiplies.
-__global__ void __launch_bounds__(256, 4) cg_collide_fast_kernel(CgArgs a) {
+__global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= a.n) return;
   const float* __restrict__ fs = static_cast<const float*>(a.f_src);
@@ -78,11 +78,12 @@ __global__ void __launch_bounds__(256, 4) cg_collide_fast_kernel(CgArgs a) {
 #pragma unroll
   for (int t = 1; t < kQ; t++) {
     const int q = opp(cg::row(t));
-    const int32_t s = tb[q];
-    const int32_t lo = q * npad;
+    // a pull from row q itself is a fluid neighbour; behind a wall the entry
+    // points into the opposite row
+    const uint32_t m = (uint32_t)(tb[q] - q * npad);
     float pn;
-    if (s >= lo && s < lo + npad) {
-      pn = psi[s - lo];
+    if (m < (uint32_t)npad) {
+      pn = psi[m];
     } else {
       pn = psi_s;
       wall = true;
@@ -135,20 +136,24 @@ __global__ void __launch_bounds__(256, 4) cg_collide_fast_kernel(CgArgs a) {
   // the phase is not driven
   const bool no_force = ((a.p.body_force_phase == 1) && (psi_x < (float)a.p.flux_psi)) ||
                         ((a.p.body_force_phase == -1) && (psi_x > -(float)a.p.flux_psi));
+  // (the undriven case scales the force by 0 so that the rows that are zero
+  // for every node stay compile-time zeros)
+  const float fg = no_force ? 0.f : 1.f;
+  const float fx = fg * gx, fy = fg * gy, fz = fg * gz;
   float MG[kQ];
 #pragma unroll
   for (int k = 0; k < kQ; k++) MG[k] = 0.f;
-  if (!no_force) {
-    const float xx = ux * gx, yy = uy * gy, zz = uz * gz;
+  {
+    const float xx = ux * fx, yy = uy * fy, zz = uz * fz;
     MG[1] = 2.f * (xx + yy + zz);
-    MG[3] = gx;
-    MG[5] = gy;
-    MG[7] = gz;
+    MG[3] = fx;
+    MG[5] = fy;
+    MG[7] = fz;
     MG[9] = 4.f * xx - 2.f * yy - 2.f * zz;
     MG[11] = 2.f * yy - 2.f * zz;
-    MG[13] = ux * gy + uy * gx;
-    MG[14] = uy * gz + uz * gy;
-    MG[15] = ux * gz + uz * gx;
+    MG[13] = ux * fy + uy * fx;
+    MG[14] = uy * fz + uz * fy;
+    MG[15] = ux * fz + uz * fx;
   }
 
   // equilibrium moments with the surface-tension perturbation (CG3:2836-2851)
