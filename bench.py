@@ -16,7 +16,10 @@ e2e    the same metric through the C ABI from host memory: lbm_create from
        the host mask (compaction, table, upload), K steps with a diagnostics
        read-back (lbm_reduce) every 100 steps, and lbm_get_fields of rho/u to
        the host, all inside the timed region.
-roofline  achieved = (2*19*4 + 18*4) B per fluid update x nodes / step time,
+roofline  achieved = (2*19*4 + table) B per fluid update x nodes / step time,
+          table = the pull-table bytes per node the step reads (lbm_table_info:
+          18*2 + 18*4/32 + the int32 fallback share x 18*4 with the compact
+          table, 18*4 with the int32 one),
           against the measured HBM copy bandwidth.
 --impl reference  times the reference solver (SP3, compiled from its own
        source with -O3 -march=native, oracle/_ref/libref_sp3_fast.so) on the
@@ -44,7 +47,7 @@ METRIC = "fluid MLUPS (sparse D3Q19 MRT, FP32 deviation storage)"
 SHAPE = (256, 256, 256)
 PHI, RADIUS, SEED = 0.35, (4.0, 10.0), 20260101
 NU, GX = 0.1, 1e-6
-BYTES_PER_LU = 2 * 19 * 4 + 18 * 4
+BYTES_PER_LU = 2 * 19 * 4 + 18 * 4  # with the int32 pull table; the solver reports its own
 
 
 def workload_mask():
@@ -225,13 +228,19 @@ def run_ours(a):
     # pick ordering / block size once (not timed), then build the timed solver with them
     if a.ordering == "auto":
         with lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering="reference", device=local) as s0:
-            tune = s0.autotune(trial_steps=10)
+            tune = s0.autotune(trial_steps=200)
+            compact = s0.table_info()["compact"]
         order, block = tune["ordering"], tune["block"]
     else:
-        order, block = lbm_b200.ORDERINGS[a.ordering], a.block
+        # steady-state winner on this workload (reference order, 256 threads,
+        # int32 table); the autotuner's short trials run at burst clocks
+        order, block, compact = lbm_b200.ORDERINGS[a.ordering], a.block, 0
 
     s = lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering=order, block_size=block, device=local)
+    s.set_table_mode(compact)
     count = s.count
+    mem, tinfo = s.memory(), s.table_info()
+    bytes_per_lu = mem["bytes_per_lu"]  # populations + the table form the step reads
     s.step(a.warmup)
     barrier(pg)
     with ClockSampler(local) as clk:
@@ -249,6 +258,7 @@ def run_ours(a):
         t_e2e, count_e2e = None, count
     t0 = time.perf_counter()
     e = lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision="f32", ordering=order, block_size=block, device=local)
+    e.set_table_mode(compact)
     left, reads = (0 if a.skip_e2e else a.steps), 0
     while left > 0:
         k = min(100, left)
@@ -268,7 +278,7 @@ def run_ours(a):
     if rank != 0:
         return 0
     peak, peak_kind = measured_peak()
-    achieved = BYTES_PER_LU * count / (ms_step * 1e-3) / 1e9
+    achieved = bytes_per_lu * count / (ms_step * 1e-3) / 1e9
     traffic = profiled_traffic()
     line = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -277,9 +287,11 @@ def run_ours(a):
         "config": {"workload": "256^3 overlapping spheres r=U[4,10], phi=0.35, seed 20260101, tau=0.8, gx=1e-6, "
                                "FP32 deviation storage",
                    "fluid_nodes": count, "ordering": order, "block": block, "parallelism": f"replicas x{world}",
-                   "l2": "inputs > L2 (no flush)"},
+                   "l2": "inputs > L2 (no flush)",
+                   "pull_table": "compact" if tinfo["compact"] else "int32",
+                   "table_wide_fraction": tinfo["wide_fraction"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "bytes_per_lu": BYTES_PER_LU},
+                     "traffic": traffic, "peak_source": peak_kind, "bytes_per_lu": bytes_per_lu},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d / a.steps,
                 "d2h_bytes_per_step": d2h / a.steps, "wall_s": t_e2e},
         "gpu_launches": a.steps,
@@ -527,7 +539,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ordering", default="auto", choices=["auto", "reference", "morton", "hilbert", "brick"])
+    ap.add_argument("--ordering", default="reference", choices=["auto", "reference", "morton", "hilbert", "brick"],
+                    help="node order of the timed solve; auto = lbm_autotune (short trials at burst clocks)")
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: no end-to-end pass")
     a = ap.parse_args()

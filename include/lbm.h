@@ -256,9 +256,10 @@ LBM_API lbm_status lbm_export_compaction(lbm_handle* h, int32_t* coor);
  * device pull table -- for the bit-exact table test. */
 LBM_API lbm_status lbm_export_table(lbm_handle* h, int32_t* nei_loc);
 
-/* Chooses ordering x block size by timing `trial_steps` steps of each
- * candidate on this geometry; the state is restored afterwards.  Writes the
- * chosen ordering / block size and their measured MLUPS. */
+/* Chooses ordering x block size x pull-table form by timing `trial_steps`
+ * steps of each candidate on this geometry; the state is restored afterwards.
+ * Writes the chosen ordering / block size and their measured MLUPS (the
+ * table form: lbm_table_info). */
 LBM_API lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* block_out,
                         double* mlups_out);
 
@@ -266,8 +267,24 @@ LBM_API lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_ou
 LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
 
 /* Memory facts: bytes of device memory the handle holds and the algorithmic
- * bytes one fluid-node update moves (2*19*s + 18*4). */
+ * bytes one fluid-node update moves (2*19*s populations + the pull-table
+ * bytes of lbm_table_info). */
 LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
+
+/* Form of the pull table the step kernel reads (the reference's nei_loc,
+ * SP3:1099-1151, as a pull table).  compact = 0 (default): the int32 table.
+ * compact = 1: per aligned group of 32 nodes and direction one int32 base
+ * and per node a 16-bit offset from it, 18*2 + 18*4/32 bytes per node
+ * instead of 18*4; groups whose sources spread wider than the offsets reach
+ * read the int32 table.  The two give identical results; the compact form
+ * moves fewer bytes but waits on more dependent loads, and lbm_autotune
+ * times both.  The other kernels (reductions, exports, faces) always read
+ * the int32 table. */
+LBM_API lbm_status lbm_set_table_mode(lbm_handle* h, int compact);
+/* current mode, table bytes per node the step reads, and the share of
+ * (group, direction) pairs that fall back to the int32 table */
+LBM_API lbm_status lbm_table_info(lbm_handle* h, int* compact, double* table_bytes_per_node,
+                                  double* wide_fraction);
 
 /* ----------------------------------------------- reference output formats */
 

@@ -1,4 +1,5 @@
 // C ABI of the single-phase solver (include/lbm.h).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -79,6 +80,12 @@ struct lbm_handle {
   // dense cell -> internal index map for box sums, built on first use
   DevBuf cell_idx;
   bool cell_idx_valid = false;
+  // compact pull table of the step kernel (built after every layout); the
+  // fraction of (warp, direction) pairs that keep reading the full table
+  DevBuf ct_base, ct_off, ct_wide;
+  bool ct_ok = false;
+  bool ct_on = false;  // the int32 table unless chosen (lbm_set_table_mode, lbm_autotune)
+  double ct_wide_frac = 1.0;
   // field export: device buffers kept between calls, pinned staging
   DevBuf x_rint, x_uint, x_rref, x_uref;
   PinnedStage stage;
@@ -129,6 +136,33 @@ const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz) {
 
 namespace {
 
+// Compact form of the pull table (read by the step kernel; the other kernels
+// keep reading the int32 table).
+lbm_status build_compact_table(lbm_handle* h) {
+  const int npad = h->geo.npad;
+  h->ct_ok = false;
+  if (!h->ct_base.p) {
+    LBM_CUDA_TRY(h->ct_base.alloc((size_t)18 * (npad / 32) * sizeof(int32_t)));
+    LBM_CUDA_TRY(h->ct_off.alloc((size_t)18 * npad * sizeof(uint16_t)));
+    LBM_CUDA_TRY(h->ct_wide.alloc(sizeof(unsigned long long)));
+  }
+  LBM_CUDA_TRY(launch_compact_table(h->table.as<int32_t>(), h->geo.count, npad, h->ct_base.as<int32_t>(),
+                                    h->ct_off.as<uint16_t>(), h->ct_wide.as<unsigned long long>(), h->stream));
+  unsigned long long wide = 0;
+  LBM_CUDA_TRY(cudaMemcpyAsync(&wide, h->ct_wide.p, sizeof(wide), cudaMemcpyDeviceToHost, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->ct_wide_frac = (double)wide / (18.0 * (npad / 32));
+  h->ct_ok = true;
+  h->drop_graphs();
+  return LBM_OK;
+}
+
+// Table bytes the step kernel reads per node.
+double table_bytes_per_node(const lbm_handle* h) {
+  if (!(h->ct_ok && h->ct_on)) return 18.0 * 4.0;
+  return 18.0 * 2.0 + 18.0 * 4.0 / 32.0 + h->ct_wide_frac * 18.0 * 4.0;
+}
+
 lbm_status upload_layout(lbm_handle* h) {
   Geometry& g = h->geo;
   const size_t npad = (size_t)g.npad;
@@ -143,7 +177,7 @@ lbm_status upload_layout(lbm_handle* h) {
   h->last_p = g.count > 0 ? g.int_of[g.count] : -1;
   h->drop_graphs();
   h->cell_idx_valid = false;
-  return LBM_OK;
+  return build_compact_table(h);
 }
 
 // Host copies of the compaction and node order, built on first need.
@@ -248,6 +282,11 @@ StepArgs step_args(lbm_handle* h, bool write) {
   a.fp16_scale = h->fp16_scale;
   const int n = h->geo.count;
   a.n_main = h->bc.active ? h->bc.n_main : n;
+  if (h->ct_ok && h->ct_on) {
+    a.ct_base = h->ct_base.as<int32_t>();
+    a.ct_off = h->ct_off.as<uint16_t>();
+    a.nwarps = h->geo.npad / 32;
+  }
   a.snap_begin = h->bc.active ? h->bc.snap_begin : n;
   a.nsnap = std::max(n - a.snap_begin, 1);
   a.snap_dst = h->bc.active ? h->snap[1 - h->cur].as<double>() : nullptr;
@@ -562,6 +601,7 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
     h->ordering = LBM_ORDER_REFERENCE;
     h->last_p = h->geo.count - 1;
     LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));  // before the scratch is freed
+    if ((st = build_compact_table(h.get())) != LBM_OK) return st;
   } else if ((st = layout(h.get(), ord)) != LBM_OK) {
     return st;
   }
@@ -786,11 +826,29 @@ lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu)
     size_t b = 0;
     for (const DevBuf* d : {&h->pop[0], &h->pop[1], &h->table, &h->ref_of, &h->window, &h->rho_given, &h->u_given,
                             &h->rho_prev, &h->u_prev, &h->partials, &h->result, &h->snap[0], &h->snap[1],
-                            &h->bc_ops, &h->bc_off, &h->bc_mi, &h->bnd_f})
+                            &h->bc_ops, &h->bc_off, &h->bc_mi, &h->bnd_f, &h->ct_base, &h->ct_off})
       b += d->bytes;
     *device_bytes = b;
   }
-  if (bytes_per_lu) *bytes_per_lu = 2.0 * kQ * (double)store_bytes(h->kind) + 18.0 * 4.0;
+  if (bytes_per_lu) *bytes_per_lu = 2.0 * kQ * (double)store_bytes(h->kind) + table_bytes_per_node(h);
+  return LBM_OK;
+}
+
+lbm_status lbm_set_table_mode(lbm_handle* h, int compact) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (compact != 0 && compact != 1) return fail(LBM_ERR_ARG, "lbm_set_table_mode: mode must be 0 or 1");
+  if (compact && !h->ct_ok) return fail(LBM_ERR_STATE, "lbm_set_table_mode: no compact table for this layout");
+  if (h->ct_on != (compact == 1)) h->drop_graphs();
+  h->ct_on = compact == 1;
+  return LBM_OK;
+}
+
+lbm_status lbm_table_info(lbm_handle* h, int* compact, double* table_bytes_per_node_out, double* wide_fraction) {
+  if (!h) return fail(LBM_ERR_ARG, "null handle");
+  if (compact) *compact = (h->ct_ok && h->ct_on) ? 1 : 0;
+  if (table_bytes_per_node_out) *table_bytes_per_node_out = table_bytes_per_node(h);
+  if (wide_fraction) *wide_fraction = h->ct_wide_frac;
   return LBM_OK;
 }
 
@@ -833,27 +891,53 @@ lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* 
   const bool uprev0 = h->uprev_valid;
   const int orders[4] = {LBM_ORDER_REFERENCE, LBM_ORDER_MORTON, LBM_ORDER_HILBERT, LBM_ORDER_BRICK};
   const int blocks[4] = {128, 256, 512, 64};
-  double best = -1.0;
-  int best_o = h->ordering, best_b = h->block;
+  // every candidate once, then the three fastest again with four times the
+  // steps (single short trials of near-equal candidates are at the mercy of
+  // clock and power-cap noise)
+  struct Cand {
+    int o, b, ct;
+    double ml;
+  };
+  std::vector<Cand> cands;
+  auto time_cand = [&](const Cand& c, int steps, double* ml) -> lbm_status {
+    h->block = c.b;
+    h->ct_on = c.ct == 1;
+    h->drop_graphs();
+    h->given_macro = false;  // timing only; the state is restored below
+    h->cur = 0;
+    lbm_status s2;
+    if ((s2 = run_steps(h, 2)) != LBM_OK) return s2;  // warm-up
+    if ((s2 = run_steps(h, steps)) != LBM_OK) return s2;
+    *ml = (double)n * steps / (h->last_ms * 1e3);
+    return LBM_OK;
+  };
   for (int oi = 0; oi < 4; oi++) {
     if ((st = layout(h, orders[oi])) != LBM_OK) return st;
-    for (int bi = 0; bi < 4; bi++) {
-      h->block = blocks[bi];
-      h->drop_graphs();
-      h->given_macro = false;  // timing only; the state is restored below
-      h->cur = 0;
-      if ((st = run_steps(h, 2)) != LBM_OK) return st;  // warm-up
-      if ((st = run_steps(h, trial_steps)) != LBM_OK) return st;
-      const double ml = (double)n * trial_steps / (h->last_ms * 1e3);
-      if (ml > best) {
-        best = ml;
-        best_o = orders[oi];
-        best_b = blocks[bi];
+    for (int bi = 0; bi < 4; bi++)
+      for (int ct = 0; ct < (h->ct_ok ? 2 : 1); ct++) {
+        Cand c{orders[oi], blocks[bi], ct, 0.0};
+        if ((st = time_cand(c, trial_steps, &c.ml)) != LBM_OK) return st;
+        cands.push_back(c);
       }
+  }
+  std::sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.ml > y.ml; });
+  if (cands.size() > 3) cands.resize(3);
+  double best = -1.0;
+  int best_o = h->ordering, best_b = h->block;
+  bool best_ct = h->ct_on;
+  for (Cand& c : cands) {
+    if ((st = layout(h, c.o)) != LBM_OK) return st;
+    if ((st = time_cand(c, 4 * trial_steps, &c.ml)) != LBM_OK) return st;
+    if (c.ml > best) {
+      best = c.ml;
+      best_o = c.o;
+      best_b = c.b;
+      best_ct = c.ct == 1;
     }
   }
   if ((st = layout(h, best_o)) != LBM_OK) return st;
   h->block = best_b;
+  h->ct_on = best_ct && h->ct_ok;
   h->drop_graphs();
   h->cur = cur0;
   LBM_CUDA_TRY(launch_import_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,

@@ -212,8 +212,20 @@ struct StepArgs {
   int snap_begin;
   int nsnap;
   double* snap_dst;
+  // compact pull table (null = read `table`): per aligned warp of 32 nodes
+  // and direction q a base node index ct_base[(q-1)*nwarps + w] (-1: the
+  // warp reads `table` for q) and per node a 16-bit offset from it (0xFFFF:
+  // halfway bounce-back, source opp(q)*npad + p); offsets of directions
+  // 2i+1, 2i+2 share one 32-bit word, ct_off as [9][npad][2]
+  const int32_t* ct_base;
+  const uint16_t* ct_off;
+  int nwarps;
 };
 cudaError_t launch_step(Store kind, const StepArgs& a, int block, cudaStream_t st);
+// Builds the compact pull table from `table` ([18][npad], n fluid nodes);
+// counts the (warp, direction) pairs left on the full table in *wide (device).
+cudaError_t launch_compact_table(const int32_t* table, int n, int npad, int32_t* ct_base, uint16_t* ct_off,
+                                 unsigned long long* wide, cudaStream_t st);
 
 constexpr int kSnapRows = kQ + 4;  // per-step record of a node: f_0..f_18, rho, ux, uy, uz
 

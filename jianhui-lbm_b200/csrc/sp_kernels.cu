@@ -18,12 +18,75 @@ cudaError_t launch_boundary_f64(const BcArgs& a, cudaStream_t st);
 cudaError_t import_f64(void*, const int32_t*, const int32_t*, int, int, const double*, cudaStream_t);
 cudaError_t import_macro_f64(void*, void*, const int32_t*, int, int, const double*, const double*, cudaStream_t);
 
-template <Store K, int BS, bool GIVEN, bool WRITE>
+// Compact pull table: per aligned warp of 32 nodes and direction q one int32
+// base node index (-1: the warp reads the int32 table for q) and per node a
+// 16-bit offset from it (0xFFFF: halfway bounce-back, source opp(q)*npad +
+// p), the offsets of directions 2i+1 and 2i+2 packed in one 32-bit word
+// ([9][npad] words): 18*2 + 18*4/32 bytes of table per node instead of 72.
+__device__ __forceinline__ size_t ct_off_index(int q, int p, int npad) {
+  return (size_t)((q - 1) >> 1) * 2 * npad + 2 * (size_t)p + ((q - 1) & 1);
+}
+
+// One thread per (node, direction) row of 32 nodes: the warp's fluid sources
+// in row q as a base plus 16-bit offsets, or -1 when they spread wider.
+__global__ void __launch_bounds__(256) compact_table_kernel(const int32_t* __restrict__ table, int n, int npad,
+                                                           int32_t* __restrict__ ct_base,
+                                                           uint16_t* __restrict__ ct_off,
+                                                           unsigned long long* __restrict__ wide) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;  // npad is a multiple of 256: whole warps
+  const int q = blockIdx.y + 1;
+  if (p >= npad) return;
+  const int32_t e = table[(size_t)(q - 1) * npad + p];
+  const bool live = p < n;
+  const unsigned m = (unsigned)(e - q * npad);
+  const bool fluid = live && m < (unsigned)npad;
+  const bool bounce = live && e == opp(q) * npad + p;
+  const unsigned lo = __reduce_min_sync(0xffffffffu, fluid ? m : 0xffffffffu);
+  const unsigned hi = __reduce_max_sync(0xffffffffu, fluid ? m : 0u);
+  const bool odd = __any_sync(0xffffffffu, live && !fluid && !bounce);
+  const bool any = lo != 0xffffffffu;
+  const bool too_wide = odd || (any && hi - lo > 0xFFFEu);
+  const size_t w = p >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    ct_base[(size_t)(q - 1) * (npad >> 5) + w] = too_wide ? -1 : (any ? (int32_t)lo : 0);
+    if (too_wide) atomicAdd(wide, 1ull);
+  }
+  ct_off[ct_off_index(q, p, npad)] = (too_wide || !fluid) ? (uint16_t)0xFFFF : (uint16_t)(m - lo);
+}
+
+cudaError_t launch_compact_table(const int32_t* table, int n, int npad, int32_t* ct_base, uint16_t* ct_off,
+                                 unsigned long long* wide, cudaStream_t st) {
+  if (npad % 256 != 0) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(wide, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  compact_table_kernel<<<dim3(npad / 256, 18), 256, 0, st>>>(table, n, npad, ct_base, ct_off, wide);
+  return cudaGetLastError();
+}
+
+template <Store K, int BS, bool GIVEN, bool WRITE, bool CT>
 __global__ void __launch_bounds__(BS) step_dev_kernel(StepArgs a) {
   using T = typename Traits<K>::T;
   using A = typename Traits<K>::A;
   using Mac = typename Traits<K>::Mac;
   const int p = blockIdx.x * BS + threadIdx.x;
+  // the block's warp bases of the compact table, read once into shared
+  // memory; the offset words are loaded before the barrier so that their
+  // latency overlaps the bases'
+  __shared__ int32_t sbase[CT ? 18 : 1][CT ? BS / 32 : 1];
+  uint32_t ow[CT ? 9 : 1];
+  if (CT) {
+    if (p < a.n_main) {
+      const uint32_t* __restrict__ off = reinterpret_cast<const uint32_t*>(a.ct_off);
+#pragma unroll
+      for (int i = 0; i < 9; i++) ow[i] = __ldg(off + (size_t)i * a.npad + p);
+    }
+    for (int k = threadIdx.x; k < 18 * (BS / 32); k += BS) {
+      const int qq = k / (BS / 32), w = k % (BS / 32);
+      const int gw = blockIdx.x * (BS / 32) + w;
+      sbase[qq][w] = gw < a.nwarps ? __ldg(a.ct_base + (size_t)qq * a.nwarps + gw) : -1;
+    }
+    __syncthreads();
+  }
   if (p >= a.n_main) return;
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
@@ -33,7 +96,21 @@ __global__ void __launch_bounds__(BS) step_dev_kernel(StepArgs a) {
   A f[kQ];
   f[0] = load_pop<K>(src + p, inv_scale);
 #pragma unroll
-  for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(src + __ldg(a.table + (size_t)(q - 1) * a.npad + p), inv_scale);
+  if (CT) {
+    const int wl = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 1; q < kQ; q++) {
+      const int32_t b = sbase[q - 1][wl];
+      const int o = ((q - 1) & 1) ? (int)(ow[(q - 1) >> 1] >> 16) : (int)(ow[(q - 1) >> 1] & 0xFFFFu);
+      int32_t t = 0;
+      if (b < 0) t = __ldg(a.table + (size_t)(q - 1) * a.npad + p);
+      const int32_t c = o == 0xFFFF ? opp(q) * a.npad + p : q * a.npad + b + o;
+      f[q] = load_pop<K>(src + (b < 0 ? t : c), inv_scale);
+    }
+  } else {
+#pragma unroll
+    for (int q = 1; q < kQ; q++) f[q] = load_pop<K>(src + __ldg(a.table + (size_t)(q - 1) * a.npad + p), inv_scale);
+  }
 
   PairSplit<A> ps;
   split_pairs(f, ps);
@@ -153,14 +230,25 @@ static cudaError_t launch_dev_bs(const StepArgs& a, cudaStream_t st) {
   const int grid = (a.n_main + BS - 1) / BS;
   if (grid == 0) return cudaSuccess;
   const bool given = a.rho_in != nullptr, write = a.rho_out != nullptr;
-  if (given && write)
-    step_dev_kernel<K, BS, true, true><<<grid, BS, 0, st>>>(a);
-  else if (given)
-    step_dev_kernel<K, BS, true, false><<<grid, BS, 0, st>>>(a);
-  else if (write)
-    step_dev_kernel<K, BS, false, true><<<grid, BS, 0, st>>>(a);
-  else
-    step_dev_kernel<K, BS, false, false><<<grid, BS, 0, st>>>(a);
+  if (a.ct_base != nullptr) {
+    if (given && write)
+      step_dev_kernel<K, BS, true, true, true><<<grid, BS, 0, st>>>(a);
+    else if (given)
+      step_dev_kernel<K, BS, true, false, true><<<grid, BS, 0, st>>>(a);
+    else if (write)
+      step_dev_kernel<K, BS, false, true, true><<<grid, BS, 0, st>>>(a);
+    else
+      step_dev_kernel<K, BS, false, false, true><<<grid, BS, 0, st>>>(a);
+  } else {
+    if (given && write)
+      step_dev_kernel<K, BS, true, true, false><<<grid, BS, 0, st>>>(a);
+    else if (given)
+      step_dev_kernel<K, BS, true, false, false><<<grid, BS, 0, st>>>(a);
+    else if (write)
+      step_dev_kernel<K, BS, false, true, false><<<grid, BS, 0, st>>>(a);
+    else
+      step_dev_kernel<K, BS, false, false, false><<<grid, BS, 0, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -252,6 +252,8 @@ _SIGNATURES = {
     "lbm_autotune": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "lbm_last_step_ms": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
     "lbm_memory": ([C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_double)], C.c_int),
+    "lbm_set_table_mode": ([C.c_void_p, C.c_int], C.c_int),
+    "lbm_table_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "lbm_reduce_noalloc": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                             C.c_void_p, C.c_void_p], C.c_int),
     "lbm_batch_create": ([C.c_int, C.POINTER(Instance), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
@@ -922,6 +924,15 @@ class SinglePhase:
         v = C.c_double()
         _check(lib().lbm_last_step_ms(self._h, C.byref(v)))
         return v.value
+
+    def set_table_mode(self, compact):
+        """1: compact pull table (default), 0: the int32 table; identical results."""
+        _check(lib().lbm_set_table_mode(self._h, int(compact)))
+
+    def table_info(self):
+        c, b, w = C.c_int(), C.c_double(), C.c_double()
+        _check(lib().lbm_table_info(self._h, C.byref(c), C.byref(b), C.byref(w)))
+        return {"compact": c.value, "table_bytes_per_node": b.value, "wide_fraction": w.value}
 
     def memory(self):
         b = C.c_size_t()

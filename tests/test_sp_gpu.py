@@ -115,6 +115,47 @@ def test_orderings_and_blocks_give_identical_fp32_results(L):
         assert np.array_equal(o, outs[0])
 
 
+@pytest.mark.parametrize("precision", ["f32", "f16", "f64fast"])
+def test_compact_pull_table_gives_the_int32_table_results(L, precision):
+    """The compact pull table (per-warp base + 16-bit offsets, int32 fallback
+    for warps whose sources spread wider) reads the same sources as the int32
+    table: populations bit-identical after 41 steps (single steps and graph
+    chains), for two orderings.  98 k fluid nodes, so the warps at the
+    periodic wraps exceed the offset range and exercise the fallback."""
+    mask = spheres((64, 64, 48), 0.5, 3.5, seed=23)
+    for order in ("reference", "morton"):
+        outs = []
+        for mode in (1, 0):
+            with L.SinglePhase(mask, 0.1, (1e-6, 2e-7, 0), precision=precision, ordering=order) as s:
+                info = s.table_info()
+                assert info["compact"] == 0 and info["table_bytes_per_node"] == 72.0
+                assert 0.0 < info["wide_fraction"] < 0.05, info
+                s.set_table_mode(1)
+                info = s.table_info()
+                assert abs(info["table_bytes_per_node"] - (36 + 2.25 + 72 * info["wide_fraction"])) < 1e-9
+                s.set_table_mode(mode)
+                assert s.table_info()["compact"] == mode
+                s.step(5)
+                s.step(36)
+                outs.append((s.populations(), s.reduce()["perm"]))
+        assert np.array_equal(outs[0][0], outs[1][0]), order
+        assert outs[0][1] == outs[1][1]
+
+
+def test_compact_pull_table_with_pressure_faces(L):
+    """With pressure faces the step kernel covers the interior nodes only; the
+    compact table there gives the int32 table's results bit for bit."""
+    mask = spheres((40, 36, 32), 0.5, 3.0, seed=29)
+    bc = L.Boundary.make(sub_bc=2, in_bc=1, pressure=(1, 1, 0, 0, 0, 0), rho=(1.0, 1.004, 1.0, 1.0, 1.0, 1.0))
+    outs = []
+    for mode in (1, 0):
+        with L.SinglePhase(mask, 0.1, (0.0, 0.0, 0.0), precision="f32", bc=bc) as s:
+            s.set_table_mode(mode)
+            s.step(40)
+            outs.append(s.populations())
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_set_state_round_trip_and_restart(L):
     mask = spheres((24, 20, 18), 0.5, 3.0, seed=4)
     with L.SinglePhase(mask, 0.1, (1e-5, 0, 0), precision="f64") as a:
