@@ -375,6 +375,12 @@ LBM_API lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a);
  * the sums to the nodes inside it (the reference does so when one of
  * par_per_x/y/z equals 1).  All -1 = whole box. */
 LBM_API lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict_nodes);
+/* Constant-phase faces (in_psi_BC = 1 with psi_xp..psi_zn = 1,
+ * CG3:3386-3620): after every macro step the fluid nodes on each enabled face
+ * of the box take back their initial phase (psi = psi0, rho_r = (psi0 + 1)/2,
+ * rho_b = 1 - rho_r).  faces in INPUT order xp, xn, yp, yn, zp, zn; 1 = on,
+ * 0 = off. */
+LBM_API lbm_status lbm_cg_set_phase_faces(lbm_cg_handle* h, const int faces[6]);
 /* Restores a state like Backup_init (CG3:5438-5690): f [(count+1)*19] in the
  * CG velocity order, psi, rho_r, rho_b [(count+1)], reference id order (row 0
  * ignored).  The next step takes psi / rho_r / rho_b as given and rho, u from f. */
@@ -440,7 +446,8 @@ LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, doub
  * force off until stab_time when the stabiliser is on, the flux thresholds
  * rel_perm_psi / rel_perm_psi2, PerDir and the permeability window.  Options
  * outside a fully periodic run with the phase read from file (pressure or
- * velocity faces, psi faces, random or mixture initialisation, a
+ * velocity faces, psi faces other than the initial phase, random or mixture
+ * initialisation, a
  * self-defined lattice velocity, a non-zero initial velocity, drainage /
  * imbibition control, capillary-pressure stepping, dynamic input) are
  * rejected with LBM_ERR_ARG naming the field. */

@@ -55,6 +55,9 @@ struct lbm_cg_handle {
   Dev f[2], gr, gb, rec, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
   Dev u_prev, axis, partials2, result2;  // Error's u0 and the saturation position sums
   Dev win;                                // permeability window flags, or none
+  Dev face_nodes, face_psi0;              // constant-phase face nodes and their initial phase
+  int nface = 0;
+  std::vector<double> psi0;               // initial phase per node (internal order), as read
   long long window_volume = 0;            // divisor of the fluxes and the saturation
   bool uprev_valid = false;
   int perdir = 1;
@@ -100,10 +103,20 @@ CgArgs cg_args(lbm_cg_handle* h, int c, int given, bool write_u = false) {
   return a;
 }
 
+// The colour pass (psi, rho_r, rho_b of the pending macro step) and the
+// constant-phase faces that comput_macro_variables applies after it.
+cudaError_t colour_pass(lbm_cg_handle* h, const CgArgs& a) {
+  cudaError_t e = h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream);
+  if (e == cudaSuccess && h->nface > 0)
+    e = cg_phase_faces(h->f64, h->face_nodes.as<int32_t>(), h->face_psi0.as<double>(), h->nface, h->psi.p,
+                       h->rho_r.p, h->rho_b.p, h->stream);
+  return e;
+}
+
 cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u = false) {
   const CgArgs a = cg_args(h, c, given, write_u);
   cudaError_t e = cudaSuccess;
-  if (!given) e = h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream);
+  if (!given) e = colour_pass(h, a);
   if (e != cudaSuccess) return e;
   return h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
 }
@@ -197,7 +210,7 @@ lbm_status cg_check(lbm_cg_handle* h) {
 lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double* u_out, double* r2 = nullptr) {
   if (!h->given) {
     const CgArgs a = cg_args(h, h->cur, 0);
-    LBM_CUDA_TRY(h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream));
+    LBM_CUDA_TRY(colour_pass(h, a));
   }
   CgReduceArgs ra{};
   ra.f = h->f[h->cur].p;
@@ -338,6 +351,7 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
     rr[x] = (v * rho + rho) / 2;
     rb[x] = rho - rr[x];
   }
+  h->psi0.assign(ps.begin(), ps.begin() + n);
   if (h->f64) {
     LBM_CUDA_TRY(cudaMemcpyAsync(h->psi.p, ps.data(), sizeof(double) * npad, cudaMemcpyHostToDevice, h->stream));
     LBM_CUDA_TRY(cudaMemcpyAsync(h->rho_r.p, rr.data(), sizeof(double) * npad, cudaMemcpyHostToDevice, h->stream));
@@ -549,6 +563,41 @@ lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict
   return LBM_OK;
 }
 
+lbm_status lbm_cg_set_phase_faces(lbm_cg_handle* h, const int faces[6]) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!faces) return fail(LBM_ERR_ARG, "lbm_cg_set_phase_faces: null faces");
+  for (int f = 0; f < 6; f++)
+    if (faces[f] != 0 && faces[f] != 1)
+      return fail(LBM_ERR_ARG, "lbm_cg_set_phase_faces: a face is 0 (off) or 1 (initial phase)");
+  const Geometry& g = h->geo;
+  std::vector<int32_t> nodes;
+  std::vector<double> vals;
+  for (int x = 0; x < g.count; x++) {
+    const int c = g.coor[g.ref_of[x]];  // i*ny*nz + j*nz + k
+    const int i = c / (g.ny * g.nz), j = (c % (g.ny * g.nz)) / g.nz, k = c % g.nz;
+    // faces in INPUT order xp, xn, yp, yn, zp, zn (CG3:2027-2101 lists)
+    const bool on = (faces[0] && i == g.nx - 1) || (faces[1] && i == 0) || (faces[2] && j == g.ny - 1) ||
+                    (faces[3] && j == 0) || (faces[4] && k == g.nz - 1) || (faces[5] && k == 0);
+    if (on) {
+      nodes.push_back(x);
+      vals.push_back(h->psi0[x]);
+    }
+  }
+  h->nface = (int)nodes.size();
+  if (h->nface > 0) {
+    LBM_CUDA_TRY(h->face_nodes.alloc(nodes.size() * sizeof(int32_t)));
+    LBM_CUDA_TRY(h->face_psi0.alloc(vals.size() * sizeof(double)));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->face_nodes.p, nodes.data(), nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                 h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->face_psi0.p, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
+    LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  drop_graphs(h);  // the chains captured so far do not reset the faces
+  return LBM_OK;
+}
+
 lbm_status lbm_cg_set_state(lbm_cg_handle* h, const double* f, const double* psi, const double* rho_r,
                             const double* rho_b) {
   lbm_status st = cg_check(h);
@@ -597,8 +646,11 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
   if (parsed_out) *parsed_out = in;
   // a fully periodic run with the phase read from file (CG3:2355-2380)
   if (in.in_bc != 0) return fail(LBM_ERR_ARG, "in_BC: pressure / velocity faces are not supported by lbm_cg");
-  if (in.in_psi_bc != 0 && (in.psi_xp || in.psi_xn || in.psi_yp || in.psi_yn || in.psi_zp || in.psi_zn))
-    return fail(LBM_ERR_ARG, "psi_xp..psi_zn: constant-phase faces are not supported by lbm_cg");
+  const int pf[6] = {in.psi_xp, in.psi_xn, in.psi_yp, in.psi_yn, in.psi_zp, in.psi_zn};
+  for (int f = 0; f < 6; f++)
+    if (in.in_psi_bc == 1 && pf[f] != 0 && pf[f] != 1)
+      return fail(LBM_ERR_ARG, "psi_xp..psi_zn: only constant-phase faces of the initial phase (1) are "
+                               "supported; 2 (copy the +x neighbour) and 3 (random) are not");
   if (in.ini_sat >= 0)
     return fail(LBM_ERR_ARG, "ini_Sat: random initial phase (seeded from the clock) is not supported; use -1");
   if (in.mix_psi_thickness > 0) return fail(LBM_ERR_ARG, "mix_psi_thickness: mixture injection is not supported");
@@ -644,6 +696,12 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
                       in.par_per_z ? in.per_zn : 0, in.par_per_z ? in.per_zp : in.nz - 1};
     const int restrict_nodes = (in.par_per_x - 1) * (in.par_per_y - 1) * (in.par_per_z - 1) == 0;
     if ((st = lbm_cg_set_window(h, w, restrict_nodes)) != LBM_OK) {
+      lbm_cg_destroy(h);
+      return st;
+    }
+  }
+  if (in.in_psi_bc == 1 && (pf[0] || pf[1] || pf[2] || pf[3] || pf[4] || pf[5])) {
+    if ((st = lbm_cg_set_phase_faces(h, pf)) != LBM_OK) {
       lbm_cg_destroy(h);
       return st;
     }

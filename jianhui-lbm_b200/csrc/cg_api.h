@@ -66,6 +66,10 @@ bool build_cg_inverse(double MI[kQ][kQ]);
 // f in the CG direction order, reference layout [(count+1)*19]
 cudaError_t cg_export_f(bool f64, const void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,
                         double* out, cudaStream_t st);
+// Constant-phase faces: nodes[i] (internal index) takes psi0[i] after the
+// colour pass, rho_r = (psi0 + 1)/2, rho_b = 1 - rho_r.
+cudaError_t cg_phase_faces(bool f64, const int32_t* nodes, const double* psi0, int nface, void* psi, void* rho_r,
+                           void* rho_b, cudaStream_t st);
 cudaError_t cg_import_f(bool f64, void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,
                         const double* in, cudaStream_t st);
 

@@ -156,7 +156,7 @@ void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPl
 // Two pinned staging buffers for device -> pageable host copies (allocated
 // on first use, owned by a handle; one copy at a time).
 struct PinnedStage {
-  static constexpr size_t kChunk = size_t(8) << 20;
+  static constexpr size_t kChunk = size_t(16) << 20;
   void* buf[2] = {nullptr, nullptr};
   cudaEvent_t ev[2] = {nullptr, nullptr};
   PinnedStage() = default;

@@ -1,5 +1,7 @@
 // Device -> pageable host copies through pinned staging memory.
+#include <algorithm>
 #include <cstring>
+#include <thread>
 
 #include "lbm_internal.h"
 
@@ -11,6 +13,29 @@ PinnedStage::~PinnedStage() {
     if (ev[i]) cudaEventDestroy(ev[i]);
   }
 }
+
+namespace {
+
+// Host copy out of the staging buffer split over a few threads: one thread
+// writes fresh pageable memory at well under the DMA's rate.
+void copy_parallel(char* dst, const char* src, size_t bytes) {
+  constexpr int kThreads = 4;
+  constexpr size_t kMinSplit = size_t(1) << 20;
+  if (bytes < kThreads * kMinSplit) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t part = (bytes / kThreads + 63) & ~size_t(63);
+  std::thread workers[kThreads - 1];
+  for (int t = 1; t < kThreads; t++) {
+    const size_t off = std::min(bytes, t * part), len = std::min(bytes, (t + 1) * part) - off;
+    workers[t - 1] = std::thread([=] { std::memcpy(dst + off, src + off, len); });
+  }
+  std::memcpy(dst, src, std::min(bytes, part));
+  for (auto& w : workers) w.join();
+}
+
+}  // namespace
 
 // Chunks of kChunk bytes alternate between two pinned buffers: the DMA of
 // chunk i runs while the host copies chunk i-1 out of the other buffer, so
@@ -41,7 +66,7 @@ cudaError_t d2h_staged(PinnedStage& s, void* dst, const void* src, size_t bytes,
       const size_t j = i - 1;
       cudaError_t e = cudaEventSynchronize(s.ev[j & 1]);
       if (e != cudaSuccess) return e;
-      std::memcpy(d8 + j * PinnedStage::kChunk, s.buf[j & 1], len(j));
+      copy_parallel(d8 + j * PinnedStage::kChunk, static_cast<const char*>(s.buf[j & 1]), len(j));
     }
   }
   return cudaSuccess;

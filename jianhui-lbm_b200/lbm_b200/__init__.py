@@ -284,6 +284,7 @@ _SIGNATURES = {
     "lbm_cg_set_cap_a": ([C.c_void_p, C.c_double], C.c_int),
     "lbm_cg_set_window": ([C.c_void_p, _I32P, C.c_int], C.c_int),
     "lbm_cg_set_state": ([C.c_void_p, _F64P, _F64P, _F64P, _F64P], C.c_int),
+    "lbm_cg_set_phase_faces": ([C.c_void_p, _I32P], C.c_int),
     "lbm_read_cg_input": ([C.c_char_p, C.POINTER(CGInput)], C.c_int),
     "lbm_read_phase": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
     "lbm_cg_create_from_input": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(CGInput)], C.c_int),
@@ -486,6 +487,10 @@ class ColourGradient:
         """window = (xn, xp, yn, yp, zn, zp) inclusive, or None for the whole box."""
         w = np.full(6, -1, dtype=np.int32) if window is None else np.ascontiguousarray(window, dtype=np.int32)
         _check(lib().lbm_cg_set_window(self._h, w, int(bool(restrict_nodes))))
+
+    def set_phase_faces(self, faces):
+        """Constant initial phase on the box faces (xp, xn, yp, yn, zp, zn; 1 = on)."""
+        _check(lib().lbm_cg_set_phase_faces(self._h, np.ascontiguousarray(faces, dtype=np.int32)))
 
     def set_state(self, f, psi, rho_r, rho_b):
         """Restores f [(count+1), 19] (CG velocity order) and psi / rho_r /

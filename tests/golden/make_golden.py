@@ -246,6 +246,10 @@ CG_RUNS = {
                                  L40="1 0 0", L41="10 3", L56=0, L62="1 4", L65="100 2.0e-3"),
     # body-force ramp along y through three points (the first segment starts
     # from gx, as the reference writes it), z the permeability direction
+    # constant-phase faces of the initial phase on both x faces and the y+
+    # face (in_psi_BC = 1, the reference's sample input turns the x faces on),
+    # checkpoint at the end only
+    "cg_outputs_psi.npz": dict(L7=1, L15="1 1", L16="1 0", L29=-1, L30=-1, L45=0),
     "cg_outputs_ramp.npz": dict(L8="1.0e-5 2.0e-6 -1.0e-6", L26=3, L27=25, L28=0, L29=-1, L30=-1, L31=-1,
                                 L50="2 2", L51="40 1.0 1.0 8.0e-6", L52="90 1.0 1.0 3.0e-6",
                                 L53="120 1.0 1.0 5.0e-6"),

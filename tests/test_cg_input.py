@@ -75,7 +75,8 @@ def test_phase_file_reads_as_float(L, tmp_path):
 
 @pytest.mark.parametrize("lines,field", [
     (dict(L6=1), "in_BC"),
-    (dict(L7=1, L15="1 1"), "psi_xp"),
+    (dict(L7=1, L15="2 0"), "psi_xp"),
+    (dict(L7=1, L17="0 3"), "psi_xp"),
     (dict(L37=0.5), "ini_Sat"),
     (dict(L68=3), "mix_psi_thickness"),
     (dict(L33="1 1.0 2.0"), "lattice_v"),
