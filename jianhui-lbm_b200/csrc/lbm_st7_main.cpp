@@ -14,7 +14,10 @@
 // Out_Mode 1 layout (z, y, x dimensions, one value per line, ST7:2235-2553,
 // 3150-3296) or the Out_Mode 0 layout (x fastest, ST7:2695-3150), and
 // LBM_checkpoint_{psi,fg}_<n>.<rank>.bin_input at fre_backup (Backup,
-// ST7:3681-3714); USE BACKUP DATA restarts from those files in the working
+// ST7:3681-3714), the dispersion statistics of Sub_Dis 1-3 (plane sums of the
+// concentration along x, y or z in Statistical_data_concentration_<X|Y|Z>_<n>.sta
+// and the dispersion coefficient in bodyforce.txt, Statistical_psi
+// ST7:3442-3638); USE BACKUP DATA restarts from those files in the working
 // directory (Backup_init, ST7:3716-3802).
 #include <chrono>
 #include <cmath>
@@ -104,7 +107,7 @@ int main(int argc, char** argv) {
   if (lbm_read_st7_input(argv[1], &in) != LBM_OK) return die("lbm_read_st7_input");
   // what the reference's loop does not run or this driver does not support
   if (in.lattice_v != 0) return die_msg("lattice_v: self-defined lattice velocity is not supported");
-  if (in.sub_dis > 0 && in.fre_dis >= 0) return die_msg("Sub_Dis: dispersion statistics are not supported");
+  if (in.sub_dis > 0 && in.fre_dis == 0) return die_msg("freDis = 0: the reference takes n % 0; use -1 or a positive interval");
   if (in.fre_re <= 0) return die_msg("freRe must be positive");
   if (in.fre_ve == 0 || in.fre_psi == 0 || in.fre_backup == 0)
     return die_msg("freVe / frePsi / fre_backup = 0: the reference takes n % 0; use -1 or a positive interval");
@@ -231,6 +234,70 @@ int main(int argc, char** argv) {
     u_ave_e = u_compt;
   }
   const double c_s2 = 1.0 * 1.0 / 3, dt = 1.0, dx = 1.0;
+  // psi_total (ST7:1083-1105): every rank sums the initial concentration of
+  // its pore cells (i, j, k order, the float values), rank 0 adds the ranks
+  double psi_total = 0;
+  {
+    for (int r = 0; r < nranks; r++) {
+      double part = 0;
+      for (int i = sl.first_x[r]; i < sl.first_x[r + 1]; i++)
+        for (int j = 0; j < ny; j++)
+          for (int k = 0; k < nz; k++) {
+            const size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+            if (mask[c] == 0) part += c0[c];
+          }
+      psi_total += part;
+    }
+  }
+  // the statistics window: an axis without a partial window spans the box (ST7:853-858)
+  const int win[6] = {in.par_per_x ? in.per_xn : 0, in.par_per_x ? in.per_xp : nx - 1,
+                      in.par_per_y ? in.per_yn : 0, in.par_per_y ? in.per_yp : ny - 1,
+                      in.par_per_z ? in.per_zn : 0, in.par_per_z ? in.per_zp : nz - 1};
+  double dispersion = 0, disp_pre = 0;
+  // Statistical_psi: plane sums of C along the axis, in the reference's
+  // summation order (a plane along x lies in one rank; along y or z every
+  // rank sums its slab and rank 0 adds the ranks)
+  auto statistics = [&](long long m, const std::vector<double>& conc) -> bool {
+    const int ax = in.sub_dis - 1;
+    if (ax < 0 || ax > 2) return true;
+    const int len = ax == 0 ? nx : (ax == 1 ? ny : nz);
+    std::vector<double> s_psi(len, 0.0);
+    if (ax == 0) {
+      for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+          for (int k = 0; k < nz; k++) {
+            const size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+            if (mask[c] == 0) s_psi[i] += conc[ref_id[c]];
+          }
+    } else {
+      std::vector<double> part(len);
+      for (int r = 0; r < nranks; r++) {
+        std::fill(part.begin(), part.end(), 0.0);
+        for (int a2 = 0; a2 < len; a2++)
+          for (int i = sl.first_x[r]; i < sl.first_x[r + 1]; i++)
+            for (int b = 0; b < (ax == 1 ? nz : ny); b++) {
+              const int j = ax == 1 ? a2 : b, k = ax == 1 ? b : a2;
+              const size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+              if (mask[c] == 0) part[a2] += conc[ref_id[c]];
+            }
+        for (int a2 = 0; a2 < len; a2++) s_psi[a2] += part[a2];
+      }
+    }
+    std::ostringstream name;
+    name << out << "Statistical_data_concentration_" << "XYZ"[ax] << "_" << m << ".sta";
+    std::ofstream o(name.str());
+    if (!o) return false;
+    double EX = 0, EX2 = 0;
+    for (int i = win[2 * ax]; i <= win[2 * ax + 1]; i++) {
+      o << s_psi[i] << std::endl;
+      EX += i * dx * s_psi[i] / psi_total;
+      EX2 += (i * dx * i * dx) * s_psi[i] / psi_total;
+    }
+    const double DX = EX2 - EX * EX;
+    dispersion = (DX - disp_pre) * 0.5 / (in.fre_dis * dt);
+    disp_pre = DX;
+    return true;
+  };
   const double s_v = 1 / (in.nu / (c_s2 * dt) + 0.5);
   double u_max = 0, u_ave = 0, Re = 0;
   int the = 0, tme = 0, tse = 0, th = 0, tm = 0, ts = 0;
@@ -300,7 +367,9 @@ int main(int argc, char** argv) {
         }
       });
     }
-    const bool want_c = (in.fre_psi >= 0 && n % in.fre_psi == 0) || (in.fre_backup >= 0 && n % in.fre_backup == 0 && n > 0);
+    const bool stats = in.fre_dis >= 0 && n % in.fre_dis == 0 && in.sub_dis > 0;
+    const bool want_c = (in.fre_psi >= 0 && n % in.fre_psi == 0) ||
+                        (in.fre_backup >= 0 && n % in.fre_backup == 0 && n > 0) || stats;
     if (want_c && lbm_st7_get_concentration(h, conc.data()) != LBM_OK) return die("lbm_st7_get_concentration");
     if (in.fre_psi >= 0 && n % in.fre_psi == 0) {
       std::ofstream o(out + "LBM_psi_" + tag.str() + ".vtk");
@@ -308,6 +377,13 @@ int main(int argc, char** argv) {
       o << "SCALARS sample_scalars float" << std::endl;
       o << "LOOKUP_TABLE default" << std::endl;
       for_cells([&](size_t c) { o << (mask[c] == 0 ? conc[ref_id[c]] : in.ref_psi) << std::endl; });
+    }
+    if (stats) {
+      if (!statistics(n, conc)) return die_msg("cannot write the statistics of step " + tag.str());
+      if (n > in.ini_psi) {
+        // appended without emptying the file first, as the reference does (ST7:510-517, 682-686)
+        std::ofstream(out + "bodyforce.txt", std::ios::app) << dispersion << "  " << disp_pre << std::endl;
+      }
     }
     if (in.fre_backup >= 0 && n % in.fre_backup == 0 && n > 0) {
       std::vector<double> g((size_t)(count + 1) * 7);

@@ -417,7 +417,9 @@ def st7_program_outputs():
     program runs 61 steps with reports every 20, velocity VTK every 40,
     concentration VTK every 20, checkpoints every 40, solids written as 0.5,
     in both output layouts (Out_Mode 1: st7_outputs.npz, Out_Mode 0:
-    st7_outputs_b.npz); and a restart from the step-40 checkpoint (copied to
+    st7_outputs_b.npz), with the dispersion statistics along x
+    (st7_outputs_dis.npz) and along z with a y window (st7_outputs_dis3.npz);
+    and a restart from the step-40 checkpoint (copied to
     the unprefixed names Backup_init reads) runs 31 more steps
     (st7_outputs_restart.npz)."""
     import shutil
@@ -439,10 +441,16 @@ def st7_program_outputs():
         vel = {f"Velocity_for_solute_100.{r}.bin": open(os.path.join(d, f"Velocity_for_solute_100.{r}.bin"), "rb").read()
                for r in range(ST7_NRANKS)}
         open(os.path.join(d, "phase.dat"), "w").write(phase)
-        runs = {"st7_outputs.npz": ("./st_", dict(L29=1)), "st7_outputs_b.npz": ("./sb_", dict(L29=0))}
+        # dispersion statistics along x every 20 steps (written after step 10)
+        # and along z every 40, both layouts of the run above
+        runs = {"st7_outputs.npz": ("./st_", dict(L29=1)), "st7_outputs_b.npz": ("./sb_", dict(L29=0)),
+                "st7_outputs_dis.npz": ("./sd_", dict(L29=1, L33="1 20", L39=10)),
+                "st7_outputs_dis3.npz": ("./sz_", dict(L29=0, L33="3 40", L39=-1, L40="0 1 0", L42="8 2"))}
         for fname, (prefix, kv) in runs.items():
-            text = solute_input(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=60, L7="0.0 0.5", L23=ST7_D,
-                                L28=20, L30=40, L32=20, L33="0 1000", L36=prefix, L45=40, L47=100, **kv)
+            base = dict(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=60, L7="0.0 0.5", L23=ST7_D,
+                        L28=20, L30=40, L32=20, L33="0 1000", L36=prefix, L45=40, L47=100)
+            base.update(kv)
+            text = solute_input(**base)
             open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
             assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
             save_st7(fname, mask, phase, text, vel, collect_cg(d, prefix[2:]))
