@@ -449,7 +449,7 @@ LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, doub
  * velocity faces, psi faces other than the initial phase, random or mixture
  * initialisation, a
  * self-defined lattice velocity, a non-zero initial velocity, drainage /
- * imbibition control, capillary-pressure stepping, dynamic input) are
+ * imbibition control, dynamic input) are
  * rejected with LBM_ERR_ARG naming the field. */
 LBM_API lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
                                             lbm_cg_input* parsed_out);

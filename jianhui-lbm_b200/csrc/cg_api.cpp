@@ -658,7 +658,10 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
   if (in.inivx != 0 || in.inivy != 0 || in.inivz != 0)
     return fail(LBM_ERR_ARG, "initial velocity: only a fluid at rest is supported");
   if (in.rel_perm_id_dir != 0) return fail(LBM_ERR_ARG, "rel_perm_id_dir: imbibition / drainage control is not supported");
-  if (in.pressure_change2 != 0) return fail(LBM_ERR_ARG, "pressure_change2: capillary-pressure stepping is not supported");
+  if (in.pressure_change2 < 0 || in.pressure_change2 > 3)
+    return fail(LBM_ERR_ARG, "pressure_change2: the capillary-pressure axis is 0 (off) or 1..3");
+  if (in.pressure_change2 > 0 && (in.chan_no <= 0 || in.interval_pre <= 0))
+    return fail(LBM_ERR_ARG, "pressure_change2: chan_no and interval_pre must be positive");
   if (in.input_dynamic != 0) return fail(LBM_ERR_ARG, "input_dynamic: dynamic input update is not supported");
   if (in.fre_re <= 0) return fail(LBM_ERR_ARG, "freRe must be positive");
   if (in.fre_psi == 0) return fail(LBM_ERR_ARG, "frePsi = 0: the reference takes n % 0; use -1 or a positive interval");

@@ -14,7 +14,8 @@
 // stabiliser's force switch at stab_time (CG3:851-852), the force or pressure
 // ramps of pressure_change (pressure_bodyforce_change, CG3:1252-1420), the
 // surface-tension change of rel_perm_ift (CG3:892-893) and the least-squares
-// fit of the relative permeabilities (Least_Square_Rel_Perm, CG3:1201-1250).
+// fit of the relative permeabilities (Least_Square_Rel_Perm, CG3:1201-1250)
+// and the capillary-pressure stepping (pressure_capillary, CG3:1427-1600).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -60,10 +61,10 @@ struct Drive {
 // pressure_change names.  Kept as written: the first segment of the y and z
 // ramps starts from gx, and the fifth segment is taken for every step in
 // (pre_chan_3, pre_chan_5].  Returns true when the force changed.
-bool ramp(const lbm_cg_input& in, long long n, const double p_n0[3], const double p_p0[3], Drive* d) {
+bool ramp(const lbm_cg_input& in, long long n, const double g_in[3], const double p_n0[3], const double p_p0[3],
+          Drive* d) {
   const int a = in.pressure_change - 1;
   if (a < 0 || a > 2) return false;
-  const double g_in[3] = {in.gx, in.gy, in.gz};
   const int* c = in.pre_chan;
   const double *pn = in.pre_chan_pn, *pp = in.pre_chan_pp, *f = in.pre_chan_f;
   const bool pressure = in.pre_chan_pb == 1;
@@ -77,7 +78,7 @@ bool ramp(const lbm_cg_input& in, long long n, const double p_n0[3], const doubl
       d->g[a] = f0 + (f[k] - (k == 0 ? g_in[a] : f0)) * s;
     }
   };
-  if (n <= c[0]) seg(p_n0[a], p_p0[a], in.gx, 0, (double)c[0], c[0]);
+  if (n <= c[0]) seg(p_n0[a], p_p0[a], g_in[0], 0, (double)c[0], c[0]);
   if (n <= c[1] && n > c[0]) seg(pn[0], pp[0], f[0], 1, (double)(c[1] - c[0]), c[1]);
   if (n <= c[2] && n > c[1]) seg(pn[1], pp[1], f[1], 2, (double)(c[2] - c[1]), c[2]);
   if (n <= c[3] && n > c[2]) seg(pn[2], pp[2], f[2], 3, (double)(c[3] - c[2]), c[3]);
@@ -91,6 +92,73 @@ bool ramp_at(const lbm_cg_input& in, long long n) {
   const int* c = in.pre_chan;
   return n <= c[0] || (n <= c[1] && n > c[0]) || (n <= c[2] && n > c[1]) || (n <= c[3] && n > c[2]) ||
          (n <= c[4] && n > c[2]);
+}
+
+// pressure_capillary (CG3:1427-1600): capillary-pressure stepping.  From
+// step start to start + interval_pre the force (or the face pressures) along
+// the axis of pressure_change2 ramps by 1/chan_no of the way to its target;
+// then, once the saturation changed by less than sat_cri_d between reports
+// for sat_cri reports after the first such one, the reached value becomes
+// the new base, the point (S_l, 1 - S_l, force x length or |dp|/3) goes to
+// Capillary_Pressure.txt and the next ramp starts, chan_no times.
+struct Capillary {
+  bool on = false;
+  int a = 0;
+  bool pressure = false;
+  double pre_in = 0, pre_ip = 0;
+  int error_sat = 0, ind = 0, num = 0;
+  long long start = 0;
+  bool ramping(const lbm_cg_input& in, long long n) const {
+    return on && num < in.chan_no && n <= start + in.interval_pre;
+  }
+};
+
+// One step's update; returns true when the force changed.
+bool capillary_step(const lbm_cg_input& in, Capillary& cp, long long n, double S_l, double S_l_r, double gbase[3],
+                    double p_n0[3], double p_p0[3], Drive* d, const std::string& f_cap, const int len[3]) {
+  if (!cp.on) return false;
+  const int a = cp.a;
+  const double err = std::abs((S_l_r - S_l) / S_l);
+  const long long lim = cp.start + in.interval_pre;
+  if (err < in.sat_cri_d && n % in.fre_re == 0 && n > lim && cp.num < in.chan_no) {
+    if (cp.ind == 1) {
+      cp.error_sat += 1;
+    } else {
+      cp.error_sat = 0;
+      cp.ind = 1;
+    }
+  } else if (err >= in.sat_cri_d && n % in.fre_re == 0 && n > lim && cp.num < in.chan_no) {
+    cp.ind = 0;
+    cp.error_sat = 0;
+  }
+  bool changed = false;
+  if (n <= lim && cp.num < in.chan_no) {
+    const double s = 1 - (double)(lim - n) / in.interval_pre;
+    if (cp.pressure) {
+      d->p_n[a] = p_n0[a] + cp.pre_in * s;
+      d->p_p[a] = p_p0[a] + cp.pre_ip * s;
+    } else {
+      const double before = d->g[a];
+      d->g[a] = gbase[a] + cp.pre_in * s;
+      changed = !(d->g[a] == before);
+    }
+  }
+  if (cp.error_sat >= in.sat_cri) {
+    cp.error_sat = 0;
+    cp.ind = 0;
+    cp.start = n;
+    cp.num++;
+    std::ofstream fc(f_cap, std::ios::app);
+    if (cp.pressure) {
+      p_n0[a] = d->p_n[a];
+      p_p0[a] = d->p_p[a];
+      fc << S_l << " " << 1 - S_l << " " << std::abs(d->p_p[a] - d->p_n[a]) / 3 << std::endl;
+    } else {
+      gbase[a] = d->g[a];
+      fc << S_l << " " << 1 - S_l << " " << d->g[a] * len[a] << std::endl;
+    }
+  }
+  return changed;
 }
 
 // Least_Square_Rel_Perm (CG3:1201-1250): a line through the last
@@ -197,7 +265,23 @@ int main(int argc, char** argv) {
   drv.g[0] = stab ? 0.0 : in.gx;
   drv.g[1] = stab ? 0.0 : in.gy;
   drv.g[2] = stab ? 0.0 : in.gz;
-  const double p_n0[3] = {in.p_xn, in.p_yn, in.p_zn}, p_p0[3] = {in.p_xp, in.p_yp, in.p_zp};
+  double p_n0[3] = {in.p_xn, in.p_yn, in.p_zn}, p_p0[3] = {in.p_xp, in.p_yp, in.p_zp};
+  double gbase[3] = {in.gx, in.gy, in.gz};  // gx, gy, gz: moved by the capillary stepping
+  const int len[3] = {nx, ny, nz};
+  Capillary cap;
+  if (in.pressure_change2 >= 1 && in.pressure_change2 <= 3) {
+    // CG3:560-576
+    cap.on = true;
+    cap.a = in.pressure_change2 - 1;
+    cap.pressure = in.pre_chan_pb2 == 1;
+    if (cap.pressure) {
+      cap.pre_in = (in.pre_chan_pns - p_n0[cap.a]) / (double)in.chan_no;
+      cap.pre_ip = (in.pre_chan_pps - p_p0[cap.a]) / (double)in.chan_no;
+    } else {
+      cap.pre_in = (in.pre_chan_fs - gbase[cap.a]) / (double)in.chan_no;
+    }
+  }
+  const std::string f_cap = out + "Capillary_Pressure.txt";
   for (int a = 0; a < 3; a++) {
     drv.p_n[a] = p_n0[a];
     drv.p_p[a] = p_p0[a];
@@ -244,28 +328,30 @@ int main(int argc, char** argv) {
   while (n <= in.n_max) {
     if (stab && n == in.stab_time) {
       // CG3:851-852, before this step's collision
-      drv.g[0] = in.gx;
-      drv.g[1] = in.gy;
-      drv.g[2] = in.gz;
-      if (lbm_cg_set_body_force(h, in.gx, in.gy, in.gz, LBM_CG_FORCE_BEFORE_COLLISION) != LBM_OK)
+      for (int k = 0; k < 3; k++) drv.g[k] = gbase[k];
+      if (lbm_cg_set_body_force(h, drv.g[0], drv.g[1], drv.g[2], LBM_CG_FORCE_BEFORE_COLLISION) != LBM_OK)
         return die("lbm_cg_set_body_force");
     }
     // last step of this chunk: the next report, the step before the
     // stabiliser switch, or a ramp step (ramps run one step at a time)
     long long last = n;
-    if (!ramp_at(in, n)) {
+    if (!ramp_at(in, n) && !cap.ramping(in, n)) {
       last = ((n + in.fre_re - 1) / in.fre_re) * in.fre_re;
       if (last > in.n_max) last = in.n_max;
       if (stab && in.stab_time > n && in.stab_time - 1 < last) last = in.stab_time - 1;
       for (long long k = n + 1; k <= last; k++)
-        if (ramp_at(in, k)) {
+        if (ramp_at(in, k) || cap.ramping(in, k)) {
           last = k - 1;
           break;
         }
     }
     if (lbm_cg_step(h, (int)(last - n + 1)) != LBM_OK) return die("lbm_cg_step");
     n = last;
-    if (ramp(in, n, p_n0, p_p0, &drv) &&
+    // pressure_bodyforce_change then pressure_capillary, between this step's
+    // collision and its macro step (CG3:854-858)
+    const bool moved = ramp(in, n, gbase, p_n0, p_p0, &drv);
+    const bool moved2 = capillary_step(in, cap, n, S_l, S_l_r, gbase, p_n0, p_p0, &drv, f_cap, len);
+    if ((moved || moved2) &&
         lbm_cg_set_body_force(h, drv.g[0], drv.g[1], drv.g[2], LBM_CG_FORCE_BEFORE_MACRO) != LBM_OK)
       return die("lbm_cg_set_body_force");
     if (n % in.fre_re != 0) {

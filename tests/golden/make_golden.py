@@ -250,6 +250,11 @@ CG_RUNS = {
     # face (in_psi_BC = 1, the reference's sample input turns the x faces on),
     # checkpoint at the end only
     "cg_outputs_psi.npz": dict(L7=1, L15="1 1", L16="1 0", L29=-1, L30=-1, L45=0),
+    # capillary-pressure stepping along x with the body force: three steps
+    # of 30 steps each towards 3e-5, the next one after two reports in a row
+    # with the saturation changing by less than 1e-2; reports every 10 steps
+    "cg_outputs_cap.npz": dict(L4=250, L27=10, L28=0, L29=-1, L30=-1, L31=-1, L58="1 2 30",
+                               L59="1.0 0.993 3e-5 3 2", L60="1e-2"),
     "cg_outputs_ramp.npz": dict(L8="1.0e-5 2.0e-6 -1.0e-6", L26=3, L27=25, L28=0, L29=-1, L30=-1, L31=-1,
                                 L50="2 2", L51="40 1.0 1.0 8.0e-6", L52="90 1.0 1.0 3.0e-6",
                                 L53="120 1.0 1.0 5.0e-6"),

@@ -82,7 +82,8 @@ def test_phase_file_reads_as_float(L, tmp_path):
     (dict(L33="1 1.0 2.0"), "lattice_v"),
     (dict(L22="1e-3 0 0"), "initial velocity"),
     (dict(L64="1 5"), "rel_perm_id_dir"),
-    (dict(L58="1 1 2000"), "pressure_change2"),
+    (dict(L58="4 1 2000"), "pressure_change2"),
+    (dict(L58="1 2 0"), "pressure_change2"),
     (dict(L66="1 1000"), "input_dynamic"),
     (dict(L31=0), "frePsi"),
 ])

@@ -10,6 +10,7 @@ variants of INPUT_cg.dat on 14x12x10 spheres with a blob phase field:
   cg_outputs_ramp.npz    a three-point body-force ramp along y, PerDir 3;
   cg_outputs_psi.npz     constant-phase faces (the initial phase) on x- and
                          x+ and y+;
+  cg_outputs_cap.npz     capillary-pressure stepping of the body force along x;
   cg_outputs_restart.npz the first run's step-100 checkpoint read back and run
                          60 more steps.
 The driver, run on the same inputs at FP64, must write the same files: text
@@ -82,7 +83,7 @@ def compare(tmp_path, golden, prefix):
 
 
 @pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_sched.npz", "cg_outputs_ramp.npz",
-                                     "cg_outputs_psi.npz"])
+                                     "cg_outputs_psi.npz", "cg_outputs_cap.npz"])
 def test_cg_driver_writes_the_reference_files(L, fixture, tmp_path):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
