@@ -375,7 +375,8 @@ def run_serve(a):
     tol, every = 1e-6, 100
     lat, results, ids = [], {}, {}
     with lbm_b200.Server(capacity_nodes=a.pool_nodes, max_active=64, precision="f32", tol=tol, check_every=every,
-                         max_steps=400000, device=local, target_active_nodes=a.target_nodes) as srv:
+                         max_steps=400000, device=local, target_active_nodes=a.target_nodes,
+                         policy=a.policy) as srv:
         barrier(pg)
         t0 = srv.now()
         nxt = 0
@@ -424,7 +425,7 @@ def run_serve(a):
             "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{a.requests} Poisson requests at {a.rate}/s, edge log-U[32,192], porosity "
                                    "U[0.2,0.5], r U[3,8], gx=1e-6, tau=0.8, stop test 1e-6 per 100 steps",
-                       "seed": 505, "pool_nodes": a.pool_nodes, "target_active_nodes": a.target_nodes},
+                       "seed": 505, "pool_nodes": a.pool_nodes, "target_active_nodes": a.target_nodes, "policy": a.policy},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
             "makespan_s": t_end, "converged": sum(r["status"] == 0 for r in results.values()),
@@ -529,6 +530,7 @@ def main():
     ap.add_argument("--instances", type=int, default=64, help="batch: number of config-4 solves")
     ap.add_argument("--batch-block", type=int, default=0, help="batch: fixed block size, reference order (0 = autotune)")
     ap.add_argument("--rate", type=float, default=8.0)
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"], help="serve: admission order")
     ap.add_argument("--pool-nodes", type=int, default=96 * 1024 * 1024)
     ap.add_argument("--fp64-sample", type=int, default=6)
     ap.add_argument("--target-nodes", type=int, default=1024 * 1024,

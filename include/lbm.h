@@ -632,7 +632,13 @@ typedef struct lbm_server_config {
                                     (0 = no limit but memory): enough nodes to
                                     keep HBM busy, no more, so each resident
                                     solve gets a large share of the device */
+  int policy;                /* admission order: LBM_SERVE_FIFO (arrival) or
+                                LBM_SERVE_SHORTEST_FIRST (least estimated
+                                work first: cells x nx^2; a stream of small
+                                requests can hold a large one back) */
 } lbm_server_config;
+#define LBM_SERVE_FIFO 0
+#define LBM_SERVE_SHORTEST_FIRST 1
 
 typedef struct lbm_server_result {
   long long request_id;
@@ -649,8 +655,8 @@ LBM_API lbm_status lbm_server_create(const lbm_server_config* c, lbm_server** ou
 LBM_API lbm_status lbm_server_submit(lbm_server* s, const lbm_instance* req, long long* request_id);
 /* One round: the resident solves advance check_every steps on the device
  * while the host prepares queued requests; finished solves are retired and
- * their nodes freed; queued requests are admitted (first fit, in arrival
- * order with skip-ahead) as slots and pool memory allow. */
+ * their nodes freed; queued requests are admitted (first fit, in the
+ * policy's order with skip-ahead) as slots and pool memory allow. */
 LBM_API lbm_status lbm_server_pump(lbm_server* s, int* n_active, int* n_queued);
 /* Moves up to max finished results into out; *n_out = number written. */
 LBM_API lbm_status lbm_server_poll(lbm_server* s, lbm_server_result* out, int max, int* n_out);

@@ -698,6 +698,8 @@ void lbm_server_config_default(lbm_server_config* c) {
 lbm_status lbm_server_create(const lbm_server_config* c, lbm_server** out) {
   if (!c || !out || c->max_active <= 0 || c->check_every <= 0 || !(c->tol > 0))
     return fail(LBM_ERR_ARG, "lbm_server_create: bad config");
+  if (c->policy != LBM_SERVE_FIFO && c->policy != LBM_SERVE_SHORTEST_FIRST)
+    return fail(LBM_ERR_ARG, "lbm_server_create: unknown admission policy");
   *out = nullptr;
   if (c->precision != LBM_PREC_F32 && c->precision != LBM_PREC_F16)
     return fail(LBM_ERR_ARG, "lbm_server_create: precision must be F32 or F16");
@@ -773,11 +775,18 @@ lbm_status lbm_server_pump(lbm_server* s, int* n_active, int* n_queued) {
   long long resident = 0;
   for (int i = 0; i < P.nslots; i++)
     if (P.slot_job[i]) resident += P.slot_job[i]->geo.count;
+  if (s->cfg.policy == LBM_SERVE_SHORTEST_FIRST) {
+    // estimated work = cells x (extent along x)^2: the steps to the stop
+    // test grow with the square of the length the flow develops over
+    auto work = [](const std::unique_ptr<Job>& j) { return (double)j->nx * j->ny * j->nz * j->nx * (double)j->nx; };
+    std::stable_sort(s->queue.begin(), s->queue.end(),
+                     [&](const std::unique_ptr<Job>& a, const std::unique_ptr<Job>& b) { return work(a) < work(b); });
+  }
   for (auto it = s->queue.begin(); it != s->queue.end();) {
     Job& j = **it;
     if (!j.built) build_job(&j, P.ordering);
     if (s->cfg.target_active_nodes > 0 && resident > 0 && resident + j.geo.count > s->cfg.target_active_nodes)
-      break;  // in arrival order: later requests wait too
+      break;  // in queue order: later requests wait too
     const int slot = P.free_slot();
     if (slot < 0) break;
     const int t0 = P.alloc_tiles((j.geo.count + kTile - 1) / kTile);

@@ -132,7 +132,8 @@ class SolveResult(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("capacity_nodes", C.c_longlong), ("max_active", C.c_int), ("precision", C.c_int),
                 ("ordering", C.c_int), ("block", C.c_int), ("tol", C.c_double), ("check_every", C.c_int),
-                ("max_steps", C.c_longlong), ("device", C.c_int), ("target_active_nodes", C.c_longlong)]
+                ("max_steps", C.c_longlong), ("device", C.c_int), ("target_active_nodes", C.c_longlong),
+                ("policy", C.c_int)]
 
 
 class ServerResult(C.Structure):
@@ -635,9 +636,11 @@ class Server:
     """Continuous-batching permeability solve server on one GPU."""
 
     def __init__(self, capacity_nodes=64 * 1024 * 1024, max_active=256, precision="f32", ordering="reference",
-                 block=256, tol=1e-6, check_every=100, max_steps=1_000_000, device=0, target_active_nodes=0):
+                 block=256, tol=1e-6, check_every=100, max_steps=1_000_000, device=0, target_active_nodes=0,
+                 policy="fifo"):
         c = ServerConfig()
         lib().lbm_server_config_default(C.byref(c))
+        c.policy = {"fifo": 0, "shortest": 1}[policy] if isinstance(policy, str) else int(policy)
         c.target_active_nodes = int(target_active_nodes)
         c.capacity_nodes = int(capacity_nodes)
         c.max_active = int(max_active)

@@ -103,15 +103,15 @@ def test_batch_fp16_close_to_fp32(L, masks):
             np.testing.assert_allclose(c["perm"][0], a["perm"][0], rtol=1e-2)
 
 
-@pytest.mark.parametrize("target", [0, 30000])
-def test_server_continuous_batching_matches_batch(L, masks, target):
+@pytest.mark.parametrize("target,policy", [(0, "fifo"), (30000, "fifo"), (30000, "shortest")])
+def test_server_continuous_batching_matches_batch(L, masks, target, policy):
     tol, every = 1e-4, 50
     with L.Batch([(m, NU, G) for m in masks], precision="f32") as b:
         want = b.run(tol=tol, check_every=every, max_steps=20000)
     # a pool that holds the biggest request but not all of them at once
     big = max(int((m == 0).sum()) for m in masks)
     with L.Server(capacity_nodes=big + 2048, max_active=3, precision="f32", tol=tol, check_every=every,
-                  max_steps=20000, target_active_nodes=target) as srv:
+                  max_steps=20000, target_active_nodes=target, policy=policy) as srv:
         ids = [srv.submit(m, NU, G) for m in masks]
         got, rounds, saw_queue = {}, 0, False
         while len(got) < len(masks):
@@ -126,6 +126,12 @@ def test_server_continuous_batching_matches_batch(L, masks, target):
             r = got[rid]
             assert r["status"] == 0 and r["steps"] == want[i]["steps"] and r["perm"][0] == want[i]["perm"][0]
             assert r["t_submit"] <= r["t_admit"] <= r["t_done"]
+        if policy == "shortest":
+            # admitted in ascending estimated work (cells x nx^2), not in
+            # arrival order: [0, 2, 1, 3] for these masks
+            work = [m.size * m.shape[2] ** 2 for m in masks]
+            admitted = [ids.index(r["request_id"]) for r in sorted(got.values(), key=lambda r: r["t_admit"])]
+            assert admitted == [int(i) for i in np.argsort(work)] and admitted != sorted(admitted)
 
 
 def test_server_rejects_oversized_and_bad_requests(L, masks):
