@@ -344,6 +344,23 @@ typedef struct lbm_cg_handle lbm_cg_handle;
  * reference's phase file; read as float, CG3:2144-2150). */
 LBM_API lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const double* psi, int nx, int ny,
                                  int nz, lbm_cg_handle** out);
+/* As lbm_cg_create with pressure/velocity faces: boundary_pressure
+ * (CG3:4221-4682) and boundary_velocity (CG3:4026-4220) with the rules,
+ * face lists and quirks of the single-phase solver (the two programs share
+ * these functions), acting on the post-streaming populations of the face
+ * nodes between collision and the macro step.  in_bc adds the pressure-
+ * gradient term |p_+ - p_-| c_s^2 / n_axis to the permeabilities' divisor
+ * (Comput_Perm, CG3:5137-5149).  bc may be null (fully periodic).  Replaces
+ * the reference's boundary step in its main loop (CG3:868-876). */
+LBM_API lbm_status lbm_cg_create_bc(const lbm_cg_params* p, const lbm_boundary* bc, const uint8_t* mask,
+                                    const double* psi, int nx, int ny, int nz, lbm_cg_handle** out);
+/* Face densities p_xp..p_zn and normal velocities v_xp..v_zn from now on,
+ * and whether the face rules run at the steps from now on (the reference
+ * runs them only from stab_time when the stabiliser is on, CG3:868).  A
+ * change between steps acts on the step just run, as pressure_bodyforce_change
+ * and pressure_capillary change p_* between collision and boundary_pressure
+ * (CG3:851-871). */
+LBM_API lbm_status lbm_cg_set_faces(lbm_cg_handle* h, const double rho[6], const double vel[6], int active);
 /* collision (CG3:2546-3290) + comput_macro_variables (CG3:3316-3370), n times */
 LBM_API lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps);
 LBM_API lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out);
@@ -444,13 +461,13 @@ LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, doub
 /* Reads the INPUT file, the geometry and the phase file and creates the
  * solver with the file's physics: psi_solid = ContactAngle_parameter, the
  * force off until stab_time when the stabiliser is on, the flux thresholds
- * rel_perm_psi / rel_perm_psi2, PerDir and the permeability window.  Options
- * outside a fully periodic run with the phase read from file (pressure or
- * velocity faces, psi faces other than the initial phase, random or mixture
- * initialisation, a
- * self-defined lattice velocity, a non-zero initial velocity, drainage /
- * imbibition control, dynamic input) are
- * rejected with LBM_ERR_ARG naming the field. */
+ * rel_perm_psi / rel_perm_psi2, PerDir, the permeability window and the
+ * pressure/velocity faces (Sub_BC, in_BC; their rules off until stab_time
+ * when the stabiliser is on).  Options outside a run with the phase read
+ * from file (psi faces other than the initial phase, random or mixture
+ * initialisation, a self-defined lattice velocity, a non-zero initial
+ * velocity, drainage / imbibition control, dynamic input) are rejected with
+ * LBM_ERR_ARG naming the field. */
 LBM_API lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
                                             lbm_cg_input* parsed_out);
 

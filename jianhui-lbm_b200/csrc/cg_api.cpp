@@ -60,6 +60,15 @@ struct lbm_cg_handle {
   std::vector<double> psi0;               // initial phase per node (internal order), as read
   long long window_volume = 0;            // divisor of the fluxes and the saturation
   bool uprev_valid = false;
+  // pressure/velocity faces (bc_nface = 0: none).  The rules of a step are
+  // applied to the state it leaves when that state is next used: by the
+  // following step or by a reader (faces_pending), so that a face density
+  // set between steps acts on the step just run, as the reference changes
+  // p_* between collision and boundary_pressure.
+  lbm_boundary bc{};
+  Dev bc_nodes, bc_off, bc_ops, bc_snap, bc_rec;
+  int bc_nface = 0, bc_nsnap = 0;
+  bool faces_pending = false;
   int perdir = 1;
   int cur = 0;
   // 1: initial state (rho = 1, u = 0, psi / rho_r / rho_b given);
@@ -113,18 +122,63 @@ cudaError_t colour_pass(lbm_cg_handle* h, const CgArgs& a) {
   return e;
 }
 
-cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u = false) {
-  const CgArgs a = cg_args(h, c, given, write_u);
+CgBcArgs bc_args(lbm_cg_handle* h, int c) {
+  CgBcArgs b{};
+  b.f = h->f[c].p;
+  b.table = h->table.as<int32_t>();
+  b.npad = h->geo.npad;
+  b.nodes = h->bc_nodes.as<int32_t>();
+  b.op_off = h->bc_off.as<int32_t>();
+  b.ops = h->bc_ops.as<BcOp>();
+  b.nface = h->bc_nface;
+  b.snap_nodes = h->bc_snap.as<int32_t>();
+  b.rec = h->bc_rec.as<double>();
+  b.nsnap = h->bc_nsnap;
+  for (int d = 0; d < 3; d++) b.gm[d] = h->cp.gm[d];
+  for (int f = 0; f < 6; f++) {
+    b.face_rho[f] = h->cp.face_rho[f];
+    for (int d = 0; d < 3; d++) b.face_u[f][d] = h->cp.face_u[f][d];
+  }
+  return b;
+}
+
+// The rules of the step that produced state c (pending), then the record of
+// state c that this step's rules will read when they are on.
+cudaError_t face_passes(lbm_cg_handle* h, int c, int given, bool pending) {
+  if (h->bc_nface == 0) return cudaSuccess;
+  CgBcArgs b = bc_args(h, c);
   cudaError_t e = cudaSuccess;
-  if (!given) e = colour_pass(h, a);
+  if (pending) e = cg_bc_faces(h->f64, b, h->stream);
+  if (e == cudaSuccess && h->cp.faces) {
+    b.given = given == 1;
+    e = cg_bc_record(h->f64, b, h->stream);
+  }
+  return e;
+}
+
+// Applies the pending rules to the current state before it is read.
+cudaError_t resolve_faces(lbm_cg_handle* h) {
+  if (!h->faces_pending) return cudaSuccess;
+  h->faces_pending = false;
+  return cg_bc_faces(h->f64, bc_args(h, h->cur), h->stream);
+}
+
+cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u, bool pending) {
+  const CgArgs a = cg_args(h, c, given, write_u);
+  cudaError_t e = face_passes(h, c, given, pending);
+  if (e == cudaSuccess && !given) e = colour_pass(h, a);
   if (e != cudaSuccess) return e;
   return h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
 }
 
 bool same_params(const CgParams& a, const CgParams& b) {
   bool same = a.psi_solid == b.psi_solid && a.cap_a == b.cap_a && a.body_force_phase == b.body_force_phase &&
-              a.flux_psi == b.flux_psi;
+              a.flux_psi == b.flux_psi && a.faces == b.faces;
   for (int d = 0; d < 3; d++) same = same && a.g[d] == b.g[d] && a.gm[d] == b.gm[d];
+  for (int f = 0; f < 6; f++) {
+    same = same && a.face_rho[f] == b.face_rho[f];
+    for (int d = 0; d < 3; d++) same = same && a.face_u[f][d] == b.face_u[f][d];
+  }
   return same;
 }
 
@@ -137,7 +191,9 @@ void drop_graphs(lbm_cg_handle* h) {
 }
 
 // Chains of kCgGraphSteps running steps, captured with the steady parameters
-// (gm = g); a parameter change drops them.
+// (gm = g); a parameter change drops them.  Every captured step applies the
+// previous step's rules when the faces are on, so a chain starts from a
+// state whose rules are pending exactly when the faces are on.
 lbm_status cg_graph(lbm_cg_handle* h, int c0) {
   CgParams steady = h->cp;
   for (int d = 0; d < 3; d++) steady.gm[d] = steady.g[d];
@@ -151,7 +207,7 @@ lbm_status cg_graph(lbm_cg_handle* h, int c0) {
   cudaError_t err = cudaSuccess;
   int c = c0;
   for (int s = 0; s < kCgGraphSteps && err == cudaSuccess; s++) {
-    err = one_cg_step(h, c, 0);
+    err = one_cg_step(h, c, 0, false, steady.faces != 0);
     c = 1 - c;
   }
   h->cp = saved;
@@ -208,6 +264,7 @@ lbm_status cg_check(lbm_cg_handle* h) {
 // Runs the colour pass (when the state is not the initial one) and the
 // diagnostics reduction; optional macro fields in internal order.
 lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double* u_out, double* r2 = nullptr) {
+  LBM_CUDA_TRY(resolve_faces(h));
   if (!h->given) {
     const CgArgs a = cg_args(h, h->cur, 0);
     LBM_CUDA_TRY(colour_pass(h, a));
@@ -245,8 +302,20 @@ extern "C" {
 
 lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const double* psi_cells, int nx, int ny,
                          int nz, lbm_cg_handle** out) {
+  return lbm_cg_create_bc(p, nullptr, mask, psi_cells, nx, ny, nz, out);
+}
+
+lbm_status lbm_cg_create_bc(const lbm_cg_params* p, const lbm_boundary* bc, const uint8_t* mask,
+                            const double* psi_cells, int nx, int ny, int nz, lbm_cg_handle** out) {
   if (!p || !mask || !psi_cells || !out || nx <= 0 || ny <= 0 || nz <= 0)
     return fail(LBM_ERR_ARG, "lbm_cg_create: bad argument");
+  if (bc) {
+    for (int f = 0; f < 6; f++)
+      if ((bc->pressure[f] != 0 && bc->pressure[f] != 1) || (bc->velocity[f] != 0 && bc->velocity[f] != 1))
+        return fail(LBM_ERR_ARG, "lbm_cg_create: face flags must be 0 or 1");
+    if (bc_active(*bc) && (bc->sub_bc < 0 || bc->sub_bc > 3))
+      return fail(LBM_ERR_ARG, "lbm_cg_create: Sub_BC must be 0..3");
+  }
   *out = nullptr;
   if (!(p->nu_l > 0) || !(p->nu_g > 0)) return fail(LBM_ERR_ARG, "lbm_cg_create: viscosities must be positive");
   if (p->precision != LBM_PREC_F64 && p->precision != LBM_PREC_F32)
@@ -272,6 +341,14 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
 
   // constants of init (CG3:2226-2260)
   CgParams& cp = h->cp;
+  if (bc) {
+    h->bc = *bc;
+    cp.faces = 1;
+    for (int f = 0; f < 6; f++) {
+      cp.face_rho[f] = bc->rho[f];
+      cp.face_u[f][f / 2] = bc->vel[f];
+    }
+  }
   cp.psi_solid = p->psi_solid;
   cp.cap_a = p->cap_a;
   cp.g[0] = cp.gm[0] = p->gx;
@@ -327,13 +404,35 @@ lbm_status lbm_cg_create(const lbm_cg_params* p, const uint8_t* mask, const doub
   LBM_CUDA_TRY(cudaMemcpyAsync(h->ref_of.p, g.ref_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice,
                                h->stream));
   std::vector<uint8_t> order;
+  // the FP64 inverse also serves the Sub_BC 2 pressure rule of both precisions
+  LBM_CUDA_TRY(cg_set_mi_f64(&h->MI[0][0], h->stream));
   if (h->f64) {
     build_colour_order(g, order);
     LBM_CUDA_TRY(h->corder.alloc(order.size()));
     LBM_CUDA_TRY(cudaMemcpyAsync(h->corder.p, order.data(), order.size(), cudaMemcpyHostToDevice, h->stream));
-    LBM_CUDA_TRY(cg_set_mi_f64(&h->MI[0][0], h->stream));
   } else {
     LBM_CUDA_TRY(cg_set_mi_f32(&h->MI[0][0], h->stream));
+  }
+  BcLists bl;
+  if (bc) bc_node_lists(*bc, g, &bl);
+  if (!bl.nodes.empty()) {
+    h->bc_nface = (int)bl.nodes.size();
+    h->bc_nsnap = (int)bl.snap_nodes.size();
+    LBM_CUDA_TRY(h->bc_nodes.alloc(bl.nodes.size() * sizeof(int32_t)));
+    LBM_CUDA_TRY(h->bc_off.alloc(bl.op_off.size() * sizeof(int32_t)));
+    LBM_CUDA_TRY(h->bc_ops.alloc(bl.ops.size() * sizeof(BcOp)));
+    LBM_CUDA_TRY(h->bc_snap.alloc(std::max<size_t>(bl.snap_nodes.size(), 1) * sizeof(int32_t)));
+    LBM_CUDA_TRY(h->bc_rec.alloc((size_t)(kQ + 4) * std::max(h->bc_nsnap, 1) * sizeof(double)));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_nodes.p, bl.nodes.data(), bl.nodes.size() * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_off.p, bl.op_off.data(), bl.op_off.size() * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_ops.p, bl.ops.data(), bl.ops.size() * sizeof(BcOp), cudaMemcpyHostToDevice,
+                                 h->stream));
+    if (!bl.snap_nodes.empty())
+      LBM_CUDA_TRY(cudaMemcpyAsync(h->bc_snap.p, bl.snap_nodes.data(), bl.snap_nodes.size() * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, h->stream));
+    LBM_CUDA_TRY(cudaMemsetAsync(h->bc_rec.p, 0, h->bc_rec.bytes, h->stream));
   }
   // init (CG3:2360-2380): f = feq(1, 0) = first column of M^-1 in CG order,
   // psi from the phase file as float, rho_r = (psi + 1)/2, rho_b = 1 - rho_r
@@ -382,6 +481,9 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   // falls between the pending macro step and the next collision
   bool special = h->given != 0;
   for (int d = 0; d < 3; d++) special = special || h->cp.gm[d] != h->cp.g[d];
+  // ... and when the state's pending rules differ from what a chain assumes
+  const bool faces_on = h->bc_nface > 0 && h->cp.faces;
+  special = special || (h->bc_nface > 0 && h->faces_pending != faces_on);
   if (left - (special ? 1 : 0) - 1 >= kCgGraphSteps) {
     const int c0 = h->cur;
     for (int c = 0; c < 2; c++)
@@ -390,7 +492,7 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   }
   LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
   if (special) {
-    LBM_CUDA_TRY(one_cg_step(h, h->cur, h->given, left == 1));
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, h->given, left == 1, h->faces_pending));
     h->cur = 1 - h->cur;
     h->given = 0;
     for (int d = 0; d < 3; d++) h->cp.gm[d] = h->cp.g[d];
@@ -402,10 +504,11 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   }
   // the last step also writes its pre-collision u (Error's u0 of the next report)
   while (left > 0) {
-    LBM_CUDA_TRY(one_cg_step(h, h->cur, 0, left == 1));
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, 0, left == 1, faces_on));
     h->cur = 1 - h->cur;
     left--;
   }
+  h->faces_pending = faces_on;
   h->uprev_valid = true;
   LBM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
   LBM_CUDA_TRY(cudaEventSynchronize(h->ev1));
@@ -425,7 +528,16 @@ lbm_status lbm_cg_reduce(lbm_cg_handle* h, lbm_cg_diag* out) {
   const Geometry& g = h->geo;
   // fluxes and saturation over the window volume, Error over the box; the
   // porosity is the window's pore fraction (CG3:1851, 5217-5227, 5361)
-  const double V = (double)g.nx * g.ny * g.nz, Vw = (double)h->window_volume, phi = g.porosity, dp = 0.0;
+  const double V = (double)g.nx * g.ny * g.nz, Vw = (double)h->window_volume, phi = g.porosity;
+  // pressure-gradient term (CG3:5137-5149): |p_+ - p_-| c_s^2 / (N + 1) / dx
+  // along PerDir (x for anything but 2 and 3), when in_BC is set
+  double dp = 0.0;
+  if (h->bc.in_bc != 0) {
+    const int a = h->prm.perdir == 2 ? 1 : h->prm.perdir == 3 ? 2 : 0;
+    const int ext[3] = {g.nx, g.ny, g.nz};
+    const double c_s2 = 1.0 * 1.0 / 3, dx = 1.0;
+    dp = std::fabs(h->cp.face_rho[2 * a] - h->cp.face_rho[2 * a + 1]) * c_s2 / ext[a] / dx;
+  }
   const double* gg = h->cp.gm;  // gxs when the macro step ran
   std::memset(out, 0, sizeof(*out));
   out->step = h->step;
@@ -494,6 +606,7 @@ lbm_status lbm_cg_get_populations(lbm_cg_handle* h, double* f) {
   lbm_status st = cg_check(h);
   if (st != LBM_OK) return st;
   if (!f) return fail(LBM_ERR_ARG, "lbm_cg_get_populations: null output");
+  LBM_CUDA_TRY(resolve_faces(h));
   const int n = h->geo.count;
   Dev o;
   LBM_CUDA_TRY(o.alloc((size_t)(n + 1) * kQ * sizeof(double)));
@@ -518,6 +631,20 @@ lbm_status lbm_cg_set_body_force(lbm_cg_handle* h, double gx, double gy, double 
   h->prm.gx = gx;
   h->prm.gy = gy;
   h->prm.gz = gz;
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_set_faces(lbm_cg_handle* h, const double rho[6], const double vel[6], int active) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!rho || !vel) return fail(LBM_ERR_ARG, "lbm_cg_set_faces: null argument");
+  for (int f = 0; f < 6; f++) {
+    h->cp.face_rho[f] = rho[f];
+    h->bc.rho[f] = rho[f];
+    h->bc.vel[f] = vel[f];
+    for (int d = 0; d < 3; d++) h->cp.face_u[f][d] = d == f / 2 ? vel[f] : 0.0;
+  }
+  h->cp.faces = active != 0;
   return LBM_OK;
 }
 
@@ -627,6 +754,7 @@ lbm_status lbm_cg_set_state(lbm_cg_handle* h, const double* f, const double* psi
   }
   h->given = 2;
   h->uprev_valid = false;
+  h->faces_pending = false;  // the state given is the one after its step's rules
   return LBM_OK;
 }
 
@@ -644,8 +772,12 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
   lbm_status st = read_cg_input_file(input_path, &in);
   if (st != LBM_OK) return st;
   if (parsed_out) *parsed_out = in;
-  // a fully periodic run with the phase read from file (CG3:2355-2380)
-  if (in.in_bc != 0) return fail(LBM_ERR_ARG, "in_BC: pressure / velocity faces are not supported by lbm_cg");
+  // the phase read from file (CG3:2355-2380)
+  const int pre[6] = {in.pre_xp, in.pre_xn, in.pre_yp, in.pre_yn, in.pre_zp, in.pre_zn};
+  const int vel[6] = {in.vel_xp, in.vel_xn, in.vel_yp, in.vel_yn, in.vel_zp, in.vel_zn};
+  for (int f = 0; f < 6; f++)
+    if ((pre[f] != 0 && pre[f] != 1) || (vel[f] != 0 && vel[f] != 1))
+      return fail(LBM_ERR_ARG, "pre_* / vel_*: face flags must be 0 or 1");
   const int pf[6] = {in.psi_xp, in.psi_xn, in.psi_yp, in.psi_yn, in.psi_zp, in.psi_zn};
   for (int f = 0; f < 6; f++)
     if (in.in_psi_bc == 1 && pf[f] != 0 && pf[f] != 1)
@@ -688,8 +820,22 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
   p.precision = precision;
   p.device = 0;
   p.perdir = in.perdir;
+  // pressure/velocity faces, their rules from stab_time when the stabiliser
+  // is on (CG3:868)
+  lbm_boundary bc{};
+  bc.sub_bc = in.sub_bc;
+  bc.in_bc = in.in_bc;
+  const double rho_f[6] = {in.p_xp, in.p_xn, in.p_yp, in.p_yn, in.p_zp, in.p_zn};
+  const double vel_f[6] = {in.v_xp, in.v_xn, in.v_yp, in.v_yn, in.v_zp, in.v_zn};
+  for (int f = 0; f < 6; f++) {
+    bc.pressure[f] = pre[f];
+    bc.velocity[f] = vel[f];
+    bc.rho[f] = rho_f[f];
+    bc.vel[f] = vel_f[f];
+  }
   lbm_cg_handle* h = nullptr;
-  if ((st = lbm_cg_create(&p, mask.data(), psi.data(), in.nx, in.ny, in.nz, &h)) != LBM_OK) return st;
+  if ((st = lbm_cg_create_bc(&p, &bc, mask.data(), psi.data(), in.nx, in.ny, in.nz, &h)) != LBM_OK) return st;
+  if (stab && in.stab_time > 0) h->cp.faces = 0;
   if (in.par_per_x || in.par_per_y || in.par_per_z) {
     // an axis without a partial window spans the whole box (CG3:1707-1712);
     // the sums are limited to the window when one of par_per_* is 1

@@ -15,6 +15,11 @@ struct CgParams {
   double flux_psi;
   // viscosity interpolation (CG3 init, delta = 0.1)
   double wl, wg, lg0, l1, l2, g1, g2, delta;
+  // pressure/velocity faces: rules on at this step, face densities and
+  // velocities (xp, xn, yp, yn, zp, zn)
+  int faces;
+  double face_rho[6];
+  double face_u[6][3];
 };
 
 struct CgArgs {
@@ -53,6 +58,28 @@ struct CgReduceArgs {
   double* result2;         // |du|^2, |u|^2, |u|, max |u|^2, sd_l, sd_g, 0, 0
   const uint8_t* win;      // [npad] 1 = node inside the permeability window, or null (all)
 };
+
+// Pressure/velocity faces of the two-phase model: the record pass stores f,
+// rho, u of the nodes the rules read ([23][nsnap] doubles); the face pass
+// applies the rules to the face nodes' pulled populations in place.
+struct CgBcArgs {
+  void* f;                  // [19][npad] populations whose pulled state is acted on
+  const int32_t* table;
+  int npad;
+  const int32_t* nodes;     // [nface] face nodes (internal index)
+  const int32_t* op_off;    // [nface + 1]
+  const BcOp* ops;
+  int nface;
+  const int32_t* snap_nodes;  // [nsnap] nodes the rules read
+  double* rec;              // [23][nsnap]: f_0..f_18 (CG order), rho, ux, uy, uz
+  int nsnap;
+  int given;                // record pass: rho = 1, u = 0 (initial state)
+  double gm[3];             // record pass: force of the macro step
+  double face_rho[6];       // xp, xn, yp, yn, zp, zn
+  double face_u[6][3];
+};
+cudaError_t cg_bc_record(bool f64, const CgBcArgs& a, cudaStream_t st);
+cudaError_t cg_bc_faces(bool f64, const CgBcArgs& a, cudaStream_t st);
 
 cudaError_t cg_set_mi_f64(const double* mi, cudaStream_t st);
 cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st);

@@ -55,6 +55,178 @@ cudaError_t cg_phase_faces(bool f64, const int32_t* nodes, const double* psi0, i
   return cudaGetLastError();
 }
 
+// ------------------------------------------------- pressure/velocity faces
+// boundary_pressure (CG3:4221-4682) and boundary_velocity (CG3:4026-4220)
+// act on the post-streaming populations F of the face nodes between
+// collision and comput_macro_variables, reading f, rho and u of the previous
+// macro step.  Both kernels work on full populations in double in the CG
+// direction order with CG3's feq (CG3:2503-2520), M (CG3:63-83), MI and LR.
+
+// feq (CG3:2503-2520) with lat_c = 1, in the reference's operation order.
+__device__ __forceinline__ double cg_feq(int k, double rho, double ux, double uy, double uz) {
+  const double c2 = 1.0, c4 = 1.0;
+  const double eu = (double)cg::ex(k) * ux + (double)cg::ey(k) * uy + (double)cg::ez(k) * uz;
+  const double uv = ux * ux + uy * uy + uz * uz;
+  return weight(k) * rho * (1.0 + 3.0 * eu / c2 + 4.5 * eu * eu / c4 - 1.5 * uv / c2);
+}
+
+__device__ __forceinline__ int cg_lr(int k) { return k == 0 ? 0 : ((k & 1) ? k + 1 : k - 1); }
+
+// F of node x (CG order, full populations) from its pulled slots.
+template <typename T, bool DEV>
+__device__ __forceinline__ void cg_pull_full(const T* __restrict__ f, const int32_t* __restrict__ table, int npad,
+                                             int x, double (&F)[kQ]) {
+#pragma unroll
+  for (int k = 0; k < kQ; k++) {
+    const double v = (double)f[cg_slot(table, npad, x, cg::row(k))];
+    F[k] = DEV ? v + weight(k) : v;
+  }
+}
+
+// Record pass: f, rho, u of every node a rule reads, as the macro step
+// computes them (CG3:3330-3352; u with the pending macro step's force).
+template <typename T, bool DEV>
+__global__ void __launch_bounds__(128) cg_bc_record_kernel(CgBcArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nsnap) return;
+  const int x = a.snap_nodes[i];
+  double F[kQ];
+  cg_pull_full<T, DEV>(static_cast<const T*>(a.f), a.table, a.npad, x, F);
+  double rho, ux, uy, uz;
+  if (a.given) {
+    rho = 1.0;
+    ux = uy = uz = 0.0;
+  } else {
+    double r = F[0];
+#pragma unroll
+    for (int k = 1; k < kQ; k++) r = r + F[k];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+    for (int k = 0; k < kQ; k++) {
+      if (cg::ex(k) == 1) sx = sx + F[k];
+      if (cg::ex(k) == -1) sx = sx - F[k];
+      if (cg::ey(k) == 1) sy = sy + F[k];
+      if (cg::ey(k) == -1) sy = sy - F[k];
+      if (cg::ez(k) == 1) sz = sz + F[k];
+      if (cg::ez(k) == -1) sz = sz - F[k];
+    }
+    rho = r;
+    ux = (sx + 1.0 * a.gm[0] / 2.0) / rho;
+    uy = (sy + 1.0 * a.gm[1] / 2.0) / rho;
+    uz = (sz + 1.0 * a.gm[2] / 2.0) / rho;
+  }
+  const size_t ns = (size_t)a.nsnap;
+#pragma unroll
+  for (int k = 0; k < kQ; k++) a.rec[k * ns + i] = F[k];
+  a.rec[kQ * ns + i] = rho;
+  a.rec[(kQ + 1) * ns + i] = ux;
+  a.rec[(kQ + 2) * ns + i] = uy;
+  a.rec[(kQ + 3) * ns + i] = uz;
+}
+
+// Face pass: the operations of each face node in program order on its pulled
+// F, written back to the same slots (each (node, direction) owns one slot).
+template <typename T, bool DEV>
+__global__ void __launch_bounds__(128) cg_bc_faces_kernel(CgBcArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nface) return;
+  const int x = a.nodes[b];
+  T* __restrict__ f = static_cast<T*>(a.f);
+  double F[kQ];
+  cg_pull_full<T, DEV>(f, a.table, a.npad, x, F);
+  const double* __restrict__ S = a.rec;
+  const size_t ns = (size_t)a.nsnap;
+  for (int o = a.op_off[b]; o < a.op_off[b + 1]; o++) {
+    const BcOp op = a.ops[o];
+    const double rb = a.face_rho[op.face];
+    const double ubx = a.face_u[op.face][0], uby = a.face_u[op.face][1], ubz = a.face_u[op.face][2];
+    const size_t nb = (size_t)(op.nb < 0 ? 0 : op.nb);
+    switch (op.kind) {
+      case kBcPressureRest:
+#pragma unroll
+        for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, rb, 0.0, 0.0, 0.0);
+        break;
+      case kBcPressureNbU: {
+        const double ux = S[(kQ + 1) * ns + nb], uy = S[(kQ + 2) * ns + nb], uz = S[(kQ + 3) * ns + nb];
+#pragma unroll
+        for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, rb, ux, uy, uz);
+        break;
+      }
+      case kBcPressureMoment: {
+        double m[kQ];
+#pragma unroll
+        for (int i = 0; i < kQ; i++) {
+          double acc = 0.0;
+#pragma unroll
+          for (int j = 0; j < kQ; j++) acc = acc + (double)cg::mcoef(i, j) * S[j * ns + nb];
+          m[i] = acc;
+        }
+        m[0] = rb;
+#pragma unroll
+        for (int i = 0; i < kQ; i++) {
+          double acc = 0.0;
+#pragma unroll
+          for (int j = 0; j < kQ; j++) acc = acc + c_MIcg[i * kQ + j] * m[j];
+          F[i] = acc;
+        }
+        break;
+      }
+      case kBcPressureNeq: {
+        const double ux = S[(kQ + 1) * ns + nb], uy = S[(kQ + 2) * ns + nb], uz = S[(kQ + 3) * ns + nb];
+        const double rn = S[kQ * ns + nb];
+#pragma unroll
+        for (int k = 0; k < kQ; k++) {
+          const double f4 = op.nb4 >= 0 ? S[k * ns + (size_t)op.nb4] : 0.0;
+          F[k] = cg_feq(k, rb, ux, uy, uz) + f4 - cg_feq(k, rn, ux, uy, uz);
+        }
+        break;
+      }
+      case kBcVelocityEq:
+#pragma unroll
+        for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, 1.0, ubx, uby, ubz);
+        break;
+      case kBcVelocityNeq:
+#pragma unroll
+        for (int k = 0; k < kQ; k++) {
+          const int e = op.axis == 0 ? cg::ex(k) : (op.axis == 1 ? cg::ey(k) : cg::ez(k));
+          if (op.sign > 0 ? e < 0 : e > 0)
+            F[k] = cg_feq(cg_lr(k), 1.0, ubx, uby, ubz) - F[cg_lr(k)] + cg_feq(k, 1.0, ubx, uby, ubz);
+        }
+        break;
+      case kBcVelocityNbRho: {
+        const double rn = S[kQ * ns + nb];
+#pragma unroll
+        for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, rn, ubx, uby, ubz);
+        break;
+      }
+      default:
+        break;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kQ; k++) f[cg_slot(a.table, a.npad, x, cg::row(k))] = (T)(DEV ? F[k] - weight(k) : F[k]);
+}
+
+cudaError_t cg_bc_record(bool f64, const CgBcArgs& a, cudaStream_t st) {
+  if (a.nsnap <= 0) return cudaSuccess;
+  const int g = (a.nsnap + 127) / 128;
+  if (f64)
+    cg_bc_record_kernel<double, false><<<g, 128, 0, st>>>(a);
+  else
+    cg_bc_record_kernel<float, true><<<g, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t cg_bc_faces(bool f64, const CgBcArgs& a, cudaStream_t st) {
+  if (a.nface <= 0) return cudaSuccess;
+  const int g = (a.nface + 127) / 128;
+  if (f64)
+    cg_bc_faces_kernel<double, false><<<g, 128, 0, st>>>(a);
+  else
+    cg_bc_faces_kernel<float, true><<<g, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t cg_reduce_f64(const CgReduceArgs& a, int nblocks, cudaStream_t st) {
   cg_reduce_kernel<true><<<nblocks, 256, 0, st>>>(a);
   cg_reduce_final_kernel<<<1, 1024, 0, st>>>(a.partials, nblocks, a.result);

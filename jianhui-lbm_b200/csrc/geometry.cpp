@@ -212,14 +212,16 @@ bool bc_active(const lbm_boundary& bc) {
 //     past that list is outside the reference's array; it is dropped);
 //   - pressure Sub_BC 3 takes f - f_eq from the -y neighbour on every face;
 //   - velocity Sub_BC 2: x flags act on the z faces, z flags on the x faces.
-void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPlan* plan) {
-  *plan = BcPlan{};
+namespace {
+
+// One operation of the boundary program, nb / nb4 as reference ids (0 = none).
+struct BcRaw {
+  int32_t target;
+  BcOp op;
+};
+
+std::vector<BcRaw> bc_program(const lbm_boundary& bc, const Geometry* g) {
   const int n = g->count;
-  if (!bc_active(bc) || n == 0) {
-    plan->n_main = plan->snap_begin = n;
-    return;
-  }
-  plan->active = true;
   const int nx = g->nx, ny = g->ny, nz = g->nz;
   std::vector<int32_t> rid((size_t)nx * ny * nz, 0);  // x-fastest cell -> reference id, 0 = solid
   for (int id = 1; id <= n; id++) {
@@ -258,13 +260,9 @@ void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPl
   // INPUT face index (xp, xn, yp, yn, zp, zn) -> list slot, inward push direction
   static const int slot_of[6] = {1, 0, 3, 2, 5, 4};
   static const int dir_in[6] = {2, 1, 4, 3, 6, 5};
-  struct Raw {
-    int32_t target;
-    BcOp op;  // nb / nb4 as reference ids here
-  };
-  std::vector<Raw> prog;
+  std::vector<BcRaw> prog;
   auto emit = [&](int32_t target, int8_t kind, int face, int32_t nb, int32_t nb4, int axis = 0, int sign = 0) {
-    prog.push_back(Raw{target, BcOp{kind, (int8_t)face, (int8_t)axis, (int8_t)sign, nb, nb4}});
+    prog.push_back(BcRaw{target, BcOp{kind, (int8_t)face, (int8_t)axis, (int8_t)sign, nb, nb4}});
   };
   bool any_pre = false, any_vel = false;
   for (int s = 0; s < 6; s++) {
@@ -320,10 +318,26 @@ void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPl
           }
     }
   }
+  (void)n;
+  return prog;
+}
+
+}  // namespace
+
+void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPlan* plan) {
+  (void)mask;
+  *plan = BcPlan{};
+  const int n = g->count;
+  if (!bc_active(bc) || n == 0) {
+    plan->n_main = plan->snap_begin = n;
+    return;
+  }
+  plan->active = true;
+  const std::vector<BcRaw> prog = bc_program(bc, g);
   // classes: 2 = written, 1 = read, 0 = neither
   std::vector<uint8_t> cls((size_t)n + 1, 0);
-  for (const Raw& r : prog) cls[r.target] = 2;
-  for (const Raw& r : prog) {
+  for (const BcRaw& r : prog) cls[r.target] = 2;
+  for (const BcRaw& r : prog) {
     if (r.op.nb > 0 && cls[r.op.nb] == 0) cls[r.op.nb] = 1;
     if (r.op.nb4 > 0 && cls[r.op.nb4] == 0) cls[r.op.nb4] = 1;
   }
@@ -342,16 +356,48 @@ void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPl
   // per boundary node, its operations in program order
   const int nb_nodes = n2;
   plan->op_off.assign((size_t)nb_nodes + 1, 0);
-  for (const Raw& r : prog) plan->op_off[g->int_of[r.target] - plan->n_main + 1]++;
+  for (const BcRaw& r : prog) plan->op_off[g->int_of[r.target] - plan->n_main + 1]++;
   for (int i = 0; i < nb_nodes; i++) plan->op_off[i + 1] += plan->op_off[i];
   plan->ops.resize(prog.size());
   std::vector<int32_t> fill(plan->op_off.begin(), plan->op_off.end() - 1);
   auto slot = [&](int32_t id) { return id > 0 ? g->int_of[id] - plan->snap_begin : -1; };
-  for (const Raw& r : prog) {
+  for (const BcRaw& r : prog) {
     BcOp op = r.op;
     op.nb = slot(r.op.nb);
     op.nb4 = slot(r.op.nb4);
     plan->ops[fill[g->int_of[r.target] - plan->n_main]++] = op;
+  }
+}
+
+void bc_node_lists(const lbm_boundary& bc, const Geometry& g, BcLists* out) {
+  *out = BcLists{};
+  if (!bc_active(bc) || g.count == 0) return;
+  const std::vector<BcRaw> prog = bc_program(bc, &g);
+  // written nodes in order of their first operation, read nodes in order of
+  // first use; both as internal indices
+  std::vector<int32_t> face_of((size_t)g.count + 1, -1), snap_of((size_t)g.count + 1, -1);
+  for (const BcRaw& r : prog) {
+    if (face_of[r.target] < 0) {
+      face_of[r.target] = (int32_t)out->nodes.size();
+      out->nodes.push_back(g.int_of[r.target]);
+    }
+    for (int32_t id : {r.op.nb, r.op.nb4})
+      if (id > 0 && snap_of[id] < 0) {
+        snap_of[id] = (int32_t)out->snap_nodes.size();
+        out->snap_nodes.push_back(g.int_of[id]);
+      }
+  }
+  const size_t nf = out->nodes.size();
+  out->op_off.assign(nf + 1, 0);
+  for (const BcRaw& r : prog) out->op_off[face_of[r.target] + 1]++;
+  for (size_t i = 0; i < nf; i++) out->op_off[i + 1] += out->op_off[i];
+  out->ops.resize(prog.size());
+  std::vector<int32_t> fill(out->op_off.begin(), out->op_off.end() - 1);
+  for (const BcRaw& r : prog) {
+    BcOp op = r.op;
+    op.nb = r.op.nb > 0 ? snap_of[r.op.nb] : -1;
+    op.nb4 = r.op.nb4 > 0 ? snap_of[r.op.nb4] : -1;
+    out->ops[fill[face_of[r.target]]++] = op;
   }
 }
 

@@ -16,6 +16,8 @@
 // surface-tension change of rel_perm_ift (CG3:892-893) and the least-squares
 // fit of the relative permeabilities (Least_Square_Rel_Perm, CG3:1201-1250)
 // and the capillary-pressure stepping (pressure_capillary, CG3:1427-1600).
+// Pressure and velocity faces (boundary_pressure / boundary_velocity,
+// CG3:868-876) follow the face densities these schedules move.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -324,6 +326,20 @@ int main(int argc, char** argv) {
     o << "The expected completion time is " << th << "h" << tm << "m" << ts << "s" << std::endl;
   };
 
+  // face densities p_xp..p_zn as the ramps move them, and whether the face
+  // rules run (from stab_time with the stabiliser, CG3:868)
+  const double v_face[6] = {in.v_xp, in.v_xn, in.v_yp, in.v_yn, in.v_zp, in.v_zn};
+  bool faces_on = !(stab && in.stab_time > 0);
+  double rho_set[6] = {in.p_xp, in.p_xn, in.p_yp, in.p_yn, in.p_zp, in.p_zn};
+  auto sync_faces = [&](bool force) {
+    const double r[6] = {drv.p_p[0], drv.p_n[0], drv.p_p[1], drv.p_n[1], drv.p_p[2], drv.p_n[2]};
+    bool same = !force;
+    for (int f = 0; f < 6; f++) same = same && r[f] == rho_set[f];
+    if (same) return true;
+    for (int f = 0; f < 6; f++) rho_set[f] = r[f];
+    return lbm_cg_set_faces(h, rho_set, v_face, faces_on ? 1 : 0) == LBM_OK;
+  };
+
   long long n = 0;
   while (n <= in.n_max) {
     if (stab && n == in.stab_time) {
@@ -331,6 +347,8 @@ int main(int argc, char** argv) {
       for (int k = 0; k < 3; k++) drv.g[k] = gbase[k];
       if (lbm_cg_set_body_force(h, drv.g[0], drv.g[1], drv.g[2], LBM_CG_FORCE_BEFORE_COLLISION) != LBM_OK)
         return die("lbm_cg_set_body_force");
+      faces_on = true;
+      if (!sync_faces(true)) return die("lbm_cg_set_faces");
     }
     // last step of this chunk: the next report, the step before the
     // stabiliser switch, or a ramp step (ramps run one step at a time)
@@ -354,6 +372,7 @@ int main(int argc, char** argv) {
     if ((moved || moved2) &&
         lbm_cg_set_body_force(h, drv.g[0], drv.g[1], drv.g[2], LBM_CG_FORCE_BEFORE_MACRO) != LBM_OK)
       return die("lbm_cg_set_body_force");
+    if (!sync_faces(false)) return die("lbm_cg_set_faces");
     if (n % in.fre_re != 0) {
       n++;
       continue;

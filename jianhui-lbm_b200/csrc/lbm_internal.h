@@ -152,6 +152,14 @@ bool bc_active(const lbm_boundary& bc);
 // Reorders g (ref_of / int_of) into the three classes, keeping the order
 // within each class, and builds the per-node operation lists.
 void bc_partition(const uint8_t* mask, const lbm_boundary& bc, Geometry* g, BcPlan* plan);
+// The same program without reordering: the written nodes (internal indices)
+// with their operations (CSR, program order per node) and the nodes whose
+// state the operations read; BcOp.nb / nb4 index snap_nodes (-1 = none).
+struct BcLists {
+  std::vector<int32_t> nodes, op_off, snap_nodes;
+  std::vector<BcOp> ops;
+};
+void bc_node_lists(const lbm_boundary& bc, const Geometry& g, BcLists* out);
 
 // Two pinned staging buffers for device -> pageable host copies (allocated
 // on first use, owned by a handle; one copy at a time).

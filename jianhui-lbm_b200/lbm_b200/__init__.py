@@ -283,6 +283,9 @@ _SIGNATURES = {
     "lbm_cg_destroy": ([C.c_void_p], None),
     "lbm_cg_set_body_force": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int], C.c_int),
     "lbm_cg_set_cap_a": ([C.c_void_p, C.c_double], C.c_int),
+    "lbm_cg_create_bc": ([C.POINTER(CGParams), C.POINTER(Boundary), _U8P, _F64P, C.c_int, C.c_int, C.c_int,
+                          C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_cg_set_faces": ([C.c_void_p, _F64P, _F64P, C.c_int], C.c_int),
     "lbm_cg_set_window": ([C.c_void_p, _I32P, C.c_int], C.c_int),
     "lbm_cg_set_state": ([C.c_void_p, _F64P, _F64P, _F64P, _F64P], C.c_int),
     "lbm_cg_set_phase_faces": ([C.c_void_p, _I32P], C.c_int),
@@ -443,18 +446,21 @@ def read_velocity_for_solute(path, mask, order="slab"):
 class ColourGradient:
     """Colour-gradient two-phase solve (periodic) on one GPU.
 
-    ``psi`` holds the initial phase per cell, (nz, ny, nx), +1 = component r."""
+    ``psi`` holds the initial phase per cell, (nz, ny, nx), +1 = component r.
+    ``boundary`` (a ``Boundary``) adds pressure/velocity faces."""
 
     def __init__(self, mask, psi, nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0),
-                 body_force_phase=-1, flux_psi=0.99, flux_umax=0.01, precision="f32", device=0, perdir=1):
+                 body_force_phase=-1, flux_psi=0.99, flux_umax=0.01, precision="f32", device=0, perdir=1,
+                 boundary=None):
         m = np.ascontiguousarray(mask, dtype=np.uint8)
         nz, ny, nx = m.shape
         p = CGParams(float(nu_l), float(nu_g), float(psi_solid), float(cap_a), float(g[0]), float(g[1]), float(g[2]),
                      int(body_force_phase), float(flux_psi), float(flux_umax),
                      PRECISIONS[precision] if isinstance(precision, str) else int(precision), int(device), int(perdir))
         h = C.c_void_p()
-        _check(lib().lbm_cg_create(C.byref(p), m.reshape(-1), np.ascontiguousarray(psi, dtype=np.float64).reshape(-1),
-                                   nx, ny, nz, C.byref(h)))
+        _check(lib().lbm_cg_create_bc(C.byref(p), C.byref(boundary) if boundary is not None else None, m.reshape(-1),
+                                      np.ascontiguousarray(psi, dtype=np.float64).reshape(-1), nx, ny, nz,
+                                      C.byref(h)))
         self._h = h
         c, ph, st, ms = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
         _check(lib().lbm_cg_info(h, C.byref(c), C.byref(ph), C.byref(st), C.byref(ms)))
@@ -483,6 +489,12 @@ class ColourGradient:
 
     def set_cap_a(self, cap_a):
         _check(lib().lbm_cg_set_cap_a(self._h, float(cap_a)))
+
+    def set_faces(self, rho, vel, active=True):
+        """Face densities and normal velocities (xp, xn, yp, yn, zp, zn) and
+        whether the face rules run; a change acts on the step just run."""
+        arr = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(6)
+        _check(lib().lbm_cg_set_faces(self._h, arr(rho), arr(vel), int(bool(active))))
 
     def set_window(self, window, restrict_nodes=True):
         """window = (xn, xp, yn, yp, zn, zp) inclusive, or None for the whole box."""

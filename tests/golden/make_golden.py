@@ -258,6 +258,39 @@ CG_RUNS = {
     "cg_outputs_ramp.npz": dict(L8="1.0e-5 2.0e-6 -1.0e-6", L26=3, L27=25, L28=0, L29=-1, L30=-1, L31=-1,
                                 L50="2 2", L51="40 1.0 1.0 8.0e-6", L52="90 1.0 1.0 3.0e-6",
                                 L53="120 1.0 1.0 5.0e-6"),
+    # pressure/velocity faces (boundary_pressure / boundary_velocity), one
+    # Sub_BC per run, no body force unless named:
+    # Sub_BC 1 pressure on both x faces with constant-phase x faces; the
+    # step-100 checkpoint also seeds a restart (cg_outputs_pre1_restart.npz)
+    "cg_outputs_pre1.npz": dict(L6=1, L7=1, L8="0.0 0.0 0.0", L9="1 1.0 1 1.004", L15="1 1", L35=1, L29=-1,
+                                L30=-1, L45=100),
+    # Sub_BC 2 (moments of the inner neighbour) on the y faces with a body
+    # force along x; stabiliser from step 30 holds force and faces back
+    "cg_outputs_pre2.npz": dict(L6=1, L8="5.0e-6 0.0 0.0", L10="1 1.0 1 1.003", L26=2, L35=2, L36="1 30",
+                                L29=-1, L30=-1, L31=-1),
+    # Sub_BC 0 (rest equilibrium) on the z faces, z the permeability direction
+    "cg_outputs_pre0.npz": dict(L6=1, L8="0.0 0.0 0.0", L11="1 1.0 1 1.002", L26=3, L35=0, L29=-1, L30=-1,
+                                L31=-1),
+    # Sub_BC 3 (non-equilibrium part of the -y neighbour) on the y faces
+    "cg_outputs_pre3.npz": dict(L6=1, L8="0.0 0.0 0.0", L10="1 1.0 1 1.002", L26=2, L35=3, L29=-1, L30=-1,
+                                L31=-1),
+    # Sub_BC 1 on the x faces with a pressure ramp along x through three
+    # points, reports every 25 steps
+    "cg_outputs_pre_ramp.npz": dict(L6=1, L8="0.0 0.0 0.0", L9="1 1.0 1 1.004", L35=1, L27=25, L29=-1, L30=-1,
+                                    L31=-1, L50="1 1", L51="40 1.0 1.006 0.0", L52="90 1.0 1.002 0.0",
+                                    L53="120 1.0 1.004 0.0"),
+    # Sub_BC 2 velocity (non-equilibrium bounce-back; the x flags act on the
+    # z faces) with in_BC off
+    "cg_outputs_vel2.npz": dict(L8="0.0 0.0 0.0", L12="1 0.002 1 0.002", L35=2, L29=-1, L30=-1, L31=-1),
+    # Sub_BC 1 velocity (equilibrium) on the y faces and Sub_BC 1 pressure on
+    # the x faces together
+    "cg_outputs_vel1.npz": dict(L6=1, L8="0.0 0.0 0.0", L9="1 1.0 1 1.002", L13="1 0.001 1 0.001", L35=1,
+                                L29=-1, L30=-1, L31=-1),
+    # Sub_BC 3 velocity (density of the inner neighbour) on the x faces
+    "cg_outputs_vel3.npz": dict(L8="0.0 0.0 0.0", L12="1 0.002 1 0.002", L35=3, L29=-1, L30=-1, L31=-1),
+    # capillary-pressure stepping with the face pressures along x (Sub_BC 1)
+    "cg_outputs_cap_pre.npz": dict(L4=250, L6=1, L8="0.0 0.0 0.0", L9="1 1.0 1 1.0", L35=1, L27=10, L28=0,
+                                   L29=-1, L30=-1, L31=-1, L58="1 1 30", L59="1.0 1.006 2e-5 3 2", L60="1e-2"),
 }
 
 
@@ -297,15 +330,19 @@ def save_cg(fname, mask, psi, input_txt, files):
     print(fname, sorted(files))
 
 
-def cg_program_outputs():
-    """Every file the colour-gradient program writes for the runs of CG_RUNS,
-    and a restart: the first run's step-100 checkpoint read back
+def cg_program_outputs(only=None):
+    """Every file the colour-gradient program writes for the runs of CG_RUNS
+    (those whose name contains `only`, when given), and two restarts: the
+    step-100 checkpoint of cg_outputs / cg_outputs_pre1 read back
     (mode_backup_ini = 100, prefix ./out_) and run for 60 more steps
-    (cg_outputs_restart.npz, files prefixed rst_)."""
+    (cg_outputs_restart.npz / cg_outputs_pre1_restart.npz, files prefixed
+    rst_)."""
     import tempfile
 
     mask, psi = cg_geometry()
     for fname, kv in CG_RUNS.items():
+        if only and only not in fname:
+            continue
         text = cg_input_text(**kv)
         with tempfile.TemporaryDirectory() as d:
             run_cg_program(d, text, mask, psi)
@@ -314,6 +351,11 @@ def cg_program_outputs():
                 rst = cg_input_text(L4=59, L27=20, L29=-1, L30=-1, L31=40, L34="./rst_", L45=0, L46=100)
                 run_cg_program(d, rst, mask, psi, ("./out_",))
                 save_cg("cg_outputs_restart.npz", mask, psi, rst, collect_cg(d, "rst_"))
+            if fname == "cg_outputs_pre1.npz":
+                rst = cg_input_text(**{**kv, "L4": 59, "L27": 20, "L31": 40, "L34": "./rst_", "L45": 0,
+                                       "L46": 100})
+                run_cg_program(d, rst, mask, psi, ("./out_",))
+                save_cg("cg_outputs_pre1_restart.npz", mask, psi, rst, collect_cg(d, "rst_"))
         save_cg(fname, mask, psi, text, files)
 
 
@@ -525,6 +567,7 @@ def main():
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
     ap.add_argument("--cg-outputs", action="store_true")
+    ap.add_argument("--only", default=None, help="--cg-outputs: runs whose fixture name contains this")
     ap.add_argument("--st7-outputs", action="store_true")
     a = ap.parse_args()
     oracle.build()
@@ -532,7 +575,7 @@ def main():
         st7_program_outputs()
         return
     if a.cg_outputs:
-        cg_program_outputs()
+        cg_program_outputs(a.only)
         return
     if a.cg:
         cg_small()

@@ -74,7 +74,8 @@ def test_phase_file_reads_as_float(L, tmp_path):
 
 
 @pytest.mark.parametrize("lines,field", [
-    (dict(L6=1), "in_BC"),
+    (dict(L9="2 1.0 0 1.0"), "pre_"),
+    (dict(L13="0 0.0 2 0.0"), "vel_"),
     (dict(L7=1, L15="2 0"), "psi_xp"),
     (dict(L7=1, L17="0 3"), "psi_xp"),
     (dict(L37=0.5), "ini_Sat"),

@@ -12,7 +12,12 @@ variants of INPUT_cg.dat on 14x12x10 spheres with a blob phase field:
                          x+ and y+;
   cg_outputs_cap.npz     capillary-pressure stepping of the body force along x;
   cg_outputs_restart.npz the first run's step-100 checkpoint read back and run
-                         60 more steps.
+                         60 more steps;
+  cg_outputs_pre*.npz,   pressure and velocity faces (boundary_pressure,
+  cg_outputs_vel*.npz    boundary_velocity) for every Sub_BC, with the
+                         stabiliser, a pressure ramp and capillary-pressure
+                         stepping of the face pressures, and a restart from
+                         the Sub_BC 1 run's step-100 checkpoint.
 The driver, run on the same inputs at FP64, must write the same files: text
 and VTK byte for byte except the wall-clock lines of Results.txt, the
 checkpoints bit for bit (rows 1..).
@@ -82,8 +87,13 @@ def compare(tmp_path, golden, prefix):
             assert path.read_bytes() == golden[name].tobytes(), name
 
 
+FACES = ["cg_outputs_pre1.npz", "cg_outputs_pre2.npz", "cg_outputs_pre0.npz", "cg_outputs_pre3.npz",
+         "cg_outputs_pre_ramp.npz", "cg_outputs_vel2.npz", "cg_outputs_vel1.npz", "cg_outputs_vel3.npz",
+         "cg_outputs_cap_pre.npz"]
+
+
 @pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_sched.npz", "cg_outputs_ramp.npz",
-                                     "cg_outputs_psi.npz", "cg_outputs_cap.npz"])
+                                     "cg_outputs_psi.npz", "cg_outputs_cap.npz"] + FACES)
 def test_cg_driver_writes_the_reference_files(L, fixture, tmp_path):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
@@ -91,18 +101,21 @@ def test_cg_driver_writes_the_reference_files(L, fixture, tmp_path):
     compare(tmp_path, golden, "out_")
 
 
-def test_cg_driver_restart_matches_the_reference_restart(L, tmp_path):
-    first = np.load(os.path.join(GOLDEN, "cg_outputs.npz"))
+@pytest.mark.parametrize("first_name,rst_name", [("cg_outputs.npz", "cg_outputs_restart.npz"),
+                                                 ("cg_outputs_pre1.npz", "cg_outputs_pre1_restart.npz")])
+def test_cg_driver_restart_matches_the_reference_restart(L, tmp_path, first_name, rst_name):
+    first = np.load(os.path.join(GOLDEN, first_name))
     prepare(tmp_path, first)
     run_driver(L, tmp_path)  # writes out_LBM_checkpoint_*_100
-    rst = np.load(os.path.join(GOLDEN, "cg_outputs_restart.npz"))
+    rst = np.load(os.path.join(GOLDEN, rst_name))
     prepare(tmp_path, rst)
     run_driver(L, tmp_path, "./out_")
     compare(tmp_path, rst, "rst_")
 
 
-def test_cg_driver_f32_reports_match(L, tmp_path):
-    golden = np.load(os.path.join(GOLDEN, "cg_outputs.npz"))
+@pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_pre1.npz"])
+def test_cg_driver_f32_reports_match(L, tmp_path, fixture):
+    golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
     run_driver(L, tmp_path, "./", "--precision", "f32")
     want = np.loadtxt(golden["Velocity_ave_max.txt"].tobytes().decode().splitlines())
