@@ -60,14 +60,31 @@ cudaError_t cg_phase_faces(bool f64, const int32_t* nodes, const double* psi0, i
 // act on the post-streaming populations F of the face nodes between
 // collision and comput_macro_variables, reading f, rho and u of the previous
 // macro step.  Both kernels work on full populations in double in the CG
-// direction order with CG3's feq (CG3:2503-2520), M (CG3:63-83), MI and LR.
+// direction order with CG3's feq (CG3:2503-2540), M (CG3:63-83), MI and LR.
 
-// feq (CG3:2503-2520) with lat_c = 1, in the reference's operation order.
+// feq of the colour-gradient program (CG3:2503-2540): the polynomial it
+// computes first is overwritten; the value returned is row k of M^-1 applied
+// to the equilibrium moments (rho, u, u u terms with rho_0 = 1), summed from
+// j = 0 in the reference's order.
 __device__ __forceinline__ double cg_feq(int k, double rho, double ux, double uy, double uz) {
-  const double c2 = 1.0, c4 = 1.0;
-  const double eu = (double)cg::ex(k) * ux + (double)cg::ey(k) * uy + (double)cg::ez(k) * uz;
-  const double uv = ux * ux + uy * uy + uz * uz;
-  return weight(k) * rho * (1.0 + 3.0 * eu / c2 + 4.5 * eu * eu / c4 - 1.5 * uv / c2);
+  const double rho_0 = 1.0;
+  double meq[kQ];
+#pragma unroll
+  for (int j = 0; j < kQ; j++) meq[j] = 0.0;
+  meq[0] = rho;
+  meq[3] = rho_0 * ux;
+  meq[5] = rho_0 * uy;
+  meq[7] = rho_0 * uz;
+  meq[1] = rho_0 * (ux * ux + uy * uy + uz * uz);
+  meq[9] = rho_0 * (2 * ux * ux - uy * uy - uz * uz);
+  meq[11] = rho_0 * (uy * uy - uz * uz);
+  meq[13] = rho_0 * ux * uy;
+  meq[14] = rho_0 * uy * uz;
+  meq[15] = rho_0 * ux * uz;
+  double feq = 0.0;
+#pragma unroll
+  for (int j = 0; j < kQ; j++) feq = feq + c_MIcg[k * kQ + j] * meq[j];
+  return feq;
 }
 
 __device__ __forceinline__ int cg_lr(int k) { return k == 0 ? 0 : ((k & 1) ? k + 1 : k - 1); }
