@@ -88,7 +88,7 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
 
     def __enter__(self):
         try:
@@ -103,7 +103,13 @@ class ClockSampler:
 
     def _read(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            self.lines.append((time.time(), ln.strip()))
+
+    def wait_first_sample(self, limit_s=5.0):
+        """Blocks until nvidia-smi has delivered a sample (at most limit_s)."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < limit_s:
+            time.sleep(0.02)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -113,10 +119,12 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
-        sm, smax, reasons = [], None, set()
+    def summary(self, window=None):
+        """Median SM clock and throttle reasons over every sample; with
+        window = (t0, t1), also how many samples fell inside it."""
+        sm, smax, reasons, inside = [], None, set(), 0
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for t, ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -125,11 +133,33 @@ class ClockSampler:
                 smax = float(parts[2])
             except ValueError:
                 continue
+            if window and window[0] <= t <= window[1]:
+                inside += 1
             for nm, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+               "reasons": sorted(reasons), "samples": len(sm)}
+        if window:
+            out["samples_in_timed_region"] = inside
+            out["span"] = "warm-up, timed steps and the e2e leg"
+        return out
+
+
+def _strict(x):
+    """JSON-safe copy: non-finite floats (the +-inf permeability of an axis
+    without force, k = Q nu / (V g) with g = 0) become null."""
+    if isinstance(x, float):
+        return x if x == x and abs(x) != float("inf") else None
+    if isinstance(x, dict):
+        return {k: _strict(v) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_strict(v) for v in x]
+    return x
+
+
+def emit(line):
+    print(json.dumps(_strict(line), allow_nan=False), flush=True)
 
 
 def dist_setup():
@@ -197,6 +227,38 @@ def reference_sample(mask, steps, warmup, procs=None, edge=64):
             "wall_s": wall}
 
 
+def _calib_worker(args):
+    sub, steps = args
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    import oracle
+
+    ref = oracle.ReferenceSP3(fast=True)
+    count = ref.create(sub, NU, (GX, 0.0, 0.0), binary=True)
+    ref.step(1)
+    t0 = time.perf_counter()
+    ref.step(steps)
+    return count, time.perf_counter() - t0
+
+
+def reference_calibration(mask, steps=2, edge=64):
+    """One reference process on the whole 256^3 geometry beside one process on
+    a 64^3 sub-block (the unit of the timed sample), each alone on the host,
+    same number of steps: shows whether the sub-blocks run faster per core
+    than the full domain (cache effects of the smaller arrays)."""
+    import multiprocessing as mp
+
+    sub = np.ascontiguousarray(mask[:edge, :edge, :edge])
+    ctx = mp.get_context("spawn")
+    out = {}
+    for name, m in (("sub_block_64", sub), ("full_domain_256", mask)):
+        with ctx.Pool(1) as pool:
+            count, t = pool.map(_calib_worker, [(m, steps)])[0]
+        out[name] = {"fluid_nodes": count, "steps": steps, "mlups_1core": count * steps / t / 1e6}
+    out["full_over_sub"] = out["full_domain_256"]["mlups_1core"] / out["sub_block_64"]["mlups_1core"]
+    return out
+
+
 def run_reference(a):
     world, rank, local, pg = dist_setup()
     if rank != 0:
@@ -215,7 +277,7 @@ def run_reference(a):
                        "sample": cb["sample"]},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
@@ -241,10 +303,16 @@ def run_ours(a):
     count = s.count
     mem, tinfo = s.memory(), s.table_info()
     bytes_per_lu = mem["bytes_per_lu"]  # populations + the table form the step reads
+    # the sampler runs from before the warm-up to the end of the e2e leg: a
+    # short timed region (the driver's 20 steps take 4 ms) sees no sample of
+    # its own, the steps around it do
+    clk = ClockSampler(local).__enter__()
+    clk.wait_first_sample()
     s.step(a.warmup)
     barrier(pg)
-    with ClockSampler(local) as clk:
-        s.step(a.steps)  # lbm_step times the K steps with CUDA events on its stream
+    t_timed0 = time.time()
+    s.step(a.steps)  # lbm_step times the K steps with CUDA events on its stream
+    t_timed1 = time.time()
     ms = s.last_step_ms()
     diag = s.reduce()
     s.close()
@@ -268,11 +336,13 @@ def run_ours(a):
         left -= k
     rho, u = e.fields()
     t_e2e = time.perf_counter() - t0
-    npad = ((count + 255) // 256) * 256
     e.close()
+    clk.__exit__(None, None, None)
     t_e2e = allmax(pg, t_e2e)
     e2e_value = world * count * a.steps / t_e2e / 1e6
-    h2d = 18 * npad * 4 + count * 4  # pull table + node order
+    # in reference order lbm_create uploads the mask (one byte per cell) and
+    # builds the compaction and the pull table on the device
+    h2d = mask.size
     d2h = reads * 64 + rho.nbytes + u.nbytes
 
     if rank != 0:
@@ -293,18 +363,24 @@ def run_ours(a):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "bytes_per_lu": bytes_per_lu},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d / a.steps,
-                "d2h_bytes_per_step": d2h / a.steps, "wall_s": t_e2e},
+                "d2h_bytes_per_step": d2h / a.steps, "wall_s": t_e2e,
+                "what": "lbm_create from the host mask (upload of nx*ny*nz bytes; compaction and pull table built "
+                        "on the device), K steps with an lbm_reduce read-back every 100, lbm_get_fields of rho and "
+                        "u (doubles, reference id order); at small K the creation and the field read-back "
+                        "dominate the wall time"},
         "gpu_launches": a.steps,
-        "clocks": clk.summary(),
+        "clocks": clk.summary(window=(t_timed0, t_timed1)),
         "perm_x": diag["perm"][0],
     }
     if world == 1 and not a.no_cpu_baseline:
         try:
             cb = reference_sample(mask, steps=a.cpu_steps, warmup=1)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            if not a.no_cpu_calibration:
+                line["cpu_baseline"]["calibration"] = reference_calibration(mask, steps=a.calib_steps)
         except Exception as ex:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unavailable": str(ex)[:200]}
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
@@ -326,6 +402,7 @@ def run_batch(a):
     mine = shard(inst_all, world, rank, lambda x: float((x[0] == 0).sum()))
     inst = [inst_all[i] for i in mine]
     tol, every, cap = 1e-6, 100, 400000
+    clk = ClockSampler(local).__enter__()
     fixed = a.batch_block > 0
     with lbm_b200.Batch(inst, precision="f32", ordering="reference" if fixed else "auto",
                         block=a.batch_block if fixed else 0, device=local) as b:
@@ -343,6 +420,17 @@ def run_batch(a):
             d = s.run_to_convergence(tol=tol, check_every=every, max_steps=cap)
             t_single += time.perf_counter() - t0
             singles.append(d)
+    # FP64 check of a seeded sample of the instances: the bit-exact FP64
+    # kernel run to the same stop test is the reference's permeability
+    rng = np.random.default_rng(11)
+    sample = sorted(rng.choice(len(inst), size=min(a.fp64_sample, len(inst)), replace=False).tolist())
+    errs = []
+    for i in sample:
+        mask, nu, g = inst[i]
+        with lbm_b200.SinglePhase(mask, nu, g, precision="f64", device=local) as s:
+            d = s.run_to_convergence(tol=tol, check_every=every, max_steps=cap)
+        errs.append(abs(res[i]["perm"][0] - d["perm"][0]) / abs(d["perm"][0]))
+    clk.__exit__(None, None, None)
     t_batch = allmax(pg, t_batch)
     t_single = allmax(pg, t_single)
     if rank != 0:
@@ -357,8 +445,11 @@ def run_batch(a):
             "batched_wall_s": t_batch, "speedup_vs_one_at_a_time": t_single / t_batch,
             "fluid_nodes": info["total_nodes"], "node_steps": info["node_steps"],
             "mlups_batched": info["node_steps"] / t_batch / 1e6,
-            "converged": sum(r["status"] == 0 for r in res), "max_rel_perm_diff_vs_one_at_a_time": dk}
-    print(json.dumps(line))
+            "converged": sum(r["status"] == 0 for r in res), "max_rel_perm_diff_vs_one_at_a_time": dk,
+            "fp64_check": {"sample": sample, "max_rel_perm_err": max(errs) if errs else None,
+                           "anchor": "bit-exact FP64 kernel, same stop test"},
+            "clocks": clk.summary()}
+    emit(line)
     return 0
 
 
@@ -373,6 +464,7 @@ def run_serve(a):
     mine = [i for i in range(len(reqs_all)) if i % world == rank]
     reqs = [reqs_all[i] for i in mine]
     tol, every = 1e-6, 100
+    clk = ClockSampler(local).__enter__()
     lat, results, ids = [], {}, {}
     with lbm_b200.Server(capacity_nodes=a.pool_nodes, max_active=64, precision="f32", tol=tol, check_every=every,
                          max_steps=400000, device=local, target_active_nodes=a.target_nodes,
@@ -418,6 +510,7 @@ def run_serve(a):
         with lbm_b200.SinglePhase(mask, nu, g, precision="f64", device=local) as s:
             d = s.run_to_convergence(tol=tol, check_every=every, max_steps=400000)
         errs.append(abs(results[i]["perm"][0] - d["perm"][0]) / abs(d["perm"][0]))
+    clk.__exit__(None, None, None)
     if rank != 0:
         return 0
     lat = np.array(lat)
@@ -433,8 +526,56 @@ def run_serve(a):
                                    "p50": float(np.percentile(fifo_lat, 50)),
                                    "p99": float(np.percentile(fifo_lat, 99)),
                                    "gpu_busy_s": float(sum(solo))},
-            "fp64_check": {"sample": len(sample), "max_rel_perm_err": max(errs) if errs else None}}
-    print(json.dumps(line))
+            "fp64_check": {"sample": sample, "max_rel_perm_err": max(errs) if errs else None,
+                           "anchor": "bit-exact FP64 kernel, same stop test"},
+            "clocks": clk.summary()}
+    emit(line)
+    return 0
+
+
+def run_cfg2_accuracy(a):
+    """The 256^3 workload run to its stop test (relative change of u_ave over
+    100 steps below 1e-6, SP:812-816 with the configuration's tolerance) in
+    each requested storage kind; the bit-exact FP64 kernel (identical to the
+    reference's FP64 arithmetic, pinned against the compiled reference) is the
+    anchor.  Reports the permeability error (Comput_Perm, SP3:3518-3650) and
+    the velocity error max|u - u_64| / max|u_64| of each kind against it."""
+    world, rank, local, pg = dist_setup()
+    import lbm_b200
+
+    mask = workload_mask()
+    tol, every = 1e-6, 100
+    out = {}
+    with ClockSampler(local) as clk:
+        for prec in [p.strip() for p in a.precisions.split(",") if p.strip()]:
+            t0 = time.perf_counter()
+            with lbm_b200.SinglePhase(mask, NU, (GX, 0, 0), precision=prec, device=local) as s:
+                d = s.run_to_convergence(tol=tol, check_every=every, max_steps=a.max_steps)
+                wall = time.perf_counter() - t0
+                rho, u = s.fields()
+                out[prec] = {"diag": d, "u": u[1:], "count": s.count, "wall_s": wall}
+    if rank != 0:
+        return 0
+    anchor = out.get("f64")
+    res = {}
+    for prec, r in out.items():
+        d = r["diag"]
+        e = {"stop_step": d["step"], "converged": d["converged"] == 1, "status": d["status"],
+             "perm": d["perm"], "u_ave": d["u_ave"], "wall_s": r["wall_s"],
+             "fluid_mlups_wall": r["count"] * d["step"] / r["wall_s"] / 1e6}
+        if anchor is not None and prec != "f64":
+            k64 = anchor["diag"]["perm"]
+            e["perm_err_vs_fp64"] = [abs(x - y) / abs(y) if y else None for x, y in zip(d["perm"], k64)]
+            e["u_err_vs_fp64"] = float(np.abs(r["u"] - anchor["u"]).max() / np.abs(anchor["u"]).max())
+            e["u_ave_err_vs_fp64"] = abs(d["u_ave"] - anchor["diag"]["u_ave"]) / abs(anchor["diag"]["u_ave"])
+            e["stop_step_minus_fp64"] = d["step"] - anchor["diag"]["step"]
+        res[prec] = e
+    line = {"metric": "permeability error vs FP64 at the stop test", "workload": "cfg2-accuracy",
+            "config": {"workload": "256^3 overlapping spheres r=U[4,10], phi=0.35, seed 20260101, tau=0.8, gx=1e-6; "
+                                   "stop when |du_ave/u_ave| < 1e-6 over 100 steps", "fluid_nodes": out[next(iter(out))]["count"]},
+            "anchor": "f64 = the bit-exact FP64 kernel" if anchor is not None else None,
+            "results": res, "clocks": clk.summary(), "data": "synthetic", "n_gpus": world}
+    emit(line)
     return 0
 
 
@@ -451,12 +592,14 @@ def run_cg(a):
               flux_psi=0.99, flux_umax=0.01)
     steps = a.cg_steps
     out = {}
+    clk = ClockSampler(local).__enter__()
     for prec in ("f32", "f64"):
         with lbm_b200.ColourGradient(mask, psi, precision=prec, device=local, **kw) as s:
             s.step(20)
             s.step(steps - 20)
             ms = s.last_step_ms()
             out[prec] = (s.reduce(), ms / (steps - 20), s.count)
+    clk.__exit__(None, None, None)
     if rank != 0:
         return 0
     (d32, ms32, n), (d64, ms64, _) = out["f32"], out["f64"]
@@ -479,7 +622,7 @@ def run_cg(a):
             "rel_err_vs_fp64": {"saturation": abs(d32["saturation"] - d64["saturation"]) / d64["saturation"],
                                 "q_l": abs(d32["q_l"][0] - d64["q_l"][0]) / (abs(d64["q_l"][0]) + 1e-300),
                                 "q_g": abs(d32["q_g"][0] - d64["q_g"][0]) / (abs(d64["q_g"][0]) + 1e-300)}}
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
@@ -517,15 +660,16 @@ def run_solute(a):
                          "bytes_per_lu": b32},
             "fp64": {"mlups": n / (ms64 * 1e-3) / 1e6, "gbs": n * b64 / (ms64 * 1e-3) / 1e9, "bytes_per_lu": b64},
             "mass_rel_diff_f32_vs_f64": abs(m32 - m64) / abs(m64)}
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cg-steps", type=int, default=20000)
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "batch", "serve", "cg", "solute"],
-                    help="cfg2 = the headline single-domain bench; batch / serve = configs 4 / 5")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg2-accuracy", "batch", "serve", "cg", "solute"],
+                    help="cfg2 = the headline single-domain bench; cfg2-accuracy = its FP32 error against the "
+                         "bit-exact FP64 kernel at the stop test; batch / serve = configs 4 / 5")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--instances", type=int, default=64, help="batch: number of config-4 solves")
     ap.add_argument("--batch-block", type=int, default=0, help="batch: fixed block size, reference order (0 = autotune)")
@@ -541,6 +685,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-calibration", action="store_true",
+                    help="skip the one-process full-domain vs sub-block reference timing")
+    ap.add_argument("--calib-steps", type=int, default=2)
+    ap.add_argument("--precisions", default="f32,f64",
+                    help="cfg2-accuracy: storage kinds run to the stop test (f64 = the bit-exact kernel, the anchor)")
+    ap.add_argument("--max-steps", type=int, default=200000, help="cfg2-accuracy: step cap of each solve")
     ap.add_argument("--ordering", default="reference", choices=["auto", "reference", "morton", "hilbert", "brick"],
                     help="node order of the timed solve; auto = lbm_autotune (short trials at burst clocks)")
     ap.add_argument("--block", type=int, default=256)
@@ -556,6 +706,8 @@ def main():
         return run_serve(a)
     if a.workload == "cg":
         return run_cg(a)
+    if a.workload == "cfg2-accuracy":
+        return run_cfg2_accuracy(a)
     if a.workload == "solute":
         return run_solute(a)
     return run_ours(a)
