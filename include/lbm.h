@@ -187,8 +187,9 @@ LBM_API lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, 
                       lbm_handle** out);
 
 /* Reads INPUT.dat and its geometry file and creates the solver (main SP3:258-555
- * at one rank).  Unsupported INPUT features (pressure/velocity boundaries,
- * non-Newtonian module) return LBM_ERR_ARG. */
+ * at one rank), pressure/velocity faces (pre_*, vel_*, Sub_BC) included.  The
+ * INPUT features that remain unsupported -- the non-Newtonian module and a
+ * self-defined lattice velocity (lattice_v != 0) -- return LBM_ERR_ARG. */
 LBM_API lbm_status lbm_create_from_input(const char* input_path, int precision, int ordering,
                                  lbm_handle** out, lbm_input* parsed_out);
 
@@ -631,6 +632,12 @@ LBM_API lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* orderi
  * over instances in that run. */
 LBM_API lbm_status lbm_batch_info(lbm_batch* b, long long* total_nodes, double* last_run_ms,
                                   long long* node_steps);
+/* No counterpart in the reference (it solves one domain per program run).
+ * Per-chain record of the last lbm_batch_run: rows of three doubles --
+ * fluid nodes of the instances stepping when the chain started, steps in the
+ * chain, device time of the chain in ms (list, steps and per-instance stop
+ * test).  Writes min(rows, max_rows) rows; *n_rows = rows recorded. */
+LBM_API lbm_status lbm_batch_trace(lbm_batch* b, double* out, int max_rows, int* n_rows);
 LBM_API void lbm_batch_destroy(lbm_batch* b);
 
 /* ---------------------------------------- continuous-batching solve server */
@@ -698,9 +705,11 @@ LBM_API void lbm_server_destroy(lbm_server* s);
  * Its scratch (one row of partial sums per 2048-node tile) is a static
  * device array of 512 KiB that every GPU loading the library holds until the
  * process exits, so n is limited to 16,777,216 nodes; larger n is rejected
- * with LBM_ERR_ARG.  The first call on a device looks up the array's device
- * address (and loads the library's kernels there); make that first call
- * before any stream capture.  All calls share the one array and every call
+ * with LBM_ERR_ARG.  Every call looks up the array's device address on the
+ * current device (cudaGetSymbolAddress allocates nothing), so the address
+ * stays valid after a cudaDeviceReset; the first call on a device also loads
+ * the library's kernels there, so make that first call before any stream
+ * capture.  All calls share the one array and every call
  * overwrites it: calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialised by the caller. */
 LBM_API lbm_status lbm_reduce_noalloc(const double* f_dev, const double* u_prev_dev, int n, int stride,

@@ -24,10 +24,11 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-INCLUDES = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+GEN = os.path.join(BUILD, "gen")  # generated headers (mi_pattern.h)
+INCLUDES = ["-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", GEN]
 
-# (source, extra nvcc flags).  sp_faithful.cu must not contract a*b+c into FMA:
-# it reproduces the reference's FP64 arithmetic bit for bit.
+# (source, extra nvcc flags).  The *_faithful.cu files must not contract a*b+c
+# into FMA: they reproduce the reference's FP64 arithmetic bit for bit.
 CUDA_SOURCES = [
     ("sp_kernels.cu", []),
     ("sp_faithful.cu", ["-fmad=false"]),
@@ -36,7 +37,8 @@ CUDA_SOURCES = [
     ("setup_kernels.cu", []),
     ("cg_faithful.cu", ["-fmad=false"]),
     ("cg_fast.cu", []),
-    ("st7_kernels.cu", ["-fmad=false"]),
+    ("st7_kernels.cu", []),
+    ("st7_faithful.cu", ["-fmad=false"]),
     ("box_sums.cu", []),
 ]
 CXX_SOURCES = ["api.cpp", "geometry.cpp", "mrt.cpp", "io.cpp", "batch.cpp", "cg_api.cpp", "st7_api.cpp", "output.cpp", "transfer.cpp"]
@@ -49,6 +51,26 @@ def _headers():
     hs = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     hs += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     return hs
+
+
+def _generate(headers, verbose, force):
+    """Writes _build/gen/mi_pattern.h (the zero / power-of-two pattern of the
+    Gauss-Jordan M^-1, gen_mi_pattern.cpp) when its inputs changed."""
+    os.makedirs(GEN, exist_ok=True)
+    hdr = os.path.join(GEN, "mi_pattern.h")
+    srcs = [os.path.join(CSRC, "gen_mi_pattern.cpp"), os.path.join(CSRC, "mrt.cpp")]
+    if not force and os.path.exists(hdr) and \
+            all(os.path.getmtime(hdr) >= os.path.getmtime(x) for x in srcs + headers):
+        return hdr
+    exe = os.path.join(BUILD, "gen_mi_pattern")
+    _run([CXX, "-O2", "-std=c++17", "-I", os.path.join(CUDA, "include"), *INCLUDES, *srcs, "-o", exe], verbose)
+    text = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    if not os.path.exists(hdr) or open(hdr).read() != text:
+        with open(hdr, "w") as fh:
+            fh.write(text)
+    else:
+        os.utime(hdr)
+    return hdr
 
 
 def _stale(obj, src, headers):
@@ -70,6 +92,7 @@ def _run(cmd, verbose):
 def build(verbose=False, ptxas_info=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
+    headers.append(_generate(headers, verbose, force))
     sources = [os.path.join(CSRC, s) for s, _ in CUDA_SOURCES] + [os.path.join(CSRC, s) for s in CXX_SOURCES]
     exes = [os.path.join(BIN, name) for _, name in EXECUTABLES]
     sources += [os.path.join(CSRC, s) for s, _ in EXECUTABLES]

@@ -11,8 +11,6 @@
 //
 // Compiled with -fmad=false, like the bit-exact FP64 kernel, so the macro
 // step and the per-node sums are the same operations as lbm_reduce's.
-#include <mutex>
-
 #include "kernels_common.cuh"
 
 namespace lbm {
@@ -23,15 +21,11 @@ constexpr int kTileThreads = 256;
 constexpr int kNodesPerThread = 8;
 constexpr int kTileNodes = kTileThreads * kNodesPerThread;  // 2048 nodes per tile
 constexpr int kMaxTiles = 8192;                             // 16,777,216 nodes
-constexpr int kMaxDevices = 64;
 
 // One row of 8 partial sums per tile.  Every launch writes the rows of all the
 // tiles it uses before the final pass reads them, so nothing has to start at
 // zero; the contents left by the previous call are simply overwritten.
 static __device__ __align__(256) double g_tile_partials[kMaxTiles * 8];
-
-std::mutex g_scratch_mu;
-double* g_scratch[kMaxDevices] = {};
 
 __global__ void __launch_bounds__(kTileThreads)
     tile_reduce_kernel(const double* __restrict__ f, const double* __restrict__ u_prev, int n, int stride,
@@ -79,24 +73,21 @@ __global__ void __launch_bounds__(1024)
   block_reduce8(acc, result, smem);
 }
 
-// Device address of the scratch array on the current device.  The first call
-// on a device looks it up (cudaGetSymbolAddress, which also loads this
-// library's kernels onto that device); later calls reuse the address.  In host
-// code the array's name is only a host-side stand-in, never a device address.
+// Device address of the scratch array on the current device.  In host code the
+// array's name is only a host-side stand-in, never a device address, so every
+// call looks the address up on the device that is current (the first lookup on
+// a device also loads this library's kernels there).  The lookup allocates
+// nothing and is cheap once the module is loaded; not caching it keeps the
+// address valid after cudaDeviceReset recreates the device's context.
 lbm_status scratch_address(double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(LBM_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return fail(LBM_ERR_ARG, "device ordinal beyond the scratch table");
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_tile_partials);
-    if (e != cudaSuccess)
-      return fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_scratch[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch[dev];
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_tile_partials);
+  if (e != cudaSuccess)
+    return fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
   return LBM_OK;
 }
 

@@ -17,6 +17,7 @@ struct St7Args {
 };
 
 cudaError_t st7_launch_step(bool f64, const St7Args& a, cudaStream_t st);
+cudaError_t st7_launch_step_f64(const St7Args& a, cudaStream_t st);  // st7_faithful.cu, -fmad=false
 cudaError_t st7_launch_conc(bool f64, const St7Args& a, double* out, cudaStream_t st);
 cudaError_t st7_launch_init(bool f64, const St7Args& a, cudaStream_t st);
 // a.src: the state to export; a.dst: the buffer the next step pulls from

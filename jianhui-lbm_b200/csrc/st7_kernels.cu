@@ -9,44 +9,15 @@
 // which are also directions 1..6 of the D3Q19 pull table), pulled through
 // those six table rows: a table entry q'*npad + m of a D3Q7 direction has
 // q' in 1..6, so the row-6 storage index is entry - npad.  One thread per
-// node; 2*6*s + 6*4 + 3*s bytes per update.  Compiled with -fmad=false so
-// the FP64 variant keeps the reference's arithmetic.
-#include "st7_api.h"
+// node; 2*6*s + 6*4 + 3*s bytes per update.  The step kernel lives in
+// st7_kernels.cuh; its FP64 instantiation is built in st7_faithful.cu with
+// -fmad=false (the reference's unfused arithmetic), this file keeps FMA
+// contraction for the FP32 path.
+#include "st7_kernels.cuh"
 
 namespace lbm {
 
 namespace {
-
-template <typename T, bool GIVEN>
-__global__ void __launch_bounds__(256) st7_step_kernel(St7Args a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= a.n) return;
-  const T* __restrict__ src = static_cast<const T*>(a.src);
-  T* __restrict__ dst = static_cast<T*>(a.dst);
-  const T* __restrict__ u = static_cast<const T*>(a.u);
-  const size_t npad = (size_t)a.npad;
-  T g[7];
-  g[0] = T(0);
-#pragma unroll
-  for (int q = 1; q < 7; q++) g[q] = __ldg(src + (__ldg(a.table + (size_t)(q - 1) * npad + x) - npad));
-  T C;
-  if (GIVEN) {
-    C = static_cast<const T*>(a.c_given)[x];
-  } else {
-    C = T(0);
-#pragma unroll
-    for (int q = 1; q < 7; q++) C = C + g[q];
-  }
-  if (a.c_out) static_cast<T*>(a.c_out)[x] = C;
-  const T ux = u[x], uy = u[npad + x], uz = u[2 * npad + x];
-  const T tau = T(a.tau_s);
-#pragma unroll
-  for (int q = 1; q < 7; q++) {
-    const T eu = T(cx(q)) * ux + T(cy(q)) * uy + T(cz(q)) * uz;
-    const T nv = g[q] - (g[q] - T(1.0 / 6.0) * C * (T(1) + T(3) * eu)) / tau;
-    dst[(size_t)(q - 1) * npad + x] = nv;
-  }
-}
 
 // C of every node from the pulled g (the macro step), internal order.
 template <typename T>
@@ -132,21 +103,7 @@ cudaError_t st7_launch_import(bool f64, const St7Args& a, const int32_t* ref_of,
 }
 
 cudaError_t st7_launch_step(bool f64, const St7Args& a, cudaStream_t st) {
-  if (a.n == 0) return cudaSuccess;
-  const int g = (a.n + 255) / 256;
-  const bool given = a.c_given != nullptr;
-  if (f64) {
-    if (given)
-      st7_step_kernel<double, true><<<g, 256, 0, st>>>(a);
-    else
-      st7_step_kernel<double, false><<<g, 256, 0, st>>>(a);
-  } else {
-    if (given)
-      st7_step_kernel<float, true><<<g, 256, 0, st>>>(a);
-    else
-      st7_step_kernel<float, false><<<g, 256, 0, st>>>(a);
-  }
-  return cudaGetLastError();
+  return f64 ? st7_launch_step_f64(a, st) : st7_detail::launch_step<float>(a, st);
 }
 
 cudaError_t st7_launch_conc(bool f64, const St7Args& a, double* out, cudaStream_t st) {

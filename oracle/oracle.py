@@ -24,8 +24,10 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# where the fixture generators read the reference's own sample files
-REFERENCE_ROOT = os.environ.get("LBM_REFERENCE_ROOT", "/root/reference")
+# where the fixture generators read the reference's own sample files: the
+# reference project's checkout, LBM_REFERENCE_ROOT when set, else a directory
+# named "reference" beside this repository's own directory
+REFERENCE_ROOT = os.environ.get("LBM_REFERENCE_ROOT") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 _I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _U8P = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")

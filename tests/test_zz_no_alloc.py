@@ -42,15 +42,26 @@ def diag_from_sums(r, nx, ny, nz, porosity):
     return out
 
 
-def call_noalloc(L, f_ref_layout, u_prev_ref_layout, count):
+def call_noalloc(L, f_ref_layout, u_prev_ref_layout, count, pad=0):
+    """Caller-owned device arrays in the documented layout, f[q][p] and
+    u_prev[d][p] with rows of count + pad entries; the padding holds NaN, so
+    a kernel that read it would poison every sum.  u_prev_ref_layout None
+    passes NULL."""
     import torch
 
-    # caller-owned device arrays in the documented layout: f[q][p], u_prev[d][p]
-    f_dev = torch.tensor(np.ascontiguousarray(f_ref_layout[1:].T), dtype=torch.float64, device="cuda")
-    u_dev = torch.tensor(np.ascontiguousarray(u_prev_ref_layout[1:].T), dtype=torch.float64, device="cuda")
+    stride = count + pad
+
+    def rows(a):
+        host = np.full((a.shape[1], stride), np.nan)
+        host[:, :count] = a[1:].T
+        return torch.tensor(host, dtype=torch.float64, device="cuda")
+
+    f_dev = rows(f_ref_layout)
+    u_dev = rows(u_prev_ref_layout) if u_prev_ref_layout is not None else None
     out = torch.full((8,), float("nan"), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    st = L.lib().lbm_reduce_noalloc(C.c_void_p(f_dev.data_ptr()), C.c_void_p(u_dev.data_ptr()), count, count,
+    st = L.lib().lbm_reduce_noalloc(C.c_void_p(f_dev.data_ptr()),
+                                   C.c_void_p(u_dev.data_ptr()) if u_dev is not None else None, count, stride,
                                    count - 1, G[0], G[1], G[2], C.c_void_p(out.data_ptr()), C.c_void_p(stream))
     assert st == 0, L.lib().lbm_last_error()
     torch.cuda.synchronize()
@@ -84,6 +95,28 @@ def test_noalloc_matches_lbm_reduce_on_two_calls(L):
         # the same inputs twice give the same sums (scratch fully rewritten)
         r2 = call_noalloc(L, f, u_prev, s.count)
         assert np.array_equal(r2, results[1])
+
+
+def test_noalloc_padded_rows_and_null_previous_velocity(L):
+    """Rows longer than the node count (stride = n + 37, NaN in the padding)
+    give lbm_reduce's sums; without u_prev the change sum is exactly zero and
+    the other seven sums are unchanged."""
+    mask = spheres((26, 22, 30), 0.5, 3.0, seed=78)
+    nz, ny, nx = mask.shape
+    with L.SinglePhase(mask, NU, G, precision="f64") as s:
+        s.step(30)
+        _, u_prev = s.fields()
+        s.step(1)
+        f = s.populations()
+        d_old = s.reduce()
+        padded = call_noalloc(L, f, u_prev, s.count, pad=37)
+        compare(diag_from_sums(padded, nx, ny, nz, s.porosity), d_old)
+        tight = call_noalloc(L, f, u_prev, s.count)
+        no_prev = call_noalloc(L, f, None, s.count, pad=37)
+    assert np.isfinite(padded).all()
+    np.testing.assert_allclose(padded, tight, rtol=1e-13)
+    assert no_prev[0] == 0.0
+    np.testing.assert_allclose(no_prev[1:], padded[1:], rtol=1e-13)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(L):
