@@ -557,7 +557,11 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
   LBM_CUDA_TRY(cudaEventCreate(&h->ev1));
   h->mask.assign(mask, mask + (size_t)nx * ny * nz);
   if (!build_mrt_constants(p->nu, &h->mrt)) return fail(LBM_ERR_ARG, "moment matrix inversion failed");
-  if (h->kind == Store::F64) LBM_CUDA_TRY(set_mi_constant(&h->mrt.MI[0][0], h->stream));
+  if (h->kind == Store::F64) {
+    if (!mi_pattern_matches(&h->mrt.MI[0][0]))
+      return fail(LBM_ERR_STATE, "M^-1 does not have the pattern the FP64 kernel was built for; rebuild the library");
+    LBM_CUDA_TRY(set_mi_constant(&h->mrt.MI[0][0], h->stream));
+  }
   if (h->kind == Store::F16) {
     double sc = p->fp16_scale;
     if (!(sc > 0)) {

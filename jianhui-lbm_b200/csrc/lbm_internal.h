@@ -286,6 +286,9 @@ cudaError_t launch_import_macro(Store kind, void* rho, void* u, const int32_t* r
 cudaError_t launch_export_macro(const double* rho_int, const double* u_int, const int32_t* ref_of, int n,
                                 int npad, double* rho_ref, double* u_ref, cudaStream_t st);
 cudaError_t set_mi_constant(const double* mi361, cudaStream_t st);
+// True when M^-1 has the zero / power-of-two pattern the bit-exact FP64
+// kernel was compiled for (mi_pattern.h, generated from mrt.cpp).
+bool mi_pattern_matches(const double* mi361);
 // uniform post-streaming state f_q = feq[q] at every node, written through
 // the inverse pull so the next step pulls exactly feq
 cudaError_t launch_init_uniform(Store kind, void* pop, const int32_t* table, int n, int npad, double fp16_scale,

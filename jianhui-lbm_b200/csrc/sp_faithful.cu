@@ -1,18 +1,37 @@
 // FP64 single-phase kernel that reproduces the reference collision bit for bit.
 //
-// This translation unit is compiled with -fmad=false: every a*b+c stays two
-// correctly rounded operations, as in the reference built without FMA
-// contraction, and every sum runs in the reference's index order.  The work
-// per node is the reference's own sequence (SP3:1423-1779):
+// This translation unit is compiled with -fmad=false: every a*b+c that is
+// written as such stays two correctly rounded operations, as in the reference
+// built without FMA contraction.  The work per node is the reference's own
+// arithmetic (SP3:1423-1779):
 //   Guo force per direction, f_eq per direction, then per moment k
 //   m_k = M_k . f, F_k = (1 - S_k/2) M_k . G, meq_k = M_k . f_eq,
 //   m*_k = m_k - S_k (m_k - meq_k) + dt F_k;   f*_q = MI_q . m*
-// with MI the Gauss-Jordan inverse the reference hard-codes.  Zero entries of
-// M are skipped (adding a +-0 product never changes a running sum); all 361
-// entries of MI are applied, so its round-off entries count as they do in the
-// reference.  Streaming is a pull through the table instead of the
-// reference's push through nei_loc, which moves values without arithmetic.
+// with MI the Gauss-Jordan inverse the reference hard-codes.  Every sum keeps
+// its terms and their order; what changes is only work whose result is
+// determined without it:
+//  * a term whose factor is exactly zero (a zero entry of M or MI, a zero
+//    velocity component e_a of a direction, a force component the kernel is
+//    specialised for being zero) adds +-0 to a sum and is left out -- it could
+//    only flip the sign of an intermediate zero, which no later +, -, * turns
+//    into a different non-zero value;
+//  * a product by a power-of-two coefficient of M or MI is exact, so product
+//    and sum are issued as one fma (one rounding, the same as the sum's);
+//  * values that the reference recomputes per direction and that are equal
+//    bit for bit (the Guo terms of opposite directions, the force terms of
+//    directions with the same e_x) are computed once;
+//  * the 19 moments of f are accumulated column by column while the pulled
+//    populations arrive: each row still adds its terms in ascending index
+//    order, so every m_k is the same chain of roundings, and the 19 pulled
+//    values are dead once the columns are done (the kernel holds 19 moment
+//    accumulators instead of f, f_eq and G at once);
+//  * the conserved moments (S_k = 0) keep m_k: m_k - 0 (m_k - meq_k) = m_k.
+// Streaming is a pull through the table instead of the reference's push
+// through nei_loc, which moves values without arithmetic.
+#include <utility>
+
 #include "bc_kernels.cuh"
+#include "mi_pattern.h"  // generated at build time from mrt.cpp's M^-1
 
 namespace lbm {
 
@@ -22,62 +41,275 @@ cudaError_t set_mi_constant(const double* mi361, cudaStream_t st) {
   return cudaMemcpyToSymbolAsync(c_MI, mi361, sizeof(double) * kQ * kQ, 0, cudaMemcpyHostToDevice, st);
 }
 
-__device__ __forceinline__ double srate(int k, double sv, double so) {
-  const bool conserved = (k == 0 || k == 3 || k == 5 || k == 7);
-  const bool viscous = (k == 1 || k == 2 || (k >= 9 && k <= 15));
-  return conserved ? 0.0 : (viscous ? sv : so);
+bool mi_pattern_matches(const double* mi361) {
+  for (int q = 0; q < kQ; q++)
+    for (int j = 0; j < kQ; j++) {
+      const double v = mi361[q * kQ + j];
+      int e;
+      const bool nz = v != 0.0, p2 = nz && std::fabs(std::frexp(v, &e)) == 0.5;
+      if (nz != (((mi_nonzero_row(q) >> j) & 1u) != 0) || p2 != (((mi_pow2_row(q) >> j) & 1u) != 0)) return false;
+    }
+  return true;
 }
 
-// Collision of one node in the reference's operation order; writes the 19
-// post-collision populations of node p.
-__device__ __forceinline__ void collide_faithful(const double (&f)[kQ], double rho, double ux, double uy, double uz,
-                                                 const StepArgs& a, int p) {
-  double* __restrict__ dst = static_cast<double*>(a.dst_pop);
-  const double c_s2 = 1.0 * 1.0 / 3;
-  const double gx = a.gx, gy = a.gy, gz = a.gz;
-  double guo[kQ], feq[kQ];
-#pragma unroll
-  for (int q = 0; q < kQ; q++) {
-    const double ex = cx(q), ey = cy(q), ez = cz(q);
-    const double lm0 = ((ex - ux) * gx + (ey - uy) * gy + (ez - uz) * gz) / c_s2;
-    const double lm1 = (ex * ux + ey * uy + ez * uz) * (ex * gx + ey * gy + ez * gz) / (c_s2 * c_s2);
-    guo[q] = weight(q) * (lm0 + lm1);
-    const double eu = ex * ux + ey * uy + ez * uz;
-    const double uv = ux * ux + uy * uy + uz * uz;
-    feq[q] = weight(q) * rho * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv);
-  }
-  double ml[kQ];
-#pragma unroll
-  for (int k = 0; k < kQ; k++) {
-    double m = 0.0, fh = 0.0, me = 0.0;
-    bool first = true;
-#pragma unroll
-    for (int j = 0; j < kQ; j++) {
-      const int c = mcoef(k, j);
-      if (c == 0) continue;
-      if (first) {
-        m = (double)c * f[j];
-        fh = (double)c * guo[j];
-        me = (double)c * feq[j];
-        first = false;
-      } else {
-        m = m + (double)c * f[j];
-        fh = fh + (double)c * guo[j];
-        me = me + (double)c * feq[j];
-      }
-    }
-    const double S = srate(k, a.s_v, a.s_o);
-    fh *= (1 - 0.5 * S);
-    ml[k] = m - S * (m - me) + 1.0 * fh;
-  }
-#pragma unroll
-  for (int q = 0; q < kQ; q++) {
-    double s = c_MI[q * kQ] * ml[0];
-#pragma unroll
-    for (int j = 1; j < kQ; j++) s = s + c_MI[q * kQ + j] * ml[j];
-    dst[(size_t)q * a.npad + p] = s;
+namespace {
+
+__host__ __device__ constexpr int first_col(int k) {
+  for (int j = 0; j < kQ; j++)
+    if (mcoef(k, j) != 0) return j;
+  return kQ;
+}
+__host__ __device__ constexpr bool pow2_coef(int c) {
+  const int a = c < 0 ? -c : c;
+  return a > 1 && (a & (a - 1)) == 0;
+}
+__host__ __device__ constexpr bool macro_rows_are_moments() {
+  // rho = sum f and j = sum e f in the macro step are rows 0, 3, 5, 7 of M
+  for (int q = 0; q < kQ; q++)
+    if (mcoef(0, q) != 1 || mcoef(3, q) != cx(q) || mcoef(5, q) != cy(q) || mcoef(7, q) != cz(q)) return false;
+  return first_col(0) == 0;
+}
+static_assert(macro_rows_are_moments(), "moment rows 0, 3, 5, 7 must be rho, j_x, j_y, j_z");
+__host__ __device__ constexpr bool conserved_moment(int k) { return k == 0 || k == 3 || k == 5 || k == 7; }
+__host__ __device__ constexpr bool mi_nz(int q, int j) { return ((mi_nonzero_row(q) >> j) & 1u) != 0; }
+__host__ __device__ constexpr bool mi_p2(int q, int j) { return ((mi_pow2_row(q) >> j) & 1u) != 0; }
+__host__ __device__ constexpr bool mi_rows_start_at_zero() {
+  for (int q = 0; q < kQ; q++)
+    if (!mi_nz(q, 0) || mi_p2(q, 0)) return false;
+  return true;
+}
+static_assert(mi_rows_start_at_zero(), "every row of M^-1 starts with a non-zero, non-power-of-two entry");
+
+__device__ __forceinline__ double srate(int k, double sv, double so) {
+  const bool viscous = (k == 1 || k == 2 || (k >= 9 && k <= 15));
+  return viscous ? sv : so;
+}
+
+// Every structural choice below (which coefficient is zero, a power of two or
+// the first of its row; which direction leads its opposite pair) is a
+// template parameter decided with if constexpr, so the kernel holds only the
+// arithmetic that remains.
+using QSeq = std::make_integer_sequence<int, kQ>;
+
+// One term M_kj v of row k, added in ascending j.
+template <int K, int J>
+__device__ __forceinline__ void moment_term(double& acc, const double v) {
+  constexpr int c = mcoef(K, J);
+  if constexpr (c == 0) {
+    return;
+  } else if constexpr (J == first_col(K)) {
+    if constexpr (c == 1)
+      acc = v;
+    else if constexpr (c == -1)
+      acc = -v;
+    else
+      acc = (double)c * v;
+  } else if constexpr (c == 1) {
+    acc = acc + v;
+  } else if constexpr (c == -1) {
+    acc = acc - v;
+  } else if constexpr (pow2_coef(c)) {
+    acc = fma((double)c, v, acc);  // c*v is exact: one rounding, as c*v then +
+  } else {
+    acc = acc + (double)c * v;
   }
 }
+
+// Column J of the moment sums: acc_k (+)= M_kJ v for every row k.
+template <int J, int... K>
+__device__ __forceinline__ void moment_column_(double (&acc)[kQ], const double v, std::integer_sequence<int, K...>) {
+  (moment_term<K, J>(acc[K], v), ...);
+}
+template <int J>
+__device__ __forceinline__ void moment_column(double (&acc)[kQ], const double v) {
+  moment_column_<J>(acc, v, QSeq{});
+}
+template <int... J>
+__device__ __forceinline__ void moments_by_column(double (&acc)[kQ], const double (&f)[kQ],
+                                                  std::integer_sequence<int, J...>) {
+  (moment_column<J>(acc, f[J]), ...);
+}
+
+// Row K of the moment sums, M_K . v, terms in ascending index order.
+template <int K, int... J>
+__device__ __forceinline__ double moment_row_(const double (&v)[kQ], std::integer_sequence<int, J...>) {
+  double acc = 0.0;
+  (moment_term<K, J>(acc, v[J]), ...);
+  return acc;
+}
+template <int K>
+__device__ __forceinline__ double moment_row(const double (&v)[kQ]) {
+  return moment_row_<K>(v, QSeq{});
+}
+
+// e_Q . a over the non-zero components of e_Q, in the order x, y, z (the
+// reference's e[0]*a0 + e[1]*a1 + e[2]*a2 with its zero products left out).
+template <int Q>
+__device__ __forceinline__ double edot(double ax, double ay, double az) {
+  constexpr int x = cx(Q), y = cy(Q), z = cz(Q);
+  static_assert(x != 0 || y != 0 || z != 0, "edot of the rest direction");
+  double s;
+  if constexpr (x != 0) s = x > 0 ? ax : -ax;
+  if constexpr (y != 0) {
+    if constexpr (x == 0)
+      s = y > 0 ? ay : -ay;
+    else
+      s = y > 0 ? s + ay : s - ay;
+  }
+  if constexpr (z != 0) {
+    if constexpr (x == 0 && y == 0)
+      s = z > 0 ? az : -az;
+    else
+      s = z > 0 ? s + az : s - az;
+  }
+  return s;
+}
+
+// A direction of each opposite pair: the one whose first non-zero component
+// is positive.
+__host__ __device__ constexpr bool leads_pair(int q) {
+  return q != 0 && (cx(q) > 0 || (cx(q) == 0 && (cy(q) > 0 || (cy(q) == 0 && cz(q) > 0))));
+}
+
+// f_eq of feq() (SP3:1382-1391; lat_c = 1 so c2 = c4 = 1):
+// w rho (1 + 3 eu + 4.5 eu eu - 1.5 uv).  For the opposite direction eu is
+// exactly -eu, so 3 eu changes sign and 4.5 eu eu is the same value.
+template <int Q>
+__device__ __forceinline__ void equilibrium_pair(double rho, double ux, double uy, double uz, double t_uv,
+                                                 double (&feq)[kQ]) {
+  if constexpr (leads_pair(Q)) {
+    const double eu = edot<Q>(ux, uy, uz);
+    const double t3 = 3.0 * eu, t45 = 4.5 * eu * eu;
+    const double wr = weight(Q) * rho;
+    feq[Q] = wr * (1.0 + t3 + t45 - t_uv);
+    feq[opp(Q)] = wr * (1.0 - t3 + t45 - t_uv);
+  }
+}
+template <int... Q>
+__device__ __forceinline__ void equilibrium_(double rho, double ux, double uy, double uz, double (&feq)[kQ],
+                                             std::integer_sequence<int, Q...>) {
+  const double uv = ux * ux + uy * uy + uz * uz;
+  const double t_uv = 1.5 * uv;
+  feq[0] = weight(0) * rho * (1.0 - t_uv);
+  (equilibrium_pair<Q>(rho, ux, uy, uz, t_uv, feq), ...);
+}
+
+// Guo forcing GuoF[q] = w_q (lm0 + lm1) (SP3:1432-1510, c_l = lat_c = 1):
+//   lm0 = ((e_x - u_x) g_x + (e_y - u_y) g_y + (e_z - u_z) g_z) / c_s2
+//   lm1 = (e.u)(e.g) / (c_s2 c_s2)
+// (e.u)(e.g) is the same for q and its opposite (both factors change sign),
+// so lm1 is divided once per pair.  GX: g_y = g_z = 0, so lm0 depends on
+// e_x alone (three values) and lm1 vanishes for e_x = 0.
+constexpr double kCs2 = 1.0 * 1.0 / 3;
+constexpr double kCs4 = kCs2 * kCs2;
+
+template <int Q>
+__device__ __forceinline__ void guo_pair_x(double ux, double uy, double uz, double gx, double l0p, double l0z,
+                                           double l0m, double (&guo)[kQ]) {
+  if constexpr (Q == 0 || (!leads_pair(Q) && cx(Q) == 0)) {
+    // e_x = 0 (the rest direction included): lm1 = (e.u)(+-0) / c_s4 = +-0
+    guo[Q] = weight(Q) * l0z;
+  } else if constexpr (leads_pair(Q) && cx(Q) == 0) {
+    guo[Q] = weight(Q) * l0z;
+  } else if constexpr (leads_pair(Q)) {  // e_x = +1, its opposite e_x = -1
+    const double l1 = (edot<Q>(ux, uy, uz) * gx) / kCs4;
+    guo[Q] = weight(Q) * (l0p + l1);
+    guo[opp(Q)] = weight(Q) * (l0m + l1);
+  }
+}
+template <int Q>
+__device__ __forceinline__ void guo_pair_any(double ux, double uy, double uz, double gx, double gy, double gz,
+                                             const double (&tx)[3], const double (&ty)[3], const double (&tz)[3],
+                                             double (&guo)[kQ]) {
+  if constexpr (leads_pair(Q)) {
+    constexpr int o = opp(Q);
+    const double l1 = (edot<Q>(ux, uy, uz) * edot<Q>(gx, gy, gz)) / kCs4;
+    const double l0q = ((tx[cx(Q) + 1] + ty[cy(Q) + 1]) + tz[cz(Q) + 1]) / kCs2;
+    const double l0o = ((tx[cx(o) + 1] + ty[cy(o) + 1]) + tz[cz(o) + 1]) / kCs2;
+    guo[Q] = weight(Q) * (l0q + l1);
+    guo[o] = weight(Q) * (l0o + l1);
+  }
+}
+template <bool GX, int... Q>
+__device__ __forceinline__ void guo_force_(double ux, double uy, double uz, double gx, double gy, double gz,
+                                           double (&guo)[kQ], std::integer_sequence<int, Q...>) {
+  if constexpr (GX) {
+    const double l0p = ((1.0 - ux) * gx) / kCs2;
+    const double l0z = ((-ux) * gx) / kCs2;
+    const double l0m = ((-1.0 - ux) * gx) / kCs2;
+    (guo_pair_x<Q>(ux, uy, uz, gx, l0p, l0z, l0m, guo), ...);
+  } else {
+    const double tx[3] = {(-1.0 - ux) * gx, (-ux) * gx, (1.0 - ux) * gx};
+    const double ty[3] = {(-1.0 - uy) * gy, (-uy) * gy, (1.0 - uy) * gy};
+    const double tz[3] = {(-1.0 - uz) * gz, (-uz) * gz, (1.0 - uz) * gz};
+    guo[0] = weight(0) * (((tx[1] + ty[1]) + tz[1]) / kCs2);
+    (guo_pair_any<Q>(ux, uy, uz, gx, gy, gz, tx, ty, tz, guo), ...);
+  }
+}
+
+// Relaxation of moment K: the non-conserved moments relax towards meq; every
+// moment gets its forcing term (dt = 1).
+template <int K>
+__device__ __forceinline__ void relax_eq(double& m, const double (&feq)[kQ], double sv, double so) {
+  if constexpr (!conserved_moment(K)) {
+    const double S = srate(K, sv, so);
+    m = m - S * (m - moment_row<K>(feq));
+  }
+}
+template <int K>
+__device__ __forceinline__ void relax_force(double& m, const double (&guo)[kQ], double sv, double so) {
+  double fh = moment_row<K>(guo);
+  if constexpr (!conserved_moment(K)) fh *= (1 - 0.5 * srate(K, sv, so));
+  m = m + fh;
+}
+
+// Back-transform row Q: f*_Q = MI_Q . m, the non-zero entries in ascending j.
+template <int Q, int J>
+__device__ __forceinline__ void mi_term(double& s, const double (&m)[kQ]) {
+  if constexpr (J == 0) {
+    s = c_MI[Q * kQ] * m[0];
+  } else if constexpr (mi_nz(Q, J)) {
+    if constexpr (mi_p2(Q, J))
+      s = fma(c_MI[Q * kQ + J], m[J], s);  // exact product: one rounding
+    else
+      s = s + c_MI[Q * kQ + J] * m[J];
+  }
+}
+template <int Q, int... J>
+__device__ __forceinline__ double mi_row(const double (&m)[kQ], std::integer_sequence<int, J...>) {
+  double s;
+  (mi_term<Q, J>(s, m), ...);
+  return s;
+}
+
+template <bool GX, int... K>
+__device__ __forceinline__ void collide_moments_(double (&m)[kQ], double rho, double ux, double uy, double uz,
+                                                 const StepArgs& a, int p, std::integer_sequence<int, K...>) {
+  {
+    double feq[kQ];
+    equilibrium_(rho, ux, uy, uz, feq, QSeq{});
+    (relax_eq<K>(m[K], feq, a.s_v, a.s_o), ...);
+  }
+  {
+    double guo[kQ];
+    guo_force_<GX>(ux, uy, uz, a.gx, a.gy, a.gz, guo, QSeq{});
+    (relax_force<K>(m[K], guo, a.s_v, a.s_o), ...);
+  }
+  double* __restrict__ dst = static_cast<double*>(a.dst_pop) + p;
+  const size_t np = (size_t)a.npad;
+  ((dst[(size_t)K * np] = mi_row<K>(m, QSeq{})), ...);
+}
+
+// Relaxation in moment space and back-transform for one node whose moments
+// m = M f (accumulated by the caller) and macro values are known; writes the
+// 19 post-collision populations of node p.
+template <bool GX>
+__device__ __forceinline__ void collide_moments(double (&m)[kQ], double rho, double ux, double uy, double uz,
+                                                const StepArgs& a, int p) {
+  collide_moments_<GX>(m, rho, ux, uy, uz, a, p, QSeq{});
+}
+
+}  // namespace
 
 __device__ __forceinline__ void pull_f64(const StepArgs& a, int p, double (&f)[kQ]) {
   const double* __restrict__ src = static_cast<const double*>(a.src_pop);
@@ -107,16 +339,53 @@ __device__ __forceinline__ void macro_in_out(const StepArgs& a, int p, bool give
   }
 }
 
-template <int BS, bool GIVEN, bool WRITE>
-__global__ void __launch_bounds__(BS) step_f64_faithful(StepArgs a) {
+// Resident blocks per SM asked of the register allocator: 16 warps (128
+// registers, no spills) for 128-512 threads; 24 warps for 64-thread blocks
+// (80 registers with a few spills) -- the autotuner times both.
+constexpr int f64_min_blocks(int bs) { return bs == 64 ? 12 : 512 / bs; }
+
+// One node per thread.  The macro step of the reference (comput_macro_variables,
+// SP3:2414-2439) is rho = sum f and u = (j + g/2) / rho with the same sums as
+// moment rows 0, 3, 5, 7, so it reads them from the accumulated moments.
+template <int BS, bool GIVEN, bool WRITE, bool GX>
+__global__ void __launch_bounds__(BS, f64_min_blocks(BS)) step_f64_faithful(StepArgs a) {
   const int p = blockIdx.x * BS + threadIdx.x;
   if (p >= a.n_main) return;
-  double f[kQ];
-  pull_f64(a, p, f);
+  double m[kQ];
+  {
+    double f[kQ];
+    pull_f64(a, p, f);
+    moments_by_column(m, f, QSeq{});
+  }
   double rho, ux, uy, uz;
-  macro_in_out(a, p, GIVEN, WRITE, f, rho, ux, uy, uz);
-  if (a.snap_dst != nullptr && p >= a.snap_begin) snap_write(a.snap_dst, a.nsnap, p - a.snap_begin, f, rho, ux, uy, uz);
-  collide_faithful(f, rho, ux, uy, uz, a, p);
+  if (GIVEN) {
+    const double* r = static_cast<const double*>(a.rho_in);
+    const double* u = static_cast<const double*>(a.u_in);
+    rho = r[p];
+    ux = u[p];
+    uy = u[a.npad + p];
+    uz = u[2 * a.npad + p];
+  } else {
+    rho = m[0];
+    ux = (m[3] + a.gx / 2) / rho;
+    uy = (m[5] + a.gy / 2) / rho;
+    uz = (m[7] + a.gz / 2) / rho;
+  }
+  if (WRITE) {
+    static_cast<double*>(a.rho_out)[p] = rho;
+    double* u = static_cast<double*>(a.u_out);
+    u[p] = ux;
+    u[a.npad + p] = uy;
+    u[2 * a.npad + p] = uz;
+  }
+  if (a.snap_dst != nullptr && p >= a.snap_begin) {
+    // nodes read by a face rule record their pulled state (pulled again:
+    // the source array is read-only during the launch)
+    double f[kQ];
+    pull_f64(a, p, f);
+    snap_write(a.snap_dst, a.nsnap, p - a.snap_begin, f, rho, ux, uy, uz);
+  }
+  collide_moments<GX>(m, rho, ux, uy, uz, a, p);
 }
 
 // Face nodes: pull, the boundary rules, macro step, record, collision.  With
@@ -138,7 +407,9 @@ __global__ void __launch_bounds__(128) bc_f64_faithful(BcArgs a) {
   double rho, ux, uy, uz;
   macro_in_out(a.s, p, GIVEN, a.s.rho_out != nullptr, f, rho, ux, uy, uz);
   snap_write(a.s.snap_dst, a.s.nsnap, p - a.s.snap_begin, f, rho, ux, uy, uz);
-  collide_faithful(f, rho, ux, uy, uz, a.s, p);
+  double m[kQ];
+  moments_by_column(m, f, QSeq{});
+  collide_moments<false>(m, rho, ux, uy, uz, a.s, p);
 }
 
 cudaError_t launch_boundary_f64(const BcArgs& a, cudaStream_t st) {
@@ -165,28 +436,36 @@ __global__ void reduce_final_kernel(const double* __restrict__ partials, int nbl
   block_reduce8(acc, result, smem);
 }
 
-template <int BS>
+template <int BS, bool GX>
 static cudaError_t launch_f64_bs(const StepArgs& a, cudaStream_t st) {
   const int grid = (a.n_main + BS - 1) / BS;
   if (grid == 0) return cudaSuccess;
   const bool given = a.rho_in != nullptr, write = a.rho_out != nullptr;
   if (given && write)
-    step_f64_faithful<BS, true, true><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, true, true, GX><<<grid, BS, 0, st>>>(a);
   else if (given)
-    step_f64_faithful<BS, true, false><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, true, false, GX><<<grid, BS, 0, st>>>(a);
   else if (write)
-    step_f64_faithful<BS, false, true><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, false, true, GX><<<grid, BS, 0, st>>>(a);
   else
-    step_f64_faithful<BS, false, false><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, false, false, GX><<<grid, BS, 0, st>>>(a);
   return cudaGetLastError();
+}
+
+template <int BS>
+static cudaError_t launch_f64_force(const StepArgs& a, cudaStream_t st) {
+  // force along x only (every configuration of the benchmarks): the
+  // specialised Guo terms; any other force: the general ones
+  if (a.gy == 0.0 && a.gz == 0.0) return launch_f64_bs<BS, true>(a, st);
+  return launch_f64_bs<BS, false>(a, st);
 }
 
 cudaError_t launch_step_f64(const StepArgs& a, int block, cudaStream_t st) {
   switch (block) {
-    case 64: return launch_f64_bs<64>(a, st);
-    case 128: return launch_f64_bs<128>(a, st);
-    case 512: return launch_f64_bs<512>(a, st);
-    default: return launch_f64_bs<256>(a, st);
+    case 64: return launch_f64_force<64>(a, st);
+    case 128: return launch_f64_force<128>(a, st);
+    case 512: return launch_f64_force<512>(a, st);
+    default: return launch_f64_force<256>(a, st);
   }
 }
 

@@ -50,6 +50,26 @@ def test_fp64_bit_exact_vs_reference_fixture(L, order):
         np.testing.assert_allclose(d["perm"], [k0, k1, k2], rtol=1e-12)
 
 
+@pytest.mark.parametrize("g", [(1e-5, -2e-6, 3e-6), (0.0, 4e-6, 0.0), (-3e-6, 0.0, 0.0)])
+def test_fp64_bit_exact_any_force_direction(L, oracle_mod, g):
+    """The FP64 kernel has a specialisation for a force along x only and a
+    general one; both reproduce the FP64 restatement of the reference's
+    collision (itself pinned to the compiled reference) bit for bit, here
+    with solids, a force with every component, one along y (general path)
+    and a negative one along x (specialised path)."""
+    mask = spheres((22, 18, 20), 0.5, 3.0, seed=33)
+    ref = oracle_mod.SinglePhaseRun(mask, 0.1, g)
+    ref.step(60)
+    f_ref, u_ref, rho_ref = ref.fields()
+    for block in (64, 256):
+        with L.SinglePhase(mask, 0.1, g, precision="f64", ordering="morton", block_size=block) as s:
+            s.step(59)
+            s.step(1)
+            assert np.array_equal(s.populations(), f_ref), (g, block)
+            rho, u = s.fields()
+            assert np.array_equal(u, u_ref) and np.array_equal(rho, rho_ref)
+
+
 def test_fp64_bit_exact_24(L):
     gd = load_golden("sp_24.npz")
     with L.SinglePhase(gd["mask"], float(gd["nu"]), tuple(gd["g"]), precision="f64", ordering="hilbert") as s:
