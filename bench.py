@@ -621,7 +621,8 @@ def run_cg(a):
             "q_g_x": {"f32": d32["q_g"][0], "f64": d64["q_g"][0]},
             "rel_err_vs_fp64": {"saturation": abs(d32["saturation"] - d64["saturation"]) / d64["saturation"],
                                 "q_l": abs(d32["q_l"][0] - d64["q_l"][0]) / (abs(d64["q_l"][0]) + 1e-300),
-                                "q_g": abs(d32["q_g"][0] - d64["q_g"][0]) / (abs(d64["q_g"][0]) + 1e-300)}}
+                                "q_g": abs(d32["q_g"][0] - d64["q_g"][0]) / (abs(d64["q_g"][0]) + 1e-300)},
+            "clocks": clk.summary()}
     emit(line)
     return 0
 
@@ -638,6 +639,7 @@ def run_solute(a):
     c0 = rng.uniform(0.0, 1.0, mask.shape)
     steps = max(a.steps // 4, 50)
     out = {}
+    clk = ClockSampler(local).__enter__()
     with lbm_b200.SinglePhase(mask, NU, (GX, 0.0, 0.0), precision="f32", device=local) as flow:
         flow.step(300)
         for prec in ("f32", "f64"):
@@ -645,6 +647,7 @@ def run_solute(a):
                 s.step(a.warmup)
                 s.step(steps)
                 out[prec] = (s.last_step_ms() / steps, s.count, float(s.concentration()[1:].sum()))
+    clk.__exit__(None, None, None)
     if rank != 0:
         return 0
     peak, peak_src = measured_peak()
@@ -659,7 +662,7 @@ def run_solute(a):
                          "frac": n * b32 / (ms32 * 1e-3) / 1e9 / peak, "traffic": None, "peak_source": peak_src,
                          "bytes_per_lu": b32},
             "fp64": {"mlups": n / (ms64 * 1e-3) / 1e6, "gbs": n * b64 / (ms64 * 1e-3) / 1e9, "bytes_per_lu": b64},
-            "mass_rel_diff_f32_vs_f64": abs(m32 - m64) / abs(m64)}
+            "mass_rel_diff_f32_vs_f64": abs(m32 - m64) / abs(m64), "clocks": clk.summary()}
     emit(line)
     return 0
 

@@ -97,6 +97,15 @@ struct Pool {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, done_ev = nullptr;
+  cudaEvent_t chain_ev0 = nullptr, chain_ev1 = nullptr;  // device time of each chain
+  // one record per chain: stepping nodes when it was launched, its steps and
+  // its device time (the graph: list, steps, per-instance check)
+  struct ChainRecord {
+    long long stepping_nodes;
+    int steps;
+    float ms;
+  };
+  std::vector<ChainRecord> trace;
   int cap = 0, ntiles = 0, nslots = 0;
   int block = 256, grid = 0;
   int ordering = LBM_ORDER_REFERENCE;
@@ -121,7 +130,7 @@ struct Pool {
   ~Pool() {
     drop_graphs();
     if (h_state) cudaFreeHost(h_state);
-    for (cudaEvent_t e : {ev0, ev1, done_ev})
+    for (cudaEvent_t e : {ev0, ev1, done_ev, chain_ev0, chain_ev1})
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -162,6 +171,8 @@ struct Pool {
     LBM_CUDA_TRY(cudaEventCreate(&ev0));
     LBM_CUDA_TRY(cudaEventCreate(&ev1));
     LBM_CUDA_TRY(cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming));
+    LBM_CUDA_TRY(cudaEventCreate(&chain_ev0));
+    LBM_CUDA_TRY(cudaEventCreate(&chain_ev1));
     const size_t s = store_bytes(kind);
     for (auto& b : pop) LBM_CUDA_TRY(b.alloc((size_t)kQ * cap * s));
     LBM_CUDA_TRY(table.alloc((size_t)18 * cap * sizeof(int32_t)));
@@ -363,7 +374,13 @@ struct Pool {
       lbm_status st = capture(cur, chain, tol, max_steps, step_grid, &ge);
       if (st != LBM_OK) return st;
     }
+    long long stepping = 0;
+    for (int i = 0; i < nslots; i++)
+      if (slot_job[i] && h_state[i].active) stepping += h_inst[i].end - h_inst[i].begin;
+    trace.push_back({stepping, chain, -1.f});
+    LBM_CUDA_TRY(cudaEventRecord(chain_ev0, stream));
     LBM_CUDA_TRY(cudaGraphLaunch(ge, stream));
+    LBM_CUDA_TRY(cudaEventRecord(chain_ev1, stream));
     cur = (chain & 1) ? 1 - cur : cur;
     LBM_CUDA_TRY(cudaMemcpyAsync(h_state, state.p, (size_t)nslots * sizeof(InstState), cudaMemcpyDeviceToHost,
                                  stream));
@@ -372,6 +389,11 @@ struct Pool {
   }
   lbm_status wait_chain() {
     LBM_CUDA_TRY(cudaEventSynchronize(done_ev));
+    if (!trace.empty() && trace.back().ms < 0) {
+      float ms = 0;
+      LBM_CUDA_TRY(cudaEventElapsedTime(&ms, chain_ev0, chain_ev1));
+      trace.back().ms = ms;
+    }
     return LBM_OK;
   }
 
@@ -566,6 +588,7 @@ lbm_status lbm_batch_run(lbm_batch* b, double tol, int check_every, long long ma
   LBM_CUDA_TRY(cudaSetDevice(P.device));
   LBM_CUDA_TRY(cudaEventRecord(P.ev0, P.stream));
   b->node_steps = 0;
+  P.trace.clear();
   std::vector<long long> before(b->n);
   for (int i = 0; i < b->n; i++) before[i] = P.h_state[i].steps;
   for (;;) {
@@ -657,6 +680,19 @@ lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* ordering_out, 
   if (ordering_out) *ordering_out = best_o;
   if (block_out) *block_out = best_b;
   if (mlups_out) *mlups_out = best;
+  return LBM_OK;
+}
+
+lbm_status lbm_batch_trace(lbm_batch* b, double* out, int max_rows, int* n_rows) {
+  if (!b || max_rows < 0 || (max_rows > 0 && !out)) return fail(LBM_ERR_ARG, "lbm_batch_trace: bad argument");
+  const auto& t = b->pool.trace;
+  const int n = (int)std::min<size_t>(t.size(), (size_t)max_rows);
+  for (int i = 0; i < n; i++) {
+    out[3 * i] = (double)t[i].stepping_nodes;
+    out[3 * i + 1] = t[i].steps;
+    out[3 * i + 2] = t[i].ms;
+  }
+  if (n_rows) *n_rows = (int)t.size();
   return LBM_OK;
 }
 

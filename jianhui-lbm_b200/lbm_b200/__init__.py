@@ -265,6 +265,7 @@ _SIGNATURES = {
     "lbm_batch_autotune": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
                            C.c_int),
     "lbm_batch_info": ([C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_longlong)], C.c_int),
+    "lbm_batch_trace": ([C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "lbm_batch_destroy": ([C.c_void_p], None),
     "lbm_server_config_default": ([C.POINTER(ServerConfig)], None),
     "lbm_server_create": ([C.POINTER(ServerConfig), C.POINTER(C.c_void_p)], C.c_int),
@@ -625,6 +626,14 @@ class Batch:
         t, ms, ns = C.c_longlong(), C.c_double(), C.c_longlong()
         _check(lib().lbm_batch_info(self._h, C.byref(t), C.byref(ms), C.byref(ns)))
         return {"total_nodes": t.value, "last_run_ms": ms.value, "node_steps": ns.value}
+
+    def trace(self):
+        """Per chain of the last run: [stepping fluid nodes, steps, device ms]."""
+        n = C.c_int()
+        _check(lib().lbm_batch_trace(self._h, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 3))
+        _check(lib().lbm_batch_trace(self._h, out.ctypes.data, n.value, C.byref(n)))
+        return out[: n.value]
 
     def close(self):
         if getattr(self, "_h", None):
