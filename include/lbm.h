@@ -393,12 +393,39 @@ LBM_API lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a);
  * the sums to the nodes inside it (the reference does so when one of
  * par_per_x/y/z equals 1).  All -1 = whole box. */
 LBM_API lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict_nodes);
-/* Constant-phase faces (in_psi_BC = 1 with psi_xp..psi_zn = 1,
- * CG3:3386-3620): after every macro step the fluid nodes on each enabled face
- * of the box take back their initial phase (psi = psi0, rho_r = (psi0 + 1)/2,
- * rho_b = 1 - rho_r).  faces in INPUT order xp, xn, yp, yn, zp, zn; 1 = on,
- * 0 = off. */
+/* Phase faces (in_psi_BC = 1, CG3:3386-3700): after every macro step the
+ * fluid nodes of each enabled face of the box are set, walking the faces x-,
+ * x+, y-, y+, z-, z+ and each face's node list in the reference's order
+ * (x faces: z outer, y inner; y faces: z outer, x inner; z faces: y outer,
+ * x inner):  1 = the initial phase psi0;  2 = the phase of the node's +x
+ * neighbour (periodic; y and z faces copy along x too), except that a node
+ * whose +x neighbour is solid resets every node of its face to psi0 before
+ * the walk goes on;  3 = +1 when draw % 10000 / 10000 < ini_Sat, else -1,
+ * the draws of lbm_cg_set_random numbered from 0 in walk order at every macro
+ * step (the reference reseeds from the clock every macro step, CG3:3321, so
+ * its pattern is the same for all steps within a second of wall time; here
+ * it is the same for every step).  rho_r = (psi + 1)/2, rho_b = 1 - rho_r.
+ * faces in INPUT order xp, xn, yp, yn, zp, zn; 0 = off. */
 LBM_API lbm_status lbm_cg_set_phase_faces(lbm_cg_handle* h, const int faces[6]);
+/* ini_Sat and the seed of the random phase faces (face flag 3) set by the
+ * next lbm_cg_set_phase_faces.  Draw k of a seed is the splitmix64 output of
+ * seed + (k + 1) * 0x9E3779B97F4A7C15 shifted right by 33 bits (a 31-bit
+ * integer, in place of the reference's rand()).  No counterpart in the
+ * reference, which seeds from the clock. */
+LBM_API lbm_status lbm_cg_set_random(lbm_cg_handle* h, double ini_sat, unsigned long long seed);
+/* Mixture injection (mix_psi_thickness > 0 with a phase face at x-): the
+ * nodes with x <= x_last relax towards equilibrium moments without the
+ * surface-tension terms (CG3:2854-2867); x_last < 0 turns it off. */
+LBM_API lbm_status lbm_cg_set_zero_sigma(lbm_cg_handle* h, int x_last);
+/* Initial phase of the mixture injection (psi_mixture_ini, CG3:6151-6350) for
+ * a [nz][ny][nx] mask: in the plane x = thickness, up to portion x its pore
+ * count of pore cells next to a solid (then next to a solid or a marked cell)
+ * are marked wetting, in square rings around the plane's centre; cells with
+ * x <= thickness whose column's cell in that plane is an unmarked pore get
+ * psi = -1, all others +1.  psi_out[nz][ny][nx].  The reference reads outside
+ * the plane when ny != nz; here such cells count as not pore. */
+LBM_API lbm_status lbm_cg_mixture_phase(const uint8_t* mask, int nx, int ny, int nz, int thickness, double portion,
+                                        double* psi_out);
 /* Restores a state like Backup_init (CG3:5438-5690): f [(count+1)*19] in the
  * CG velocity order, psi, rho_r, rho_b [(count+1)], reference id order (row 0
  * ignored).  The next step takes psi / rho_r / rho_b as given and rho, u from f. */
@@ -464,13 +491,21 @@ LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, doub
  * force off until stab_time when the stabiliser is on, the flux thresholds
  * rel_perm_psi / rel_perm_psi2, PerDir, the permeability window and the
  * pressure/velocity faces (Sub_BC, in_BC; their rules off until stab_time
- * when the stabiliser is on).  Options outside a run with the phase read
- * from file (psi faces other than the initial phase, random or mixture
- * initialisation, a self-defined lattice velocity, a non-zero initial
- * velocity, drainage / imbibition control, dynamic input) are rejected with
- * LBM_ERR_ARG naming the field. */
+ * when the stabiliser is on), the phase faces 1-3, the mixture injection
+ * (mix_psi_thickness, protion_w, zero_sigma_thickness) and the random initial
+ * phase (ini_Sat >= 0, with the window buffer ini_buf).  The reference draws
+ * its random numbers from the C library seeded with the clock (CG3:2232,
+ * 3321); here they come from the seeded generator of lbm_cg_set_random with
+ * seed 0 (lbm_cg_create_from_input_seeded takes the seed).  A self-defined
+ * lattice velocity, a non-zero initial velocity, drainage / imbibition
+ * control and dynamic input are rejected with LBM_ERR_ARG naming the field. */
 LBM_API lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
                                             lbm_cg_input* parsed_out);
+/* lbm_cg_create_from_input with the seed of the random initial phase and
+ * the random phase faces (no counterpart in the reference, which seeds from
+ * the clock). */
+LBM_API lbm_status lbm_cg_create_from_input_seeded(const char* input_path, int precision, unsigned long long seed,
+                                                   lbm_cg_handle** out, lbm_cg_input* parsed_out);
 
 /* Output writers of the colour-gradient program: velocity and density VTK
  * (output_velocity CG3:4840-4931, output_density CG3:4933-5020; the

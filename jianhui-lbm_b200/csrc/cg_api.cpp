@@ -37,6 +37,18 @@ struct Dev {
 
 constexpr int kCgGraphSteps = 16;
 
+// Draw k (0-based) of the seeded generator that stands in for the
+// reference's clock-seeded rand(): the splitmix64 output (Steele, Lea and
+// Flood 2014) of the state seed + (k + 1) * 0x9E3779B97F4A7C15, shifted right
+// by 33 bits -- a non-negative 31-bit integer, as rand() returns.
+unsigned long long cg_draw(unsigned long long seed, unsigned long long k) {
+  unsigned long long z = seed + (k + 1) * 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z = z ^ (z >> 31);
+  return z >> 33;
+}
+
 }  // namespace
 }  // namespace lbm
 
@@ -55,7 +67,17 @@ struct lbm_cg_handle {
   Dev f[2], gr, gb, rec, table, corder, psi, rho_r, rho_b, ref_of, partials, result;
   Dev u_prev, axis, partials2, result2;  // Error's u0 and the saturation position sums
   Dev win;                                // permeability window flags, or none
-  Dev face_nodes, face_psi0;              // constant-phase face nodes and their initial phase
+  Dev face_nodes, face_psi0;              // phase-face nodes and their constant values
+  Dev face_src, face_tmp;                 // copied-phase faces: source node per entry (-1: constant), values
+  bool face_copy = false;                 // some face node copies another node's phase
+  // psi / rho_r / rho_b already hold the pending macro step's colour pass
+  // (a reader ran it); the next step uses them instead of running it again,
+  // so that a phase-face change between steps acts from the next macro step
+  // on, as the reference's settings change after comput_macro_variables
+  bool colour_done = false;
+  double rand_sat = -1.0;                 // ini_Sat: threshold of the random phase faces
+  unsigned long long rand_seed = 0;       // seed of the random phase faces
+  Dev zero_sigma;                         // zero-surface-tension layer flags, or none
   int nface = 0;
   std::vector<double> psi0;               // initial phase per node (internal order), as read
   long long window_volume = 0;            // divisor of the fluxes and the saturation
@@ -116,9 +138,17 @@ CgArgs cg_args(lbm_cg_handle* h, int c, int given, bool write_u = false) {
 // constant-phase faces that comput_macro_variables applies after it.
 cudaError_t colour_pass(lbm_cg_handle* h, const CgArgs& a) {
   cudaError_t e = h->f64 ? cg_colour_f64(a, h->stream) : cg_colour_f32(a, h->stream);
-  if (e == cudaSuccess && h->nface > 0)
-    e = cg_phase_faces(h->f64, h->face_nodes.as<int32_t>(), h->face_psi0.as<double>(), h->nface, h->psi.p,
-                       h->rho_r.p, h->rho_b.p, h->stream);
+  if (e == cudaSuccess && h->nface > 0) {
+    const double* vals = h->face_psi0.as<double>();
+    if (h->face_copy) {
+      e = cg_phase_faces_gather(h->f64, h->face_src.as<int32_t>(), vals, h->nface, h->psi.p,
+                                h->face_tmp.as<double>(), h->stream);
+      vals = h->face_tmp.as<double>();
+    }
+    if (e == cudaSuccess)
+      e = cg_phase_faces(h->f64, h->face_nodes.as<int32_t>(), vals, h->nface, h->psi.p, h->rho_r.p, h->rho_b.p,
+                         h->stream);
+  }
   return e;
 }
 
@@ -163,17 +193,17 @@ cudaError_t resolve_faces(lbm_cg_handle* h) {
   return cg_bc_faces(h->f64, bc_args(h, h->cur), h->stream);
 }
 
-cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u, bool pending) {
+cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u, bool pending, bool colour_done = false) {
   const CgArgs a = cg_args(h, c, given, write_u);
   cudaError_t e = face_passes(h, c, given, pending);
-  if (e == cudaSuccess && !given) e = colour_pass(h, a);
+  if (e == cudaSuccess && !given && !colour_done) e = colour_pass(h, a);
   if (e != cudaSuccess) return e;
   return h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
 }
 
 bool same_params(const CgParams& a, const CgParams& b) {
   bool same = a.psi_solid == b.psi_solid && a.cap_a == b.cap_a && a.body_force_phase == b.body_force_phase &&
-              a.flux_psi == b.flux_psi && a.faces == b.faces;
+              a.flux_psi == b.flux_psi && a.faces == b.faces && a.zero_sigma == b.zero_sigma;
   for (int d = 0; d < 3; d++) same = same && a.g[d] == b.g[d] && a.gm[d] == b.gm[d];
   for (int f = 0; f < 6; f++) {
     same = same && a.face_rho[f] == b.face_rho[f];
@@ -265,9 +295,10 @@ lbm_status cg_check(lbm_cg_handle* h) {
 // diagnostics reduction; optional macro fields in internal order.
 lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double* u_out, double* r2 = nullptr) {
   LBM_CUDA_TRY(resolve_faces(h));
-  if (!h->given) {
+  if (!h->given && !h->colour_done) {
     const CgArgs a = cg_args(h, h->cur, 0);
     LBM_CUDA_TRY(colour_pass(h, a));
+    h->colour_done = true;
   }
   CgReduceArgs ra{};
   ra.f = h->f[h->cur].p;
@@ -477,9 +508,10 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   if (nsteps < 0) return fail(LBM_ERR_ARG, "lbm_cg_step: negative step count");
   if (nsteps == 0) return LBM_OK;
   int left = nsteps;
-  // the first step runs alone after init or restore, and when a force change
-  // falls between the pending macro step and the next collision
-  bool special = h->given != 0;
+  // the first step runs alone after init or restore, when a reader already
+  // ran the pending macro step's colour pass, and when a force change falls
+  // between the pending macro step and the next collision
+  bool special = h->given != 0 || h->colour_done;
   for (int d = 0; d < 3; d++) special = special || h->cp.gm[d] != h->cp.g[d];
   // ... and when the state's pending rules differ from what a chain assumes
   const bool faces_on = h->bc_nface > 0 && h->cp.faces;
@@ -492,7 +524,7 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   }
   LBM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
   if (special) {
-    LBM_CUDA_TRY(one_cg_step(h, h->cur, h->given, left == 1, h->faces_pending));
+    LBM_CUDA_TRY(one_cg_step(h, h->cur, h->given, left == 1, h->faces_pending, h->colour_done));
     h->cur = 1 - h->cur;
     h->given = 0;
     for (int d = 0; d < 3; d++) h->cp.gm[d] = h->cp.g[d];
@@ -510,6 +542,7 @@ lbm_status lbm_cg_step(lbm_cg_handle* h, int nsteps) {
   }
   h->faces_pending = faces_on;
   h->uprev_valid = true;
+  h->colour_done = false;
   LBM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
   LBM_CUDA_TRY(cudaEventSynchronize(h->ev1));
   float ms = 0;
@@ -690,28 +723,117 @@ lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict
   return LBM_OK;
 }
 
+lbm_status lbm_cg_set_random(lbm_cg_handle* h, double ini_sat, unsigned long long seed) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  h->rand_sat = ini_sat;
+  h->rand_seed = seed;
+  return LBM_OK;
+}
+
+// Phase faces of comput_macro_variables (in_psi_BC = 1, CG3:3386-3700), after
+// the macro step's psi, in the reference's order: the faces x-, x+, y-, y+,
+// z-, z+, each walking its node list (x faces: z outer, y inner; y faces: z
+// outer, x inner; z faces: y outer, x inner; CG3:2029-2101):
+//   1  the node takes its initial phase;
+//   2  the node takes the phase of its +x neighbour (periodic), which may be a
+//      face node already set earlier in the walk; a node whose +x neighbour
+//      is solid resets every node of the face list to its initial phase and
+//      the walk goes on;
+//   3  the node takes +1 when draw % 10000 / 10000 < ini_Sat, else -1, with
+//      the face draws numbered from 0 in walk order at every macro step (the
+//      reference reseeds from the clock at the start of the macro step,
+//      CG3:3321; here a fixed seed, lbm_cg_set_random);
+// rho_r = (psi + 1) / 2, rho_b = 1 - rho_r.  The walk is resolved here once:
+// the final value of every face node is either a constant (its initial
+// phase, a draw) or the phase some node had before the walk (flag 2 chains),
+// so every step gathers those values and then writes the face nodes.
 lbm_status lbm_cg_set_phase_faces(lbm_cg_handle* h, const int faces[6]) {
   lbm_status st = cg_check(h);
   if (st != LBM_OK) return st;
   if (!faces) return fail(LBM_ERR_ARG, "lbm_cg_set_phase_faces: null faces");
   for (int f = 0; f < 6; f++)
-    if (faces[f] != 0 && faces[f] != 1)
-      return fail(LBM_ERR_ARG, "lbm_cg_set_phase_faces: a face is 0 (off) or 1 (initial phase)");
+    if (faces[f] < 0 || faces[f] > 3)
+      return fail(LBM_ERR_ARG, "lbm_cg_set_phase_faces: a face is 0 (off), 1 (initial phase), 2 (phase of the +x "
+                               "neighbour) or 3 (random)");
+  if (!h->given && !h->colour_done) {
+    // the pending macro step keeps the faces it was computed under
+    LBM_CUDA_TRY(resolve_faces(h));
+    LBM_CUDA_TRY(colour_pass(h, cg_args(h, h->cur, 0)));
+    h->colour_done = true;
+  }
   const Geometry& g = h->geo;
-  std::vector<int32_t> nodes;
-  std::vector<double> vals;
-  for (int x = 0; x < g.count; x++) {
-    const int c = g.coor[g.ref_of[x]];  // i*ny*nz + j*nz + k
-    const int i = c / (g.ny * g.nz), j = (c % (g.ny * g.nz)) / g.nz, k = c % g.nz;
-    // faces in INPUT order xp, xn, yp, yn, zp, zn (CG3:2027-2101 lists)
-    const bool on = (faces[0] && i == g.nx - 1) || (faces[1] && i == 0) || (faces[2] && j == g.ny - 1) ||
-                    (faces[3] && j == 0) || (faces[4] && k == g.nz - 1) || (faces[5] && k == 0);
-    if (on) {
-      nodes.push_back(x);
-      vals.push_back(h->psi0[x]);
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  std::vector<int32_t> at((size_t)nx * ny * nz, -1);  // cell (i*ny*nz + j*nz + k) -> node
+  for (int x = 0; x < g.count; x++) at[g.coor[g.ref_of[x]]] = x;
+  auto node = [&](int i, int j, int k) { return at[((size_t)i * ny + j) * nz + k]; };
+  // value of a node in the walk: kind 0 = its phase before the walk (src), 1 = constant (val)
+  struct Sym {
+    int8_t kind;
+    int32_t src;
+    double val;
+  };
+  std::vector<Sym> cur((size_t)g.count);
+  for (int x = 0; x < g.count; x++) cur[x] = Sym{0, x, 0.0};
+  std::vector<uint8_t> touched((size_t)g.count, 0);
+  int slot = 0;
+  // walk order x-, x+, y-, y+, z-, z+ (faces[] is in INPUT order xp, xn, yp, yn, zp, zn)
+  const int order[6] = {1, 0, 3, 2, 5, 4};
+  for (int o = 0; o < 6; o++) {
+    const int f = order[o], flag = faces[f];
+    if (!flag) continue;
+    std::vector<int32_t> list;
+    if (f <= 1) {
+      const int i = f == 1 ? 0 : nx - 1;
+      for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+          if (node(i, j, k) >= 0) list.push_back(node(i, j, k));
+    } else if (f <= 3) {
+      const int j = f == 3 ? 0 : ny - 1;
+      for (int k = 0; k < nz; k++)
+        for (int i = 0; i < nx; i++)
+          if (node(i, j, k) >= 0) list.push_back(node(i, j, k));
+    } else {
+      const int k = f == 5 ? 0 : nz - 1;
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+          if (node(i, j, k) >= 0) list.push_back(node(i, j, k));
+    }
+    for (int32_t x : list) touched[x] = 1;
+    if (flag == 1) {
+      for (int32_t x : list) cur[x] = Sym{1, -1, h->psi0[x]};
+    } else if (flag == 2) {
+      for (size_t ii = 0; ii < list.size(); ii++) {
+        const int c = g.coor[g.ref_of[list[ii]]];
+        const int i = c / (ny * nz), j = (c % (ny * nz)) / nz, k = c % nz;
+        const int nb = node((i + 1) % nx, j, k);
+        if (nb >= 0) {
+          cur[list[ii]] = cur[nb];
+        } else {
+          for (int32_t x : list) cur[x] = Sym{1, -1, h->psi0[x]};
+        }
+      }
+    } else {
+      for (int32_t x : list) {
+        const double r = (double)(cg_draw(h->rand_seed, (unsigned long long)slot++) % 10000) / 10000;
+        cur[x] = Sym{1, -1, r < h->rand_sat ? 1.0 : -1.0};
+      }
     }
   }
+  std::vector<int32_t> nodes, src;
+  std::vector<double> vals;
+  bool copy = false;
+  for (int x = 0; x < g.count; x++) {
+    if (!touched[x]) continue;
+    const Sym& s = cur[x];
+    if (s.kind == 0 && s.src == x) continue;  // a flag-2 chain back to its own phase
+    nodes.push_back(x);
+    src.push_back(s.kind == 0 ? s.src : -1);
+    vals.push_back(s.kind == 0 ? 0.0 : s.val);
+    copy = copy || s.kind == 0;
+  }
   h->nface = (int)nodes.size();
+  h->face_copy = copy;
   if (h->nface > 0) {
     LBM_CUDA_TRY(h->face_nodes.alloc(nodes.size() * sizeof(int32_t)));
     LBM_CUDA_TRY(h->face_psi0.alloc(vals.size() * sizeof(double)));
@@ -719,9 +841,15 @@ lbm_status lbm_cg_set_phase_faces(lbm_cg_handle* h, const int faces[6]) {
                                  h->stream));
     LBM_CUDA_TRY(cudaMemcpyAsync(h->face_psi0.p, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice,
                                  h->stream));
+    if (copy) {
+      LBM_CUDA_TRY(h->face_src.alloc(src.size() * sizeof(int32_t)));
+      LBM_CUDA_TRY(h->face_tmp.alloc(vals.size() * sizeof(double)));
+      LBM_CUDA_TRY(cudaMemcpyAsync(h->face_src.p, src.data(), src.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                   h->stream));
+    }
     LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   }
-  drop_graphs(h);  // the chains captured so far do not reset the faces
+  drop_graphs(h);  // the chains captured so far do not apply these faces
   return LBM_OK;
 }
 
@@ -753,6 +881,7 @@ lbm_status lbm_cg_set_state(lbm_cg_handle* h, const double* f, const double* psi
     LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   }
   h->given = 2;
+  h->colour_done = false;
   h->uprev_valid = false;
   h->faces_pending = false;  // the state given is the one after its step's rules
   return LBM_OK;
@@ -764,8 +893,103 @@ lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, double* out)
   return read_phase_file(path, nx, ny, nz, out);
 }
 
+// Initial phase of the mixture injection (psi_mixture_ini, CG3:6151-6350).
+// In the plane x = thickness, pore cells next to a solid cell are marked
+// wetting (up to portion x the plane's pore count), starting at the plane's
+// centre and walking square rings outwards; a second pass of rings marks
+// cells next to a solid or an already marked cell (the cells it marks only
+// count as marked after the pass).  The neighbours looked at are CG
+// directions 0..17 (the cell itself included, direction 18 = (0,-1,1) not),
+// within the box (no wrap).  Every cell with x <= thickness whose column
+// (thickness, y, z) is an unmarked pore starts in component B (psi = -1),
+// every other cell in component A (psi = +1).  The reference walks the rings
+// up to max(ny, nz)/2 and reads outside the plane when ny != nz; cells outside
+// the plane count here as not pore.
+lbm_status lbm_cg_mixture_phase(const uint8_t* mask, int nx, int ny, int nz, int thickness, double portion,
+                                double* psi_out) {
+  if (!mask || !psi_out || nx <= 0 || ny <= 0 || nz <= 0)
+    return fail(LBM_ERR_ARG, "lbm_cg_mixture_phase: bad argument");
+  if (thickness <= 0 || thickness >= nx)
+    return fail(LBM_ERR_ARG, "lbm_cg_mixture_phase: thickness must lie in 1..nx-1");
+  const int ci = thickness;
+  auto solid = [&](int i, int j, int k) { return mask[((size_t)k * ny + j) * nx + i] != 0; };
+  // state of the plane x = ci: 1 solid, 0 pore, 2 marked, -2 marked in this ring pass
+  std::vector<int> s2((size_t)ny * nz);
+  auto at = [&](int j, int k) -> int& { return s2[(size_t)j * nz + k]; };
+  int fluid_sum = 0;
+  for (int j = 0; j < ny; j++)
+    for (int k = 0; k < nz; k++) {
+      at(j, k) = solid(ci, j, k) ? 1 : 0;
+      fluid_sum += at(j, k) == 0;
+    }
+  const int nw_node = (int)(fluid_sum * portion);
+  int marked = 0;
+  // state of any cell of the box: the plane's own state, elsewhere the mask
+  auto state = [&](int i, int j, int k) { return i == ci ? at(j, k) : (solid(i, j, k) ? 1 : 0); };
+  auto next_to = [&](int j, int k, bool level2) {
+    for (int ls = 0; ls < 18; ls++) {
+      const int li = ci + cg::ex(ls), lj = j + cg::ey(ls), lk = k + cg::ez(ls);
+      if (li < 0 || li >= nx || lj < 0 || lj >= ny || lk < 0 || lk >= nz) continue;
+      const int v = state(li, lj, lk);
+      if (level2 ? v > 0 : v == 1) return true;
+    }
+    return false;
+  };
+  auto visit = [&](int j, int k, bool level2) {
+    if (j < 0 || j >= ny || k < 0 || k >= nz || at(j, k) != 0) return;
+    if (next_to(j, k, level2) && marked < nw_node) {
+      at(j, k) = level2 ? -2 : 2;
+      marked++;
+    }
+  };
+  const int ceny = ny / 2, cenz = nz / 2;
+  const int rad_max = std::max(ny / 2, nz / 2);
+  visit(ceny, cenz, false);
+  for (int pass = 0; pass < 2; pass++) {
+    const bool level2 = pass == 1;
+    for (int rad = 1; marked < nw_node && rad < rad_max; rad++) {
+      for (int k = cenz - rad; k <= cenz + rad; k += 2 * rad)
+        for (int j = ceny - rad; j <= ceny + rad; j++) visit(j, k, level2);
+      for (int j = ceny - rad; j <= ceny + rad; j += 2 * rad)
+        for (int k = cenz - rad; k <= cenz + rad; k++) visit(j, k, level2);
+    }
+  }
+  for (auto& v : s2)
+    if (v == -2) v = 2;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) psi_out[((size_t)k * ny + j) * nx + i] = (i <= ci && at(j, k) == 0) ? -1.0 : 1.0;
+  return LBM_OK;
+}
+
+lbm_status lbm_cg_set_zero_sigma(lbm_cg_handle* h, int x_last) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (x_last < 0) {
+    h->zero_sigma.alloc(0);
+    h->cp.zero_sigma = nullptr;
+    return LBM_OK;
+  }
+  const Geometry& g = h->geo;
+  std::vector<uint8_t> flag((size_t)g.npad, 0);
+  for (int x = 0; x < g.count; x++) {
+    const int c = g.coor[g.ref_of[x]];  // i*ny*nz + j*nz + k
+    flag[x] = c / (g.ny * g.nz) <= x_last;
+  }
+  LBM_CUDA_TRY(h->zero_sigma.alloc(flag.size()));
+  LBM_CUDA_TRY(cudaMemcpyAsync(h->zero_sigma.p, flag.data(), flag.size(), cudaMemcpyHostToDevice, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->cp.zero_sigma = h->zero_sigma.as<uint8_t>();
+  return LBM_OK;
+}
+
 lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
                                     lbm_cg_input* parsed_out) {
+  return lbm_cg_create_from_input_seeded(input_path, precision, 0ULL, out, parsed_out);
+}
+
+lbm_status lbm_cg_create_from_input_seeded(const char* input_path, int precision, unsigned long long seed,
+                                           lbm_cg_handle** out, lbm_cg_input* parsed_out) {
   if (!out) return fail(LBM_ERR_ARG, "lbm_cg_create_from_input: null output");
   *out = nullptr;
   lbm_cg_input in;
@@ -780,16 +1004,20 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
       return fail(LBM_ERR_ARG, "pre_* / vel_*: face flags must be 0 or 1");
   const int pf[6] = {in.psi_xp, in.psi_xn, in.psi_yp, in.psi_yn, in.psi_zp, in.psi_zn};
   for (int f = 0; f < 6; f++)
-    if (in.in_psi_bc == 1 && pf[f] != 0 && pf[f] != 1)
-      return fail(LBM_ERR_ARG, "psi_xp..psi_zn: only constant-phase faces of the initial phase (1) are "
-                               "supported; 2 (copy the +x neighbour) and 3 (random) are not");
-  if (in.ini_sat >= 0)
-    return fail(LBM_ERR_ARG, "ini_Sat: random initial phase (seeded from the clock) is not supported; use -1");
-  if (in.mix_psi_thickness > 0) return fail(LBM_ERR_ARG, "mix_psi_thickness: mixture injection is not supported");
+    if (in.in_psi_bc == 1 && (pf[f] < 0 || pf[f] > 3))
+      return fail(LBM_ERR_ARG, "psi_xp..psi_zn: a phase face is 0, 1 (initial phase), 2 (+x neighbour) or 3 (random)");
+  if (in.mix_psi_thickness > 0 && in.mix_psi_thickness >= in.nx)
+    return fail(LBM_ERR_ARG, "mix_psi_thickness must be smaller than nx");
   if (in.lattice_v != 0) return fail(LBM_ERR_ARG, "lattice_v: self-defined lattice velocity is not supported");
   if (in.inivx != 0 || in.inivy != 0 || in.inivz != 0)
     return fail(LBM_ERR_ARG, "initial velocity: only a fluid at rest is supported");
-  if (in.rel_perm_id_dir != 0) return fail(LBM_ERR_ARG, "rel_perm_id_dir: imbibition / drainage control is not supported");
+  if (in.rel_perm_id_dir < 0 || in.rel_perm_id_dir > 2)
+    return fail(LBM_ERR_ARG, "rel_perm_id_dir: 0 (off), 1 (imbibition) or 2 (drainage)");
+  if (in.rel_perm_id_dir > 0 && in.rel_perm_chan_num <= 0)
+    return fail(LBM_ERR_ARG, "rel_perm_id_dir: rel_perm_chan_num must be positive");
+  // the imbibition / drainage control turns the phase faces on in init
+  // (CG3:2339-2345); a restart (Backup_init) skips it
+  if (in.rel_perm_id_dir > 0 && in.mode_backup_ini == 0) in.in_psi_bc = 1;
   if (in.pressure_change2 < 0 || in.pressure_change2 > 3)
     return fail(LBM_ERR_ARG, "pressure_change2: the capillary-pressure axis is 0 (off) or 1..3");
   if (in.pressure_change2 > 0 && (in.chan_no <= 0 || in.interval_pre <= 0))
@@ -804,7 +1032,35 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
   std::vector<double> psi(cells);
   // file paths are relative to the working directory, as in the reference
   if ((st = read_mask_file(in.geometry_file, in.nx, in.ny, in.nz, in.decbin, mask.data())) != LBM_OK) return st;
-  if ((st = read_phase_file(in.phase_file, in.nx, in.ny, in.nz, psi.data())) != LBM_OK) return st;
+  if (in.mix_psi_thickness > 0) {
+    // mixture injection: the initial phase is built from the geometry and
+    // the phase file is not read (CG3:2117-2128)
+    if ((st = lbm_cg_mixture_phase(mask.data(), in.nx, in.ny, in.nz, in.mix_psi_thickness, in.protion_w,
+                                   psi.data())) != LBM_OK)
+      return st;
+  } else if (in.ini_sat >= 0) {
+    // random initial phase (init, CG3:2384-2455): one draw per fluid node in
+    // id order, +1 when draw % 10000 / 10000 < ini_Sat; with a partial
+    // permeability window and a buffer phase (ini_buf = +-1), the nodes
+    // outside the window on a windowed axis take the buffer phase.  The
+    // reference seeds from the clock (CG3:2232); here the seed is given.
+    Geometry order;
+    compact_reference(mask.data(), in.nx, in.ny, in.nz, &order);
+    const int nyz = in.ny * in.nz;
+    for (int id = 1; id <= order.count; id++) {
+      const int c = order.coor[id];  // i*ny*nz + j*nz + k
+      const int i = c / nyz, j = (c % nyz) / in.nz, k = c % in.nz;
+      const double r = (double)(cg_draw(seed, (unsigned long long)(id - 1)) % 10000) / 10000;
+      double v = r < in.ini_sat ? 1.0 : -1.0;
+      const bool outside = (in.par_per_x > 0 && (i < in.per_xn || i > in.per_xp)) ||
+                           (in.par_per_y > 0 && (j < in.per_yn || j > in.per_yp)) ||
+                           (in.par_per_z > 0 && (k < in.per_zn || k > in.per_zp));
+      if (outside && (in.ini_buf == 1 || in.ini_buf == -1)) v = in.ini_buf;
+      psi[((size_t)k * in.ny + j) * in.nx + i] = v;
+    }
+  } else if ((st = read_phase_file(in.phase_file, in.nx, in.ny, in.nz, psi.data())) != LBM_OK) {
+    return st;
+  }
   lbm_cg_params p{};
   p.nu_l = in.nu_l;
   p.nu_g = in.nu_g;
@@ -850,7 +1106,15 @@ lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_c
     }
   }
   if (in.in_psi_bc == 1 && (pf[0] || pf[1] || pf[2] || pf[3] || pf[4] || pf[5])) {
-    if ((st = lbm_cg_set_phase_faces(h, pf)) != LBM_OK) {
+    if ((st = lbm_cg_set_random(h, in.ini_sat, seed)) != LBM_OK || (st = lbm_cg_set_phase_faces(h, pf)) != LBM_OK) {
+      lbm_cg_destroy(h);
+      return st;
+    }
+  }
+  // the surface tension is off in the layer x <= zero_sigma_thickness while
+  // the mixture injects at the x- face (CG3:2854-2855)
+  if (in.mix_psi_thickness > 0 && in.psi_xn > 0) {
+    if ((st = lbm_cg_set_zero_sigma(h, in.zero_sigma_thickness)) != LBM_OK) {
       lbm_cg_destroy(h);
       return st;
     }

@@ -20,6 +20,9 @@ struct CgParams {
   int faces;
   double face_rho[6];
   double face_u[6][3];
+  // [npad] 1 = node in the zero-surface-tension layer of the mixture
+  // injection (meq without the CapA |C| terms, CG3:2854-2867), or null
+  const uint8_t* zero_sigma;
 };
 
 struct CgArgs {
@@ -95,6 +98,10 @@ cudaError_t cg_export_f(bool f64, const void* f, const int32_t* table, const int
                         double* out, cudaStream_t st);
 // Constant-phase faces: nodes[i] (internal index) takes psi0[i] after the
 // colour pass, rho_r = (psi0 + 1)/2, rho_b = 1 - rho_r.
+// out[i] = psi[src[i]] (src >= 0) or val[i]: the values of the face rules,
+// read before any face node is written
+cudaError_t cg_phase_faces_gather(bool f64, const int32_t* src, const double* val, int nface, const void* psi,
+                                  double* out, cudaStream_t st);
 cudaError_t cg_phase_faces(bool f64, const int32_t* nodes, const double* psi0, int nface, void* psi, void* rho_r,
                            void* rho_b, cudaStream_t st);
 cudaError_t cg_import_f(bool f64, void* f, const int32_t* table, const int32_t* ref_of, int n, int npad,

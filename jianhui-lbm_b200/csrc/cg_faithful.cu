@@ -43,6 +43,30 @@ __global__ void cg_phase_faces_kernel(const int32_t* __restrict__ nodes, const d
   rho_b[x] = (T)(1.0 - rr);
 }
 
+// Faces whose value copies another node's phase of this macro step (face
+// flag 2): every value is read (the node's psi before any face rule, or a
+// constant) before any face node is written, since a copied node may itself
+// be a face node.
+template <typename T>
+__global__ void cg_phase_faces_gather_kernel(const int32_t* __restrict__ src, const double* __restrict__ val,
+                                             int nface, const T* __restrict__ psi, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nface) return;
+  const int s = src[i];
+  out[i] = s >= 0 ? (double)psi[s] : val[i];
+}
+
+cudaError_t cg_phase_faces_gather(bool f64, const int32_t* src, const double* val, int nface, const void* psi,
+                                  double* out, cudaStream_t st) {
+  if (nface <= 0) return cudaSuccess;
+  const int g = (nface + 255) / 256;
+  if (f64)
+    cg_phase_faces_gather_kernel<double><<<g, 256, 0, st>>>(src, val, nface, (const double*)psi, out);
+  else
+    cg_phase_faces_gather_kernel<float><<<g, 256, 0, st>>>(src, val, nface, (const float*)psi, out);
+  return cudaGetLastError();
+}
+
 cudaError_t cg_phase_faces(bool f64, const int32_t* nodes, const double* psi0, int nface, void* psi, void* rho_r,
                            void* rho_b, cudaStream_t st) {
   if (nface <= 0) return cudaSuccess;

@@ -156,8 +156,10 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
     MG[15] = ux * fz + uz * fx;
   }
 
-  // equilibrium moments with the surface-tension perturbation (CG3:2836-2851)
-  const float cap = (float)a.p.cap_a;
+  // equilibrium moments with the surface-tension perturbation (CG3:2836-2851),
+  // none in the zero-surface-tension layer of a mixture injection (CG3:2854-2867)
+  const bool zero_sigma = a.p.zero_sigma != nullptr && a.p.zero_sigma[x];
+  const float cap = zero_sigma ? 0.f : (float)a.p.cap_a;
   const float cc5 = 0.5f * cap * cc;
   float meq[kQ];
 #pragma unroll

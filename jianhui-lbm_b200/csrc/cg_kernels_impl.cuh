@@ -169,12 +169,23 @@ __global__ void __launch_bounds__(256) cg_collide_kernel(CgArgs a) {
   meq[3] = T(1.0) * ux;
   meq[5] = T(1.0) * uy;
   meq[7] = T(1.0) * uz;
-  meq[1] = T(1.0) * (ux * ux + uy * uy + uz * uz) + cap * cc;
-  meq[9] = T(1.0) * (T(2) * ux * ux - uy * uy - uz * uz) + T(0.5) * cap * cc * (T(2) * nx * nx - ny * ny - nz * nz);
-  meq[11] = T(1.0) * (uy * uy - uz * uz) + T(0.5) * cap * cc * (ny * ny - nz * nz);
-  meq[13] = T(1.0) * ux * uy + T(0.5) * cap * cc * (nx * ny);
-  meq[14] = T(1.0) * uy * uz + T(0.5) * cap * cc * (ny * nz);
-  meq[15] = T(1.0) * ux * uz + T(0.5) * cap * cc * (nx * nz);
+  if (a.p.zero_sigma != nullptr && a.p.zero_sigma[x]) {
+    // mixture-injection layer: the equilibrium moments without the surface
+    // tension terms (CG3:2854-2867)
+    meq[1] = T(1.0) * (ux * ux + uy * uy + uz * uz);
+    meq[9] = T(1.0) * (T(2) * ux * ux - uy * uy - uz * uz);
+    meq[11] = T(1.0) * (uy * uy - uz * uz);
+    meq[13] = T(1.0) * ux * uy;
+    meq[14] = T(1.0) * uy * uz;
+    meq[15] = T(1.0) * ux * uz;
+  } else {
+    meq[1] = T(1.0) * (ux * ux + uy * uy + uz * uz) + cap * cc;
+    meq[9] = T(1.0) * (T(2) * ux * ux - uy * uy - uz * uz) + T(0.5) * cap * cc * (T(2) * nx * nx - ny * ny - nz * nz);
+    meq[11] = T(1.0) * (uy * uy - uz * uz) + T(0.5) * cap * cc * (ny * ny - nz * nz);
+    meq[13] = T(1.0) * ux * uy + T(0.5) * cap * cc * (nx * ny);
+    meq[14] = T(1.0) * uy * uz + T(0.5) * cap * cc * (ny * nz);
+    meq[15] = T(1.0) * ux * uz + T(0.5) * cap * cc * (nx * nz);
+  }
 
   // viscosity interpolation in psi (CG3:2862-2872)
   T s_v;

@@ -1,6 +1,6 @@
 // lbm_cg -- drop-in driver for the colour-gradient two-phase sparse solver.
 //
-//   lbm_cg INPUT.dat [checkpoint_prefix] [--precision f64|f32]
+//   lbm_cg INPUT.dat [checkpoint_prefix] [--precision f64|f32] [--seed N]
 //
 // Runs the time loop of MP_3D/Multi_Component_CG_MPI_SPARSE_Software_3DPartition.cpp
 // (main, CG3:336-1100) on the GPU through liblbm.so and produces the same side
@@ -202,22 +202,26 @@ struct LeastSquares {
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::cerr << "usage: lbm_cg INPUT.dat [checkpoint_prefix] [--precision f64|f32]" << std::endl;
+    std::cerr << "usage: lbm_cg INPUT.dat [checkpoint_prefix] [--precision f64|f32] [--seed N]" << std::endl;
     return 2;
   }
   std::string pfix = "./";
   int precision = LBM_PREC_F64;
+  unsigned long long seed = 0;  // random initial phase and random phase faces
   for (int a = 2; a < argc; a++) {
     const std::string s = argv[a];
     if (s == "--precision" && a + 1 < argc)
       precision = std::string(argv[++a]) == "f32" ? LBM_PREC_F32 : LBM_PREC_F64;
+    else if (s == "--seed" && a + 1 < argc)
+      seed = std::stoull(argv[++a]);
     else if (a == 2)
       pfix = s;
   }
   Clock clock;
   lbm_cg_input in;
   lbm_cg_handle* h = nullptr;
-  if (lbm_cg_create_from_input(argv[1], precision, &h, &in) != LBM_OK) return die("lbm_cg_create_from_input");
+  if (lbm_cg_create_from_input_seeded(argv[1], precision, seed, &h, &in) != LBM_OK)
+    return die("lbm_cg_create_from_input");
   const int nx = in.nx, ny = in.ny, nz = in.nz;
   const std::string out = in.output_path;
 
@@ -306,6 +310,25 @@ int main(int argc, char** argv) {
   int count = 0;
   double porosity = 0;
   lbm_cg_info(h, &count, &porosity, nullptr, nullptr);
+  // Imbibition / drainage control (rel_perm_id_dir, CG3:615-621, 1121-1200,
+  // 2467-2484): target saturations sw[i] = (i + 1) / (chan + 1) rising (1) or
+  // (chan - i) / (chan + 1) falling (2); the first target is the first one the
+  // initial saturation has not passed.  At a report, once the saturation
+  // passes the target the phase field is written, and the next target
+  // becomes the threshold of the random phase faces (ini_Sat).  The
+  // reference reads past its target array once every target is passed; here
+  // nothing more happens then.
+  const int chan = in.rel_perm_id_dir > 0 ? in.rel_perm_chan_num : 0;
+  std::vector<double> sw((size_t)std::max(chan, 0));
+  for (int i = 0; i < chan; i++)
+    sw[i] = in.rel_perm_id_dir == 1 ? (double)(i + 1) * (1.0 / (chan + 1)) : (double)(chan - i) * (1.0 / (chan + 1));
+  // init sets the control up (CG3:2339-2345, 2467-2484); after a restart
+  // (Backup_init) its state stays zero and it never acts
+  int id_ids = 0, id_mode = in.mode_backup_ini == 0 ? 1 : 0;
+  if (chan > 0 && id_mode == 1) {
+    while (id_ids < chan && (in.rel_perm_id_dir == 1 ? S_l > sw[id_ids] : S_l < sw[id_ids])) id_ids++;
+  }
+  const int pf[6] = {in.psi_xp, in.psi_xn, in.psi_yp, in.psi_yn, in.psi_zp, in.psi_zn};
   std::vector<double> rho((size_t)count + 1);
 
   auto block = [&](std::ostream& o, long long nn) {
@@ -340,6 +363,16 @@ int main(int argc, char** argv) {
     return lbm_cg_set_faces(h, rho_set, v_face, faces_on ? 1 : 0) == LBM_OK;
   };
 
+  // output_psi (CG3:5022-5114) with its title lines (CG3:5058-5059)
+  auto write_psi = [&](long long step) {
+    std::ostringstream v, t, tag;
+    tag << step;
+    v << " - " << in.nu_l << " " << in.nu_g << " " << in.contact_angle << " " << cap_a;
+    t << "J.Yang Lattice Boltzmann Simulation 3D MC- " << S_l << " " << porosity << " " << in.reso << " "
+      << drv.g[0] << " " << drv.p_p[0] << " " << drv.p_n[0];
+    return lbm_cg_write_vtk_psi(h, (out + "LBM_psi_" + tag.str() + ".vtk").c_str(), v.str().c_str(),
+                                t.str().c_str()) == LBM_OK;
+  };
   long long n = 0;
   while (n <= in.n_max) {
     if (stab && n == in.stab_time) {
@@ -408,6 +441,19 @@ int main(int argc, char** argv) {
     Sd_l = d.sd_l;
     Sd_g = d.sd_g;
     if (in.least_square > 0) ls.push(Per_l[ls_dir] * rk, Per_g[ls_dir] * rk);
+    // Rel_Perm_Imb_Dra (CG3:1121-1200), after the least-squares fit
+    if (chan > 0 && id_mode > 0 && id_ids < chan) {
+      if (id_mode == 1 && (in.rel_perm_id_dir == 1 ? S_l > sw[id_ids] : S_l < sw[id_ids])) id_mode = 2;
+      if (id_mode == 2) {
+        if (!write_psi(n)) return die("lbm_cg_write_vtk_psi");
+        id_ids++;
+        if (id_ids < chan) {
+          id_mode = 1;
+          if (lbm_cg_set_random(h, sw[id_ids], seed) != LBM_OK || lbm_cg_set_phase_faces(h, pf) != LBM_OK)
+            return die("lbm_cg_set_phase_faces");
+        }
+      }
+    }
     {
       const double finish = clock.now();
       hms(n > 0 ? (in.n_max - n) * (finish / n) : 0.0, &th, &tm, &ts);
@@ -465,16 +511,7 @@ int main(int argc, char** argv) {
     if (in.fre_ve > 0 && n % in.fre_ve == 0 && n > 0 &&
         lbm_cg_write_vtk_velocity(h, (out + "LBM_velocity_Vector_" + tag.str() + ".vtk").c_str()) != LBM_OK)
       return die("lbm_cg_write_vtk_velocity");
-    if (in.fre_psi >= 0 && n % in.fre_psi == 0) {
-      // output_psi's title lines (CG3:5058-5059)
-      std::ostringstream v, t;
-      v << " - " << in.nu_l << " " << in.nu_g << " " << in.contact_angle << " " << cap_a;
-      t << "J.Yang Lattice Boltzmann Simulation 3D MC- " << S_l << " " << porosity << " " << in.reso << " "
-        << drv.g[0] << " " << drv.p_p[0] << " " << drv.p_n[0];
-      if (lbm_cg_write_vtk_psi(h, (out + "LBM_psi_" + tag.str() + ".vtk").c_str(), v.str().c_str(),
-                               t.str().c_str()) != LBM_OK)
-        return die("lbm_cg_write_vtk_psi");
-    }
+    if (in.fre_psi >= 0 && n % in.fre_psi == 0 && !write_psi(n)) return die("lbm_cg_write_vtk_psi");
     if (in.fre_backup > 0 && n % in.fre_backup == 0 && n > 0 && lbm_cg_write_checkpoint(h, out.c_str(), n) != LBM_OK)
       return die("lbm_cg_write_checkpoint");
     if (u_max_ref >= 5) {

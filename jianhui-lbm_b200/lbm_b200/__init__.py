@@ -290,6 +290,11 @@ _SIGNATURES = {
     "lbm_cg_set_window": ([C.c_void_p, _I32P, C.c_int], C.c_int),
     "lbm_cg_set_state": ([C.c_void_p, _F64P, _F64P, _F64P, _F64P], C.c_int),
     "lbm_cg_set_phase_faces": ([C.c_void_p, _I32P], C.c_int),
+    "lbm_cg_set_zero_sigma": ([C.c_void_p, C.c_int], C.c_int),
+    "lbm_cg_set_random": ([C.c_void_p, C.c_double, C.c_ulonglong], C.c_int),
+    "lbm_cg_create_from_input_seeded": ([C.c_char_p, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p), C.POINTER(CGInput)],
+                                        C.c_int),
+    "lbm_cg_mixture_phase": ([_U8P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _F64P], C.c_int),
     "lbm_read_cg_input": ([C.c_char_p, C.POINTER(CGInput)], C.c_int),
     "lbm_read_phase": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _F64P], C.c_int),
     "lbm_cg_create_from_input": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(CGInput)], C.c_int),
@@ -468,14 +473,15 @@ class ColourGradient:
         self.count, self.porosity = c.value, ph.value
 
     @classmethod
-    def from_input(cls, input_path, precision="f64"):
+    def from_input(cls, input_path, precision="f64", seed=0):
         """Solver of the colour-gradient program's INPUT file (geometry and
-        phase file read from the paths it names); returns (solver, input dict)."""
+        phase file read from the paths it names); returns (solver, input dict).
+        seed: the random initial phase and random phase faces."""
         self = cls.__new__(cls)
         h, inp = C.c_void_p(), CGInput()
-        _check(lib().lbm_cg_create_from_input(os.fsencode(input_path),
-                                              PRECISIONS[precision] if isinstance(precision, str) else int(precision),
-                                              C.byref(h), C.byref(inp)))
+        _check(lib().lbm_cg_create_from_input_seeded(os.fsencode(input_path),
+                                                     PRECISIONS[precision] if isinstance(precision, str)
+                                                     else int(precision), int(seed), C.byref(h), C.byref(inp)))
         self._h = h
         c, ph, st, ms = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
         _check(lib().lbm_cg_info(h, C.byref(c), C.byref(ph), C.byref(st), C.byref(ms)))
@@ -505,6 +511,15 @@ class ColourGradient:
     def set_phase_faces(self, faces):
         """Constant initial phase on the box faces (xp, xn, yp, yn, zp, zn; 1 = on)."""
         _check(lib().lbm_cg_set_phase_faces(self._h, np.ascontiguousarray(faces, dtype=np.int32)))
+
+    def set_random(self, ini_sat, seed):
+        """Threshold and seed of the random phase faces (face flag 3) for the
+        next set_phase_faces."""
+        _check(lib().lbm_cg_set_random(self._h, float(ini_sat), int(seed)))
+
+    def set_zero_sigma(self, x_last):
+        """Mixture injection: no surface tension in the layer x <= x_last (-1 = off)."""
+        _check(lib().lbm_cg_set_zero_sigma(self._h, int(x_last)))
 
     def set_state(self, f, psi, rho_r, rho_b):
         """Restores f [(count+1), 19] (CG velocity order) and psi / rho_r /
@@ -772,6 +787,16 @@ def slab_partition(mask, nranks):
     first = np.zeros(int(nranks) + 1, dtype=np.int32)
     _check(lib().lbm_slab_partition(m.reshape(-1), nx, ny, nz, int(nranks), first))
     return first
+
+
+def mixture_phase(mask, thickness, portion):
+    """Initial phase of the mixture injection (psi_mixture_ini) of a
+    [nz, ny, nx] mask: +1 / -1 per cell, [nz, ny, nx] float64."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    nz, ny, nx = m.shape
+    out = np.zeros(m.size)
+    _check(lib().lbm_cg_mixture_phase(m.reshape(-1), nx, ny, nz, int(thickness), float(portion), out))
+    return out.reshape(nz, ny, nx)
 
 
 def read_phase(path, shape):

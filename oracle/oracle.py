@@ -388,7 +388,13 @@ class ReferenceCG3:
         L.ref_cg3_get_scalars.argtypes = [_F64P, _F64P, _F64P, _F64P]
         L.ref_cg3_get_M.argtypes = [_F64P]
         L.ref_cg3_get_MI.argtypes = [_F64P]
+        L.ref_cg3_set_mixture.argtypes = [C.c_int, C.c_double]
         self.count = 0
+
+    def set_mixture(self, thickness, portion):
+        """Mixture injection for the next create(): the reference builds the
+        initial phase itself (psi_mixture_ini) instead of reading the file."""
+        self.L.ref_cg3_set_mixture(int(thickness), float(portion))
 
     def create(self, mask, psi, nu_l, nu_g, psi_solid, cap_a, g, body_force_phase=-1, flux_psi=0.99,
                flux_umax=0.01, workdir=None):

@@ -36,7 +36,16 @@ double** rows(int count, int width) {
 }  // namespace
 
 #pragma GCC visibility push(default)
+// mixture injection settings for the next ref_cg3_create (0 = off)
+static int h_mix_thickness = 0;
+static double h_mix_portion = 0.5;
+
 extern "C" {
+
+void ref_cg3_set_mixture(int thickness, double portion) {
+  h_mix_thickness = thickness;
+  h_mix_portion = portion;
+}
 
 int ref_cg3_create(const char* mask_path, const char* psi_path, int nx, int ny, int nz, int is_binary,
                    double nu_l, double nu_g, double psi_solid, double cap_a, double gx_in, double gy_in,
@@ -61,7 +70,7 @@ int ref_cg3_create(const char* mask_path, const char* psi_path, int nx, int ny, 
   ini_Sat = -1; ini_buf = 0;
   rel_perm_psi = flux_psi; rel_perm_psi2 = flux_umax;
   par_per_x = par_per_y = par_per_z = 0;
-  mix_psi_thickness = 0; zero_sigma_thickness = 0;
+  mix_psi_thickness = h_mix_thickness; protion_w = h_mix_portion; zero_sigma_thickness = 0;
   bodyforce_apply = body_force_phase;
   pressure_change = 0; pressure_change2 = 0; input_dynamic = 0;
   rel_perm_id_dir = 0; rel_perm_chan_num = 0;

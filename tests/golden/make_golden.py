@@ -228,6 +228,15 @@ def cg_geometry():
     return mask, psi
 
 
+def cg_mix_geometry():
+    """16x12x12 spheres (porosity 0.6) for the mixture-injection run: ny = nz,
+    so the reference's ring walk of the mixture initialisation (rings up to
+    max(ny, nz)/2 around the plane's centre) stays inside the plane.  The
+    phase file is not read with mixture injection; it is written all +1."""
+    mask = G.overlapping_spheres((16, 12, 12), 0.6, 2.5, seed=31)
+    return mask, np.ones(mask.shape)
+
+
 def phase_text(psi):
     return " ".join(str(int(v)) for v in psi.reshape(-1)) + "\n"
 
@@ -250,6 +259,10 @@ CG_RUNS = {
     # face (in_psi_BC = 1, the reference's sample input turns the x faces on),
     # checkpoint at the end only
     "cg_outputs_psi.npz": dict(L7=1, L15="1 1", L16="1 0", L29=-1, L30=-1, L45=0),
+    # phase faces copying the +x neighbour's phase (flag 2) on both x faces,
+    # y- and z+ (their copies run along x inside the face), the initial phase
+    # on y+; phase VTK every 50 steps
+    "cg_outputs_psi2.npz": dict(L7=1, L15="2 2", L16="1 2", L17="2 0", L29=-1, L30=-1, L45=0),
     # capillary-pressure stepping along x with the body force: three steps
     # of 30 steps each towards 3e-5, the next one after two reports in a row
     # with the saturation changing by less than 1e-2; reports every 10 steps
@@ -294,10 +307,45 @@ CG_RUNS = {
 }
 
 
-def run_cg_program(workdir, input_txt, mask, psi, args=()):
+# Runs on their own geometry: name -> (geometry function, INPUT overrides).
+CG_GEOMETRY_RUNS = {
+    # mixture injection: initial phase from psi_mixture_ini with a 3-cell
+    # buffer and a wetting share of 0.6 next to the solid, constant phase on
+    # the x- face, no surface tension for x <= 4; reports every 25 steps,
+    # phase VTK every 50, checkpoints at the end
+    "cg_outputs_mix.npz": (cg_mix_geometry, dict(L3="16 12 12", L7=1, L15="0 1", L68=3, L69=0.6, L70=4,
+                                                  L27=25, L29=-1, L30=-1, L45=0)),
+}
+
+
+# Seed of oracle/mpishim/seeded_rand.h (LBM_FIXTURE_SEED): the colour-gradient
+# program built with it draws the random numbers that lbm_cg --seed draws.
+FIXTURE_SEED = 20261203
+
+# Runs of the seeded program build (ref_cg3_main_seeded): random initial
+# phase and random phase faces; name -> INPUT overrides.
+CG_SEEDED_RUNS = {
+    # random initial phase at ini_Sat = 0.45, random phase faces (flag 3) on
+    # x+ and y+, the initial phase on x-; phase VTK every 50 steps
+    "cg_outputs_rand.npz": dict(L7=1, L15="3 1", L16="3 0", L37=0.45, L29=-1, L30=-1, L45=0),
+    # random initial phase at ini_Sat = 0.6 with a partial window 3..10 on x
+    # and buffer phase +1 outside it (the sums limited to the window)
+    "cg_outputs_rand_buf.npz": dict(L37=0.6, L38=1, L40="1 0 0", L41="10 3", L29=-1, L30=-1, L45=0),
+    # imbibition control over 50 target saturations with random phase faces
+    # on both x faces (ini_Sat 0.9, random initial phase): the targets passed
+    # at the reports of steps 10, 20, 30 write the phase field and move the
+    # faces' threshold; reports every 10 steps
+    "cg_outputs_imb.npz": dict(L64="1 50", L7=1, L15="3 3", L37=0.9, L27=10, L29=-1, L30=-1, L45=0),
+    # drainage control, the phase faces turned on by the control itself
+    # (in_psi_BC = 0 in the file), ini_Sat 0.1
+    "cg_outputs_drain.npz": dict(L64="2 50", L7=0, L15="3 3", L37=0.1, L27=10, L29=-1, L30=-1, L45=0),
+}
+
+
+def run_cg_program(workdir, input_txt, mask, psi, args=(), seeded=False):
     import subprocess
 
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cg3_main")
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cg3_main_seeded" if seeded else "ref_cg3_main")
     G.write_ascii(os.path.join(workdir, "mask.dat"), mask)
     with open(os.path.join(workdir, "phase.dat"), "w") as f:
         f.write(phase_text(psi))
@@ -321,9 +369,11 @@ def collect_cg(workdir, prefix):
     return out
 
 
-def save_cg(fname, mask, psi, input_txt, files):
+def save_cg(fname, mask, psi, input_txt, files, seed=None):
     blob = {"mask": pack(mask), "shape": np.array(mask.shape), "phase": np.frombuffer(phase_text(psi).encode(), np.uint8),
             "input": np.frombuffer(input_txt.encode(), np.uint8), "names": np.array(sorted(files))}
+    if seed is not None:
+        blob["seed"] = np.array(seed, dtype=np.uint64)
     for k, v in files.items():
         blob[k] = np.frombuffer(v, np.uint8) if isinstance(v, bytes) else np.array(v)
     np.savez_compressed(os.path.join(HERE, fname), **blob)
@@ -357,6 +407,23 @@ def cg_program_outputs(only=None):
                 run_cg_program(d, rst, mask, psi, ("./out_",))
                 save_cg("cg_outputs_pre1_restart.npz", mask, psi, rst, collect_cg(d, "rst_"))
         save_cg(fname, mask, psi, text, files)
+    for fname, kv in CG_SEEDED_RUNS.items():
+        if only and only not in fname:
+            continue
+        text = cg_input_text(**kv)
+        with tempfile.TemporaryDirectory() as d:
+            run_cg_program(d, text, mask, psi, seeded=True)
+            files = collect_cg(d, "out_")
+        save_cg(fname, mask, psi, text, files, seed=FIXTURE_SEED)
+    for fname, (geometry, kv) in CG_GEOMETRY_RUNS.items():
+        if only and only not in fname:
+            continue
+        gmask, gpsi = geometry()
+        text = cg_input_text(**kv)
+        with tempfile.TemporaryDirectory() as d:
+            run_cg_program(d, text, gmask, gpsi)
+            files = collect_cg(d, "out_")
+        save_cg(fname, gmask, gpsi, text, files)
 
 
 def bc_cases():

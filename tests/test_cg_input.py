@@ -76,13 +76,13 @@ def test_phase_file_reads_as_float(L, tmp_path):
 @pytest.mark.parametrize("lines,field", [
     (dict(L9="2 1.0 0 1.0"), "pre_"),
     (dict(L13="0 0.0 2 0.0"), "vel_"),
-    (dict(L7=1, L15="2 0"), "psi_xp"),
-    (dict(L7=1, L17="0 3"), "psi_xp"),
-    (dict(L37=0.5), "ini_Sat"),
-    (dict(L68=3), "mix_psi_thickness"),
+    (dict(L7=1, L15="4 0"), "psi_xp"),
+    (dict(L7=1, L17="0 -1"), "psi_xp"),
+    (dict(L68=20), "mix_psi_thickness"),
     (dict(L33="1 1.0 2.0"), "lattice_v"),
     (dict(L22="1e-3 0 0"), "initial velocity"),
-    (dict(L64="1 5"), "rel_perm_id_dir"),
+    (dict(L64="3 5"), "rel_perm_id_dir"),
+    (dict(L64="1 0"), "rel_perm_id_dir"),
     (dict(L58="4 1 2000"), "pressure_change2"),
     (dict(L58="1 2 0"), "pressure_change2"),
     (dict(L66="1 1000"), "input_dynamic"),

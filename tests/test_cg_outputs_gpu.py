@@ -17,7 +17,21 @@ variants of INPUT_cg.dat on 14x12x10 spheres with a blob phase field:
   cg_outputs_vel*.npz    boundary_velocity) for every Sub_BC, with the
                          stabiliser, a pressure ramp and capillary-pressure
                          stepping of the face pressures, and a restart from
-                         the Sub_BC 1 run's step-100 checkpoint.
+                         the Sub_BC 1 run's step-100 checkpoint;
+  cg_outputs_mix.npz     mixture injection on 16x12x12 spheres: the initial
+                         phase of psi_mixture_ini (3-cell buffer, wetting
+                         share 0.6), constant phase on x-, no surface tension
+                         for x <= 4;
+  cg_outputs_psi2.npz    phase faces copying the +x neighbour (flag 2) on the
+                         x faces, y- and z+, the initial phase on y+;
+  cg_outputs_rand*.npz   random initial phase (ini_Sat), random phase faces
+                         (flag 3), and a window with a buffer phase, from the
+                         program built with its clock-seeded rand() replaced
+                         by the library's seeded generator (the fixture's
+                         seed is passed to lbm_cg --seed);
+  cg_outputs_imb.npz,    imbibition / drainage control (rel_perm_id_dir)
+  cg_outputs_drain.npz   over 50 target saturations with random phase faces,
+                         same seeded program.
 The driver, run on the same inputs at FP64, must write the same files: text
 and VTK byte for byte except the wall-clock lines of Results.txt, the
 checkpoints bit for bit (rows 1..).
@@ -93,11 +107,14 @@ FACES = ["cg_outputs_pre1.npz", "cg_outputs_pre2.npz", "cg_outputs_pre0.npz", "c
 
 
 @pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_sched.npz", "cg_outputs_ramp.npz",
-                                     "cg_outputs_psi.npz", "cg_outputs_cap.npz"] + FACES)
+                                     "cg_outputs_psi.npz", "cg_outputs_cap.npz", "cg_outputs_mix.npz",
+                                     "cg_outputs_psi2.npz", "cg_outputs_rand.npz", "cg_outputs_rand_buf.npz",
+                                     "cg_outputs_imb.npz", "cg_outputs_drain.npz"] + FACES)
 def test_cg_driver_writes_the_reference_files(L, fixture, tmp_path):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
-    run_driver(L, tmp_path)
+    seed = ("--seed", str(int(golden["seed"]))) if "seed" in golden.files else ()
+    run_driver(L, tmp_path, *seed)
     compare(tmp_path, golden, "out_")
 
 
@@ -113,7 +130,9 @@ def test_cg_driver_restart_matches_the_reference_restart(L, tmp_path, first_name
     compare(tmp_path, rst, "rst_")
 
 
-@pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_pre1.npz"])
+@pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_pre1.npz", "cg_outputs_pre0.npz",
+                                     "cg_outputs_pre2.npz", "cg_outputs_pre3.npz", "cg_outputs_vel1.npz",
+                                     "cg_outputs_vel2.npz", "cg_outputs_vel3.npz", "cg_outputs_mix.npz"])
 def test_cg_driver_f32_reports_match(L, tmp_path, fixture):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
