@@ -2,9 +2,15 @@
 
 Tolerances against the FP64 oracle (the reference colour-gradient solver):
   FP64 (LBM_PREC_F64)  bit-exact: f, u, rho, psi, rho_r, rho_b; reductions 1e-12
-  FP32                 |d psi| mean <= 1e-3, saturation within 2e-3,
-                       liquid permeability within 2e-2 relative (short runs;
-                       the interface dynamics amplify round-off over long ones)
+  FP32                 300 steps: |d psi| mean <= 1e-3, saturation within 5e-4
+                       (two nodes changing phase), liquid permeability within
+                       1e-3 relative (measured 1.1e-4); 2000 steps on 48^3:
+                       saturation 2e-4, liquid and gas permeability 2e-3
+                       (measured 3.0e-5, 4.4e-4, 1.5e-4).
+The two-phase flow amplifies any round-off difference: a 1e-12 relative
+change of the body force moves the FP64 liquid flux of the 128^3 workload by
+1e-4 after 20000 steps, so FP32 is held to bounds that grow with the length
+of the run rather than to one fixed bound.
 """
 import numpy as np
 import pytest
@@ -66,9 +72,30 @@ def test_cg_fp32_close_to_fp64_oracle(L, oracle_mod):
         d = s.fields()
         r = s.reduce()
     assert np.abs(d["psi"][1:] - rd["psi"][1:]).mean() <= 1e-3
-    assert abs(r["saturation"] - sat) <= 2e-3
-    assert abs(r["perm_l"][0] - pl[0]) <= 2e-2 * abs(pl[0])
+    assert abs(r["saturation"] - sat) <= 5e-4
+    assert abs(r["perm_l"][0] - pl[0]) <= 1e-3 * abs(pl[0])
     assert abs(r["mass"] - rd["rho"][1:].sum()) <= 1e-5 * s.count
+
+
+def test_cg_fp32_close_to_fp64_over_2000_steps(L):
+    """48^3 cylinders in the regime of the 128^3 workload, 2000 steps: FP32
+    against the FP64 kernel (bit-exact with the reference colour-gradient
+    solver, pinned by the tests above)."""
+    from lbm_b200 import geometry as G
+
+    mask = G.random_cylinders((48, 48, 48), 0.6, 3.0, seed=9)
+    psi = G.blob_phase_field(mask, seed=10, saturation=0.5)
+    kw = dict(nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0), body_force_phase=-1,
+              flux_psi=0.99, flux_umax=0.01)
+    out = {}
+    for prec in ("f64", "f32"):
+        with L.ColourGradient(mask, psi, precision=prec, **kw) as s:
+            s.step(2000)
+            out[prec] = s.reduce()
+    a, b = out["f64"], out["f32"]
+    assert abs(b["saturation"] - a["saturation"]) <= 2e-4 * a["saturation"]
+    assert abs(b["perm_l"][0] - a["perm_l"][0]) <= 2e-3 * abs(a["perm_l"][0])
+    assert abs(b["perm_g"][0] - a["perm_g"][0]) <= 2e-3 * abs(a["perm_g"][0])
 
 
 def test_cg_fp64_matches_oracle_over_longer_run(L, oracle_mod):
