@@ -22,26 +22,28 @@
 namespace lbm {
 
 // Work item = BS nodes of a stepping tile (the tiles in the active list
-// order, kTile / BS items per tile).  The grid strides over the items; tile
-// constants come from the list kernel's TileWork record, so the population
-// gathers of an item wait on a single broadcast load, as in the
-// single-domain step.  The host sizes the grid per chain to the stepping
-// tile count (at most eight waves of resident blocks), so idle pool capacity
-// launches no blocks.
+// order, kTile / BS items per tile); block b takes item b.  The host launches
+// at least as many blocks as there are stepping items (a power of two at or
+// above their count, chain_grid), and the list kernel fills the entries past
+// the stepping tiles with an empty node range, so a block needs no count of
+// the stepping tiles: its population gathers wait on the single broadcast
+// load of its own entry (the single-domain step waits on none), and the
+// blocks past the list read an empty entry and exit.
 template <Store K, int BS>
 __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
   using T = typename Traits<K>::T;
   using A = typename Traits<K>::A;
   constexpr int kSub = kTile / BS;
-  const int items = *a.n_active * kSub;
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
   const size_t cap = (size_t)a.cap;
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+  {
+    const int it = blockIdx.x;
     const int i = it / kSub;
+    if (i >= a.ntiles) return;
     const TileWork w = a.work[i];
     const int p = w.p0 + (it - i * kSub) * BS + threadIdx.x;
-    if (p >= w.end) continue;
+    if (p >= w.end) return;
     const float scale = w.fp16_scale, inv_scale = 1.0f / w.fp16_scale;
     A f[kQ];
     f[0] = load_pop<K>(src + p, inv_scale);
@@ -105,6 +107,9 @@ __global__ void __launch_bounds__(1024) batch_list_kernel(BatchReduceArgs a) {
     }
   }
   if (threadIdx.x == 1023) *a.n_active = counts[1023];
+  // entries past the stepping tiles: an empty node range (p0 = end = 0)
+  TileWork none{};
+  for (int e = counts[1023] + threadIdx.x; e < a.ntiles; e += 1024) a.work[e] = none;
 }
 
 cudaError_t launch_batch_list(const BatchReduceArgs& a, cudaStream_t st) {
@@ -255,20 +260,12 @@ static cudaError_t step_k(const BatchStepArgs& a, int block, int grid, int chain
 }
 
 int batch_step_grid(int ntiles, int block) {
+  // one block per work item of the whole pool: with every tile stepping no
+  // block loops (each item's gathers wait only on its own list entry); the
+  // chains of a partly stepping pool launch a power of two at or above their
+  // item count (chain_grid), the extra blocks find no item and exit
   const int b = (block == 128 || block == 512) ? block : 256;
-  int dev = 0, sms = 148, per = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e;
-  if (b == 128)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 128>, 128, 0);
-  else if (b == 512)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 512>, 512, 0);
-  else
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_step_kernel<Store::F32, 256>, 256, 0);
-  if (e != cudaSuccess || per < 1) per = 1;
-  const long long waves = 8LL * sms * per, items = (long long)ntiles * (kTile / b);
-  return (int)std::max(1LL, std::min(waves, items));
+  return (int)std::max(1LL, (long long)ntiles * (kTile / b));
 }
 
 cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int grid, int chain_step,
