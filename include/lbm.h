@@ -483,6 +483,15 @@ typedef struct lbm_cg_input {
 } lbm_cg_input;
 
 LBM_API lbm_status lbm_read_cg_input(const char* path, lbm_cg_input* out);
+/* input_update (CG3:5765-5925, every update_fre steps when input_dynamic > 0,
+ * after the step's collision and ramps, CG3:859-861): the handle-side values
+ * of a re-read INPUT file, that is the wall colour (contact_angle), CapA, the
+ * flux thresholds (rel_perm_psi, rel_perm_psi2) from the next collision on,
+ * and the body force gx, gy, gz from this step's macro step on
+ * (LBM_CG_FORCE_BEFORE_MACRO).  n_max, the output intervals and the
+ * single-phase permeability are the caller's (the lbm_cg driver re-reads the
+ * file with lbm_read_cg_input and takes those too). */
+LBM_API lbm_status lbm_cg_input_update(lbm_cg_handle* h, const lbm_cg_input* in);
 /* Phase file (CG3:2130-2150): nx*ny*nz whitespace-separated numbers, x
  * fastest, each read as float; out [nz][ny][nx]. */
 LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, double* out);
@@ -540,16 +549,30 @@ LBM_API lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, 
  * flow -> solute coupling of SP:5093-5120 / ST7:3640-3667 without files). */
 LBM_API lbm_status lbm_st7_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
                                             lbm_st7_handle** out);
+/* The D3Q19 solute program (ST19 = Single_Phase_3D/
+ * Solute_Transport_MPI_Software_Spars.cpp; collision ST19:1346-1640): BGK on
+ * the 19 flow directions towards w_q C (1 + 3 e.u + 4.5 (e.u)^2 - 1.5 u.u),
+ * C = sum of the 19 g in the program's direction order (ST19:121-127, the
+ * colour-gradient order).  Same arguments and handle as lbm_st7_create; the
+ * lbm_st7_* calls below work on it, with 19 columns for populations. */
+LBM_API lbm_status lbm_st19_create(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz,
+                                   const double* u_nodes, const double* c0, lbm_st7_handle** out);
+LBM_API lbm_status lbm_st19_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
+                                             lbm_st7_handle** out);
+/* Directions of a solute handle: 7 (lbm_st7_create*) or 19 (lbm_st19_create*);
+ * 0 for a null handle. */
+LBM_API int lbm_st7_directions(lbm_st7_handle* h);
 /* collision + streaming + C = sum g (ST7:1345-1633), n times */
 LBM_API lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps);
 /* C per fluid node [(count+1)], reference id order, row 0 zero */
 LBM_API lbm_status lbm_st7_get_concentration(lbm_st7_handle* h, double* c);
 LBM_API lbm_status lbm_st7_info(lbm_st7_handle* h, int* count, long long* step, double* last_step_ms);
 /* g as the next step reads it (the reference's fg after comput_macro_variables,
- * ST7:1619-1633): [(count+1)*7] in reference id order, column 0 and row 0 zero */
+ * ST7:1619-1633): [(count+1)*7] in reference id order, column 0 and row 0 zero;
+ * for a D3Q19 handle [(count+1)*19] in the program's direction order */
 LBM_API lbm_status lbm_st7_get_populations(lbm_st7_handle* h, double* g);
-/* Restores g [(count+1)*7] and C [(count+1)] like Backup_init (ST7:3716-3802);
- * the next step takes C as given */
+/* Restores g [(count+1)*7] ([(count+1)*19] for D3Q19) and C [(count+1)] like
+ * Backup_init (ST7:3716-3802); the next step takes C as given */
 LBM_API lbm_status lbm_st7_set_state(lbm_st7_handle* h, const double* g, const double* c);
 
 /* INPUT file of the solute program (ST7:219-280, field order and types kept;

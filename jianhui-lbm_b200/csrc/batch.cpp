@@ -110,7 +110,7 @@ struct Pool {
   int block = 256, grid = 0;
   int ordering = LBM_ORDER_REFERENCE;
   double fp16_scale = 1.0;
-  Buf pop[2], table, tile_inst, inst, state, partials, active_tiles, n_active, work;
+  Buf pop[2], table, tile_inst, inst, state, partials, active_tiles, n_active, work, slot_off;
   SetupScratch setup;
   std::vector<InstParams> h_inst;
   InstState* h_state = nullptr;  // pinned
@@ -182,6 +182,7 @@ struct Pool {
     LBM_CUDA_TRY(partials.alloc((size_t)ntiles * 8 * sizeof(double)));
     LBM_CUDA_TRY(active_tiles.alloc((size_t)ntiles * sizeof(int)));
     LBM_CUDA_TRY(work.alloc((size_t)ntiles * sizeof(TileWork)));
+    LBM_CUDA_TRY(slot_off.alloc((size_t)(nslots + 1) * sizeof(int)));
     LBM_CUDA_TRY(n_active.alloc(sizeof(int)));
     LBM_CUDA_TRY(cudaMemsetAsync(n_active.p, 0, sizeof(int), stream));
     LBM_CUDA_TRY(cudaMallocHost((void**)&h_state, (size_t)nslots * sizeof(InstState)));
@@ -330,6 +331,7 @@ struct Pool {
     r.active_tiles = active_tiles.as<int>();
     r.n_active = n_active.as<int>();
     r.work = work.as<TileWork>();
+    r.slot_off = slot_off.as<int>();
     return r;
   }
 
@@ -338,7 +340,7 @@ struct Pool {
     LBM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     // the chain starts from the current set of stepping slots (admissions and
     // retirements happen between chains)
-    cudaError_t err = launch_batch_list(reduce_args(c0), stream);
+    cudaError_t err = launch_batch_list(reduce_args(c0), step_grid, block, stream);
     int c = c0;
     for (int s = 0; s < chain && err == cudaSuccess; s++) {
       err = launch_batch_step(kind, step_args(c), block, step_grid, s, stream);
@@ -649,7 +651,7 @@ lbm_status lbm_batch_autotune(lbm_batch* b, int trial_steps, int* ordering_out, 
       P.block = bl;
       P.grid = batch_step_grid(P.ntiles, bl);
       if ((st = batch_reset(b)) != LBM_OK) return st;
-      LBM_CUDA_TRY(launch_batch_list(P.reduce_args(P.cur), P.stream));
+      LBM_CUDA_TRY(launch_batch_list(P.reduce_args(P.cur), P.grid, P.block, P.stream));
       for (int s = 0; s < 2; s++) {  // warm-up
         LBM_CUDA_TRY(launch_batch_step(P.kind, P.step_args(P.cur), P.block, P.grid, s, P.stream));
         P.cur = 1 - P.cur;

@@ -51,7 +51,7 @@ struct BatchStepArgs {
   const int* tile_inst;
   const InstParams* inst;
   const InstState* state;
-  const int* active_tiles;  // tiles of stepping slots, ascending
+  const int* active_tiles;  // tiles of stepping slots, slot by slot
   const int* n_active;      // its length (device scalar)
   const TileWork* work;     // [n_active] per stepping tile
 };
@@ -69,10 +69,12 @@ struct BatchReduceArgs {
   int* active_tiles;
   int* n_active;
   TileWork* work;
+  int* slot_off;  // [nslots + 1] first list entry of each slot's stepping tiles
 };
 
-// Rebuilds the active tile list from tile ownership and slot states.
-cudaError_t launch_batch_list(const BatchReduceArgs& a, cudaStream_t st);
+// Rebuilds the work list from the slot states: the stepping slots' tiles,
+// then empty entries up to the tiles a step grid of step_grid blocks covers.
+cudaError_t launch_batch_list(const BatchReduceArgs& a, int step_grid, int block, cudaStream_t st);
 
 cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int grid, int chain_step,
                               cudaStream_t st);

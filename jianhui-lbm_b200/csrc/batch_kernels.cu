@@ -5,11 +5,11 @@
 // [18][cap] whose entries are flat indices q*cap + m into the same pool (an
 // instance only ever pulls from its own range).  The pool is cut into tiles
 // of kTile nodes; tile_inst[t] names the instance slot owning tile t (-1 =
-// free).  At the start of every chain a list kernel compacts the tiles of
-// stepping slots into a work list (with each tile's constants); the step
-// kernel strides over that list, so any grid is correct and the captured
-// CUDA graph of a chain only depends on the grid the host picks for the
-// stepping tile count (one graph per power of two).
+// free).  At the start of every chain the list kernels compact the tiles of
+// stepping slots into a work list (with each tile's constants); a step block
+// takes one work item, the host launches at least one block per stepping
+// item, and the captured CUDA graph of a chain only depends on the grid the
+// host picks for the stepping tile count (one graph per power of two).
 //
 // Convergence is decided on the device: every chain of check_every steps ends
 // with a per-tile sum of u, a per-instance sum of its tiles in fixed order
@@ -24,7 +24,7 @@ namespace lbm {
 // Work item = BS nodes of a stepping tile (the tiles in the active list
 // order, kTile / BS items per tile); block b takes item b.  The host launches
 // at least as many blocks as there are stepping items (a power of two at or
-// above their count, chain_grid), and the list kernel fills the entries past
+// above their count, chain_grid), and the list kernels fill the entries past
 // the stepping tiles with an empty node range, so a block needs no count of
 // the stepping tiles: its population gathers wait on the single broadcast
 // load of its own entry (the single-domain step waits on none), and the
@@ -67,16 +67,23 @@ __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int cha
   }
 }
 
-// Active tile list: one block scans tile ownership in index order.
-__global__ void __launch_bounds__(1024) batch_list_kernel(BatchReduceArgs a) {
+// Work list of a chain, in two launches whose cost follows the slots and the
+// stepping tiles, not the pool size.  (1) One block: the stepping tile count
+// of every slot, its exclusive scan into slot_off[0..nslots] (slot order) and
+// n_active.  (2) Entry e of the list: the slot whose offset range holds e
+// (binary search of slot_off), that slot's tile e - slot_off[s] with its
+// constants; entries past the stepping tiles, up to the tiles the chain grid
+// covers, get an empty node range (p0 = end = 0).
+__device__ __forceinline__ int stepping_tiles(const BatchReduceArgs& a, int s) {
+  return a.state[s].active ? a.inst[s].tile_end - a.inst[s].tile_begin : 0;
+}
+
+__global__ void __launch_bounds__(1024) batch_slot_scan_kernel(BatchReduceArgs a) {
   __shared__ int counts[1024];
-  const int chunk = (a.ntiles + 1023) / 1024;
-  const int lo = threadIdx.x * chunk, hi = min(lo + chunk, a.ntiles);
+  const int chunk = (a.nslots + 1023) / 1024;
+  const int lo = min((int)threadIdx.x * chunk, a.nslots), hi = min(lo + chunk, a.nslots);
   int c = 0;
-  for (int t = lo; t < hi; t++) {
-    const int s = a.tile_inst[t];
-    c += (s >= 0 && a.state[s].active);
-  }
+  for (int s = lo; s < hi; s++) c += stepping_tiles(a, s);
   counts[threadIdx.x] = c;
   __syncthreads();
   // inclusive scan (Hillis-Steele)
@@ -87,11 +94,34 @@ __global__ void __launch_bounds__(1024) batch_list_kernel(BatchReduceArgs a) {
     __syncthreads();
   }
   int w = counts[threadIdx.x] - c;
-  for (int t = lo; t < hi; t++) {
-    const int s = a.tile_inst[t];
-    if (s >= 0 && a.state[s].active) {
-      const InstParams& ip = a.inst[s];
-      TileWork tw;
+  for (int s = lo; s < hi; s++) {
+    a.slot_off[s] = w;
+    w += stepping_tiles(a, s);
+  }
+  if (threadIdx.x == 1023) {
+    a.slot_off[a.nslots] = counts[1023];
+    *a.n_active = counts[1023];
+  }
+}
+
+__global__ void __launch_bounds__(256) batch_work_kernel(BatchReduceArgs a, int fill_to) {
+  const int total = a.slot_off[a.nslots];
+  const int n = max(total, fill_to);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    TileWork tw{};
+    if (e < total) {
+      // the last slot whose offset is <= e (slots without stepping tiles
+      // share their offset with the next slot and are passed over)
+      int lo = 0, hi = a.nslots - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.slot_off[mid] <= e)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      const InstParams& ip = a.inst[lo];
+      const int t = ip.tile_begin + (e - a.slot_off[lo]);
       tw.p0 = t * kTile;
       tw.end = ip.end;
       for (int d = 0; d < 3; d++) {
@@ -101,19 +131,20 @@ __global__ void __launch_bounds__(1024) batch_list_kernel(BatchReduceArgs a) {
       tw.s_v = ip.s_v;
       tw.s_o = ip.s_o;
       tw.fp16_scale = ip.fp16_scale;
-      tw.fresh = a.state[s].fresh;
-      a.work[w] = tw;
-      a.active_tiles[w++] = t;
+      tw.fresh = a.state[lo].fresh;
+      a.active_tiles[e] = t;
     }
+    a.work[e] = tw;
   }
-  if (threadIdx.x == 1023) *a.n_active = counts[1023];
-  // entries past the stepping tiles: an empty node range (p0 = end = 0)
-  TileWork none{};
-  for (int e = counts[1023] + threadIdx.x; e < a.ntiles; e += 1024) a.work[e] = none;
 }
 
-cudaError_t launch_batch_list(const BatchReduceArgs& a, cudaStream_t st) {
-  batch_list_kernel<<<1, 1024, 0, st>>>(a);
+cudaError_t launch_batch_list(const BatchReduceArgs& a, int step_grid, int block, cudaStream_t st) {
+  const int b = (block == 128 || block == 512) ? block : 256;
+  const int per_tile = kTile / b;
+  const int fill_to = std::min(a.ntiles, (step_grid + per_tile - 1) / per_tile);
+  batch_slot_scan_kernel<<<1, 1024, 0, st>>>(a);
+  const int g = std::max(1, std::min((fill_to + 255) / 256, 4 * 148));
+  batch_work_kernel<<<g, 256, 0, st>>>(a, fill_to);
   return cudaGetLastError();
 }
 

@@ -689,6 +689,20 @@ lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a) {
   return LBM_OK;
 }
 
+lbm_status lbm_cg_input_update(lbm_cg_handle* h, const lbm_cg_input* in) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (!in) return fail(LBM_ERR_ARG, "lbm_cg_input_update: null input");
+  // input_update (CG3:5765-5925): the wall colour, CapA and the flux
+  // thresholds from the next collision on; gxs = gx already for this step's
+  // macro step, like a ramp
+  h->cp.psi_solid = h->prm.psi_solid = in->contact_angle;
+  h->cp.cap_a = h->prm.cap_a = in->cap_a;
+  h->cp.flux_psi = h->prm.flux_psi = in->rel_perm_psi;
+  h->prm.flux_umax = in->rel_perm_psi2;
+  return lbm_cg_set_body_force(h, in->gx, in->gy, in->gz, LBM_CG_FORCE_BEFORE_MACRO);
+}
+
 lbm_status lbm_cg_set_window(lbm_cg_handle* h, const int window[6], int restrict_nodes) {
   lbm_status st = cg_check(h);
   if (st != LBM_OK) return st;
@@ -1015,6 +1029,8 @@ lbm_status lbm_cg_create_from_input_seeded(const char* input_path, int precision
     return fail(LBM_ERR_ARG, "rel_perm_id_dir: 0 (off), 1 (imbibition) or 2 (drainage)");
   if (in.rel_perm_id_dir > 0 && in.rel_perm_chan_num <= 0)
     return fail(LBM_ERR_ARG, "rel_perm_id_dir: rel_perm_chan_num must be positive");
+  if (in.input_dynamic > 0 && in.update_fre <= 0)
+    return fail(LBM_ERR_ARG, "input_dynamic: the update interval must be positive (the reference takes n % update_fre)");
   // the imbibition / drainage control turns the phase faces on in init
   // (CG3:2339-2345); a restart (Backup_init) skips it
   if (in.rel_perm_id_dir > 0 && in.mode_backup_ini == 0) in.in_psi_bc = 1;
@@ -1022,7 +1038,6 @@ lbm_status lbm_cg_create_from_input_seeded(const char* input_path, int precision
     return fail(LBM_ERR_ARG, "pressure_change2: the capillary-pressure axis is 0 (off) or 1..3");
   if (in.pressure_change2 > 0 && (in.chan_no <= 0 || in.interval_pre <= 0))
     return fail(LBM_ERR_ARG, "pressure_change2: chan_no and interval_pre must be positive");
-  if (in.input_dynamic != 0) return fail(LBM_ERR_ARG, "input_dynamic: dynamic input update is not supported");
   if (in.fre_re <= 0) return fail(LBM_ERR_ARG, "freRe must be positive");
   if (in.fre_psi == 0) return fail(LBM_ERR_ARG, "frePsi = 0: the reference takes n % 0; use -1 or a positive interval");
   if (in.least_square > 0 && in.num_least_square < 2)

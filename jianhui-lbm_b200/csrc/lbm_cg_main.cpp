@@ -15,9 +15,12 @@
 // ramps of pressure_change (pressure_bodyforce_change, CG3:1252-1420), the
 // surface-tension change of rel_perm_ift (CG3:892-893) and the least-squares
 // fit of the relative permeabilities (Least_Square_Rel_Perm, CG3:1201-1250)
-// and the capillary-pressure stepping (pressure_capillary, CG3:1427-1600).
+// and the capillary-pressure stepping (pressure_capillary, CG3:1427-1600),
+// and with input_dynamic the INPUT file read again every update_fre steps
+// (input_update, CG3:859-861, 5765-5925).
 // Pressure and velocity faces (boundary_pressure / boundary_velocity,
 // CG3:868-876) follow the face densities these schedules move.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -263,7 +266,7 @@ int main(int argc, char** argv) {
   { std::ofstream(f_rel2, std::ios::out); }
   { std::ofstream(f_vel, std::ios::out); }
 
-  const double rk = in.reso * in.reso * 1000 / in.permeability;  // lattice permeability -> relative
+  double rk = in.reso * in.reso * 1000 / in.permeability;  // lattice permeability -> relative
   const double dt = 1.0, dx = 1.0;
   const int NY1 = ny;  // NY + 1
   const bool stab = in.stab == 1;
@@ -390,6 +393,7 @@ int main(int argc, char** argv) {
       last = ((n + in.fre_re - 1) / in.fre_re) * in.fre_re;
       if (last > in.n_max) last = in.n_max;
       if (stab && in.stab_time > n && in.stab_time - 1 < last) last = in.stab_time - 1;
+      if (in.input_dynamic > 0) last = std::min(last, ((n + in.update_fre - 1) / in.update_fre) * in.update_fre);
       for (long long k = n + 1; k <= last; k++)
         if (ramp_at(in, k) || cap.ramping(in, k)) {
           last = k - 1;
@@ -405,6 +409,28 @@ int main(int argc, char** argv) {
     if ((moved || moved2) &&
         lbm_cg_set_body_force(h, drv.g[0], drv.g[1], drv.g[2], LBM_CG_FORCE_BEFORE_MACRO) != LBM_OK)
       return die("lbm_cg_set_body_force");
+    if (in.input_dynamic > 0 && n % in.update_fre == 0) {
+      // input_update (CG3:859-861, 5765-5925): the file read again; n_max,
+      // the body force (gx = gxs), wall colour, CapA, permeability, report
+      // and output intervals and the flux thresholds take its values
+      lbm_cg_input up;
+      if (lbm_read_cg_input(argv[1], &up) != LBM_OK) return die("lbm_read_cg_input (input update)");
+      in.n_max = up.n_max;
+      gbase[0] = drv.g[0] = in.gx = up.gx;
+      gbase[1] = drv.g[1] = in.gy = up.gy;
+      gbase[2] = drv.g[2] = in.gz = up.gz;
+      in.contact_angle = up.contact_angle;
+      cap_a = in.cap_a = up.cap_a;
+      in.permeability = up.permeability;
+      rk = in.reso * in.reso * 1000 / in.permeability;
+      in.fre_re = up.fre_re;
+      in.fre_ve = up.fre_ve;
+      in.fre_de = up.fre_de;
+      in.fre_psi = up.fre_psi;
+      in.rel_perm_psi = up.rel_perm_psi;
+      in.rel_perm_psi2 = up.rel_perm_psi2;
+      if (lbm_cg_input_update(h, &in) != LBM_OK) return die("lbm_cg_input_update");
+    }
     if (!sync_faces(false)) return die("lbm_cg_set_faces");
     if (n % in.fre_re != 0) {
       n++;

@@ -1,6 +1,9 @@
 // lbm_st7 -- drop-in driver for the D3Q7 solute (passive scalar) solver.
 //
-//   lbm_st7 INPUT.dat [prefix] [--ranks N] [--precision f64|f32]
+//   lbm_st7 INPUT.dat [prefix] [--ranks N] [--precision f64|f32] [--lattice 7|19]
+// (--lattice 19: the D3Q19 solute program, Solute_Transport_MPI_Software_
+// Spars.cpp, "ST19": the same program with the 19-velocity lattice, 19
+// columns in its g checkpoints, and bodyforce.txt emptied at start)
 //
 // Runs the time loop of Single_Phase_3D/Solute_Transport_MPI_Software_Spars_6V.cpp
 // (main, ST7:187-730) on one GPU through liblbm.so.  The reference is an
@@ -87,21 +90,25 @@ struct Slabs {
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::cerr << "usage: lbm_st7 INPUT.dat [prefix] [--ranks N] [--precision f64|f32]" << std::endl;
+    std::cerr << "usage: lbm_st7 INPUT.dat [prefix] [--ranks N] [--precision f64|f32] [--lattice 7|19]" << std::endl;
     return 2;
   }
   std::string pfix = "./";
-  int precision = LBM_PREC_F64, nranks = 1;
+  int precision = LBM_PREC_F64, nranks = 1, lattice = 7;
   for (int a = 2; a < argc; a++) {
     const std::string s = argv[a];
     if (s == "--precision" && a + 1 < argc)
       precision = std::string(argv[++a]) == "f32" ? LBM_PREC_F32 : LBM_PREC_F64;
     else if (s == "--ranks" && a + 1 < argc)
       nranks = std::atoi(argv[++a]);
+    else if (s == "--lattice" && a + 1 < argc)
+      lattice = std::atoi(argv[++a]);
     else if (a == 2)
       pfix = s;
   }
   if (nranks < 1) return die_msg("--ranks must be at least 1");
+  if (lattice != 7 && lattice != 19) return die_msg("--lattice is 7 or 19");
+  const int W = lattice;  // columns of a g checkpoint row
   Clock clock;
   lbm_st7_input in;
   if (lbm_read_st7_input(argv[1], &in) != LBM_OK) return die("lbm_read_st7_input");
@@ -153,23 +160,25 @@ int main(int argc, char** argv) {
   p.precision = precision;
   p.device = 0;
   lbm_st7_handle* h = nullptr;
-  if (lbm_st7_create(&p, mask.data(), nx, ny, nz, u.data(), c0.data(), &h) != LBM_OK) return die("lbm_st7_create");
+  if ((lattice == 19 ? lbm_st19_create(&p, mask.data(), nx, ny, nz, u.data(), c0.data(), &h)
+                     : lbm_st7_create(&p, mask.data(), nx, ny, nz, u.data(), c0.data(), &h)) != LBM_OK)
+    return die("lbm_st7_create");
   if (in.mode_backup_ini != 0) {
     // Backup_init reads LBM_checkpoint_{psi,fg}_<m>.<rank>.bin_input from the
     // working directory, without the output prefix (ST7:3735-3740)
-    std::vector<double> c((size_t)count + 1, 0.0), g((size_t)(count + 1) * 7, 0.0);
+    std::vector<double> c((size_t)count + 1, 0.0), g((size_t)(count + 1) * W, 0.0);
     for (int r = 0; r < nranks; r++) {
       const size_t nr = sl.ids[r].size();
       std::ostringstream n3, n5;
       n3 << "LBM_checkpoint_psi_" << in.mode_backup_ini << "." << r << ".bin_input";
       n5 << "LBM_checkpoint_fg_" << in.mode_backup_ini << "." << r << ".bin_input";
-      std::vector<double> pr(nr + 1), gr((nr + 1) * 7);
+      std::vector<double> pr(nr + 1), gr((nr + 1) * W);
       if (!read_doubles(n3.str(), pr.data(), pr.size())) return die_msg("file open error on" + n3.str());
       if (!read_doubles(n5.str(), gr.data(), gr.size())) return die_msg("file open error on" + n5.str());
       for (size_t s = 0; s < nr; s++) {
         const int32_t id = sl.ids[r][s];
         c[id] = pr[s + 1];
-        for (int q = 0; q < 7; q++) g[(size_t)id * 7 + q] = gr[(s + 1) * 7 + q];
+        for (int q = 0; q < W; q++) g[(size_t)id * W + q] = gr[(s + 1) * W + q];
       }
     }
     if (lbm_st7_set_state(h, g.data(), c.data()) != LBM_OK) return die("lbm_st7_set_state");
@@ -211,6 +220,9 @@ int main(int argc, char** argv) {
   }
   const std::string f_res = out + "Results_solute.txt";
   { std::ofstream(f_res, std::ios::trunc); }
+  // the D3Q19 program empties bodyforce.txt at start (ST19:518), the D3Q7 one
+  // only appends to it
+  if (lattice == 19) std::ofstream(out + "bodyforce.txt", std::ios::trunc);
 
   // Error (ST7:2159-2233) on the fixed velocity: every rank skips its last
   // node (its loop stops at Count - 1); rank sums are added in rank order
@@ -386,15 +398,15 @@ int main(int argc, char** argv) {
       }
     }
     if (in.fre_backup >= 0 && n % in.fre_backup == 0 && n > 0) {
-      std::vector<double> g((size_t)(count + 1) * 7);
+      std::vector<double> g((size_t)(count + 1) * W);
       if (lbm_st7_get_populations(h, g.data()) != LBM_OK) return die("lbm_st7_get_populations");
       for (int r = 0; r < nranks; r++) {
         const size_t nr = sl.ids[r].size();
-        std::vector<double> pr(nr + 1, 0.0), gr((nr + 1) * 7, 0.0);
+        std::vector<double> pr(nr + 1, 0.0), gr((nr + 1) * W, 0.0);
         for (size_t s = 0; s < nr; s++) {
           const int32_t id = sl.ids[r][s];
           pr[s + 1] = conc[id];
-          for (int q = 0; q < 7; q++) gr[(s + 1) * 7 + q] = g[(size_t)id * 7 + q];
+          for (int q = 0; q < W; q++) gr[(s + 1) * W + q] = g[(size_t)id * W + q];
         }
         std::ostringstream n3, n5;
         n3 << out << "LBM_checkpoint_psi_" << n << "." << r << ".bin_input";

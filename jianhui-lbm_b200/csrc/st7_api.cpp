@@ -58,6 +58,7 @@ struct lbm_st7_handle {
   long long step = 0;
   double tau_s = 1.0;
   double last_ms = 0;
+  int nq = 7;  // 7: D3Q7 solute program, 19: D3Q19 solute program
   ~lbm_st7_handle() {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -77,6 +78,7 @@ St7Args st7_args(lbm_st7_handle* h, bool given) {
   a.n = h->geo.count;
   a.npad = h->geo.npad;
   a.tau_s = h->tau_s;
+  a.nq = h->nq;
   return a;
 }
 
@@ -99,10 +101,10 @@ lbm_status upload_as(lbm_st7_handle* h, Mem& m, const std::vector<double>& v) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz, const double* u_nodes,
-                          const double* c0, lbm_st7_handle** out) {
+lbm_status create_solute(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz, const double* u_nodes,
+                         const double* c0, int nq, lbm_st7_handle** out) {
   if (!p || !mask || !u_nodes || !c0 || !out || nx <= 0 || ny <= 0 || nz <= 0)
     return fail(LBM_ERR_ARG, "lbm_st7_create: bad argument");
   *out = nullptr;
@@ -113,6 +115,7 @@ lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, 
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LBM_ERR_NO_DEVICE, "no CUDA device");
   auto h = std::make_unique<lbm_st7_handle>();
   h->prm = *p;
+  h->nq = nq;
   h->f64 = p->precision == LBM_PREC_F64;
   h->device = p->device;
   const double c_s2 = 1.0 * 1.0 / 3, dt = 1.0;
@@ -128,7 +131,8 @@ lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, 
   build_pull_table(mask, &g);
   const int n = g.count, npad = g.npad;
   const size_t s = h->f64 ? 8 : 4;
-  for (auto& b : h->g) LBM_CUDA_TRY(b.alloc((size_t)6 * npad * s));
+  const int rows = nq == kQ ? kQ : 6;  // D3Q7 keeps only directions 1..6
+  for (auto& b : h->g) LBM_CUDA_TRY(b.alloc((size_t)rows * npad * s));
   LBM_CUDA_TRY(h->table.alloc((size_t)18 * npad * sizeof(int32_t)));
   LBM_CUDA_TRY(h->u.alloc((size_t)3 * npad * s));
   LBM_CUDA_TRY(h->c0.alloc((size_t)npad * s));
@@ -156,8 +160,8 @@ lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, 
   return LBM_OK;
 }
 
-lbm_status lbm_st7_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
-                                    lbm_st7_handle** out) {
+lbm_status create_solute_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0, int nq,
+                                   lbm_st7_handle** out) {
   if (!flow) return fail(LBM_ERR_ARG, "lbm_st7_create_from_flow: null flow handle");
   int count = 0;
   double por = 0;
@@ -168,8 +172,34 @@ lbm_status lbm_st7_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, c
   if ((st = lbm_get_fields(flow, nullptr, u.data())) != LBM_OK) return st;
   int nx, ny, nz;
   const uint8_t* mask = lbm_internal_mask(flow, &nx, &ny, &nz);
-  return lbm_st7_create(p, mask, nx, ny, nz, u.data(), c0, out);
+  return create_solute(p, mask, nx, ny, nz, u.data(), c0, nq, out);
 }
+
+}  // namespace
+
+extern "C" {
+
+lbm_status lbm_st7_create(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz, const double* u_nodes,
+                          const double* c0, lbm_st7_handle** out) {
+  return create_solute(p, mask, nx, ny, nz, u_nodes, c0, 7, out);
+}
+
+lbm_status lbm_st7_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
+                                    lbm_st7_handle** out) {
+  return create_solute_from_flow(p, flow, c0, 7, out);
+}
+
+lbm_status lbm_st19_create(const lbm_st7_params* p, const uint8_t* mask, int nx, int ny, int nz, const double* u_nodes,
+                           const double* c0, lbm_st7_handle** out) {
+  return create_solute(p, mask, nx, ny, nz, u_nodes, c0, kQ, out);
+}
+
+lbm_status lbm_st19_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, const double* c0,
+                                     lbm_st7_handle** out) {
+  return create_solute_from_flow(p, flow, c0, kQ, out);
+}
+
+int lbm_st7_directions(lbm_st7_handle* h) { return h ? h->nq : 0; }
 
 lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps) {
   if (!h || nsteps < 0) return fail(LBM_ERR_ARG, "lbm_st7_step: bad argument");
@@ -209,7 +239,7 @@ lbm_status lbm_st7_get_populations(lbm_st7_handle* h, double* g) {
   LBM_CUDA_TRY(cudaSetDevice(h->device));
   const int n = h->geo.count;
   Mem out;
-  const size_t bytes = sizeof(double) * (size_t)(n + 1) * 7;
+  const size_t bytes = sizeof(double) * (size_t)(n + 1) * h->nq;
   LBM_CUDA_TRY(out.alloc(bytes));
   LBM_CUDA_TRY(cudaMemsetAsync(out.p, 0, bytes, h->stream));
   LBM_CUDA_TRY(st7_launch_export(h->f64, st7_args(h, false), static_cast<const int32_t*>(h->ref_of.p),
@@ -224,7 +254,7 @@ lbm_status lbm_st7_set_state(lbm_st7_handle* h, const double* g, const double* c
   LBM_CUDA_TRY(cudaSetDevice(h->device));
   const int n = h->geo.count, npad = h->geo.npad;
   Mem in;
-  const size_t bytes = sizeof(double) * (size_t)(n + 1) * 7;
+  const size_t bytes = sizeof(double) * (size_t)(n + 1) * h->nq;
   LBM_CUDA_TRY(in.alloc(bytes));
   LBM_CUDA_TRY(cudaMemcpyAsync(in.p, g, bytes, cudaMemcpyHostToDevice, h->stream));
   St7Args a = st7_args(h, true);

@@ -14,10 +14,12 @@ struct St7Args {
   void* c_out;            // optional [npad]: C of this step's macro
   int n, npad;
   double tau_s;
+  int nq;                 // 7 (D3Q7, g as [6][npad]) or 19 (D3Q19, g as [19][npad])
 };
 
 cudaError_t st7_launch_step(bool f64, const St7Args& a, cudaStream_t st);
 cudaError_t st7_launch_step_f64(const St7Args& a, cudaStream_t st);  // st7_faithful.cu, -fmad=false
+cudaError_t st19_launch_step_f64(const St7Args& a, cudaStream_t st);  // st7_faithful.cu, -fmad=false
 cudaError_t st7_launch_conc(bool f64, const St7Args& a, double* out, cudaStream_t st);
 cudaError_t st7_launch_init(bool f64, const St7Args& a, cudaStream_t st);
 // a.src: the state to export; a.dst: the buffer the next step pulls from

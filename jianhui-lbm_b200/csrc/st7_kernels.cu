@@ -80,11 +80,74 @@ __global__ void st7_import_kernel(St7Args a, const int32_t* __restrict__ ref_of,
   for (int q = 1; q < 7; q++) dst[a.table[(size_t)(q - 1) * npad + x] - npad] = (T)row[q];
 }
 
+// D3Q19 (the solute program with 19 directions): g is [19][npad]; a node's
+// pulled value of storage row q is g[x] for q = 0, else g[table[q-1][x]].
+__device__ __forceinline__ size_t st19_slot(const St7Args& a, int x, int q) {
+  return q == 0 ? (size_t)x : (size_t)a.table[(size_t)(q - 1) * a.npad + x];
+}
+
+// C = sum of the pulled g in the program's direction order (ST19:1636-1650).
+template <typename T>
+__global__ void st19_conc_kernel(St7Args a, double* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  const T* __restrict__ src = static_cast<const T*>(a.src);
+  T C = T(0);
+  if (a.c_given) {
+    C = static_cast<const T*>(a.c_given)[x];
+  } else {
+#pragma unroll
+    for (int k = 0; k < kQ; k++) C = C + src[st19_slot(a, x, cg::row(k))];
+  }
+  out[x] = (double)C;
+}
+
+// Initial g_k = w_k C (1 + 3 e_k.u) of init (ST19:1300-1312) with the velocity
+// not yet loaded (zero): w_k C, stored through the inverse pull.
+template <typename T>
+__global__ void st19_init_kernel(St7Args a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  const T C = static_cast<const T*>(a.c_given)[x];
+  T* __restrict__ g = static_cast<T*>(a.dst);
+#pragma unroll
+  for (int q = 0; q < kQ; q++) g[st19_slot(a, x, q)] = T(weight(q)) * C * (T(1) + T(3) * T(0));
+}
+
+// g as the next step pulls it, [(count+1)*19] in reference id order and the
+// program's direction order, and its inverse.
+template <typename T>
+__global__ void st19_export_kernel(St7Args a, const int32_t* __restrict__ ref_of, double* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  const T* __restrict__ src = static_cast<const T*>(a.src);
+  double* row = out + (size_t)ref_of[x] * kQ;
+#pragma unroll
+  for (int k = 0; k < kQ; k++) row[k] = (double)src[st19_slot(a, x, cg::row(k))];
+}
+
+template <typename T>
+__global__ void st19_import_kernel(St7Args a, const int32_t* __restrict__ ref_of, const double* __restrict__ in) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.n) return;
+  T* __restrict__ dst = static_cast<T*>(a.dst);
+  const double* row = in + (size_t)ref_of[x] * kQ;
+#pragma unroll
+  for (int k = 0; k < kQ; k++) dst[st19_slot(a, x, cg::row(k))] = (T)row[k];
+}
+
 }  // namespace
 
 cudaError_t st7_launch_export(bool f64, const St7Args& a, const int32_t* ref_of, double* out, cudaStream_t st) {
   if (a.n == 0) return cudaSuccess;
   const int g = (a.n + 255) / 256;
+  if (a.nq == kQ) {
+    if (f64)
+      st19_export_kernel<double><<<g, 256, 0, st>>>(a, ref_of, out);
+    else
+      st19_export_kernel<float><<<g, 256, 0, st>>>(a, ref_of, out);
+    return cudaGetLastError();
+  }
   if (f64)
     st7_export_kernel<double><<<g, 256, 0, st>>>(a, ref_of, out);
   else
@@ -95,6 +158,13 @@ cudaError_t st7_launch_export(bool f64, const St7Args& a, const int32_t* ref_of,
 cudaError_t st7_launch_import(bool f64, const St7Args& a, const int32_t* ref_of, const double* in, cudaStream_t st) {
   if (a.n == 0) return cudaSuccess;
   const int g = (a.n + 255) / 256;
+  if (a.nq == kQ) {
+    if (f64)
+      st19_import_kernel<double><<<g, 256, 0, st>>>(a, ref_of, in);
+    else
+      st19_import_kernel<float><<<g, 256, 0, st>>>(a, ref_of, in);
+    return cudaGetLastError();
+  }
   if (f64)
     st7_import_kernel<double><<<g, 256, 0, st>>>(a, ref_of, in);
   else
@@ -103,12 +173,20 @@ cudaError_t st7_launch_import(bool f64, const St7Args& a, const int32_t* ref_of,
 }
 
 cudaError_t st7_launch_step(bool f64, const St7Args& a, cudaStream_t st) {
+  if (a.nq == kQ) return f64 ? st19_launch_step_f64(a, st) : st7_detail::launch_step19<float>(a, st);
   return f64 ? st7_launch_step_f64(a, st) : st7_detail::launch_step<float>(a, st);
 }
 
 cudaError_t st7_launch_conc(bool f64, const St7Args& a, double* out, cudaStream_t st) {
   if (a.n == 0) return cudaSuccess;
   const int g = (a.n + 255) / 256;
+  if (a.nq == kQ) {
+    if (f64)
+      st19_conc_kernel<double><<<g, 256, 0, st>>>(a, out);
+    else
+      st19_conc_kernel<float><<<g, 256, 0, st>>>(a, out);
+    return cudaGetLastError();
+  }
   if (f64)
     st7_conc_kernel<double><<<g, 256, 0, st>>>(a, out);
   else
@@ -119,6 +197,13 @@ cudaError_t st7_launch_conc(bool f64, const St7Args& a, double* out, cudaStream_
 cudaError_t st7_launch_init(bool f64, const St7Args& a, cudaStream_t st) {
   if (a.n == 0) return cudaSuccess;
   const int g = (a.n + 255) / 256;
+  if (a.nq == kQ) {
+    if (f64)
+      st19_init_kernel<double><<<g, 256, 0, st>>>(a);
+    else
+      st19_init_kernel<float><<<g, 256, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   if (f64)
     st7_init_kernel<double><<<g, 256, 0, st>>>(a);
   else

@@ -284,6 +284,7 @@ _SIGNATURES = {
     "lbm_cg_destroy": ([C.c_void_p], None),
     "lbm_cg_set_body_force": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int], C.c_int),
     "lbm_cg_set_cap_a": ([C.c_void_p, C.c_double], C.c_int),
+    "lbm_cg_input_update": ([C.c_void_p, C.POINTER(CGInput)], C.c_int),
     "lbm_cg_create_bc": ([C.POINTER(CGParams), C.POINTER(Boundary), _U8P, _F64P, C.c_int, C.c_int, C.c_int,
                           C.POINTER(C.c_void_p)], C.c_int),
     "lbm_cg_set_faces": ([C.c_void_p, _F64P, _F64P, C.c_int], C.c_int),
@@ -305,6 +306,9 @@ _SIGNATURES = {
     "lbm_cg_read_checkpoint": ([C.c_void_p, C.c_char_p, C.c_longlong], C.c_int),
     "lbm_st7_create": ([C.c_void_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P, _F64P, C.POINTER(C.c_void_p)], C.c_int),
     "lbm_st7_create_from_flow": ([C.c_void_p, C.c_void_p, _F64P, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_st19_create": ([C.c_void_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P, _F64P, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_st19_create_from_flow": ([C.c_void_p, C.c_void_p, _F64P, C.POINTER(C.c_void_p)], C.c_int),
+    "lbm_st7_directions": ([C.c_void_p], C.c_int),
     "lbm_st7_step": ([C.c_void_p, C.c_int], C.c_int),
     "lbm_st7_get_concentration": ([C.c_void_p, _F64P], C.c_int),
     "lbm_st7_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_double)], C.c_int),
@@ -365,24 +369,31 @@ class ST7Params(C.Structure):
 
 
 class Solute:
-    """D3Q7 passive-scalar solve advected by a fixed velocity field.
+    """Passive-scalar solve advected by a fixed velocity field: the D3Q7
+    solute program (lattice=7) or the D3Q19 one (lattice=19).
 
     Either ``u_nodes`` ([(count+1), 3], the order of SinglePhase.fields()) or
     ``flow`` (a SinglePhase whose current velocity is used) must be given."""
 
-    def __init__(self, mask, c0, diffusivity, u_nodes=None, flow=None, precision="f64", device=0):
+    def __init__(self, mask, c0, diffusivity, u_nodes=None, flow=None, precision="f64", device=0, lattice=7):
+        if lattice not in (7, 19):
+            raise ValueError("lattice is 7 or 19")
         p = ST7Params(float(diffusivity), PRECISIONS[precision] if isinstance(precision, str) else int(precision),
                       int(device))
         c0 = np.ascontiguousarray(c0, dtype=np.float64).reshape(-1)
         h = C.c_void_p()
+        L = lib()
         if flow is not None:
-            _check(lib().lbm_st7_create_from_flow(C.byref(p), flow._h, c0, C.byref(h)))
+            fn = L.lbm_st7_create_from_flow if lattice == 7 else L.lbm_st19_create_from_flow
+            _check(fn(C.byref(p), flow._h, c0, C.byref(h)))
         else:
             m = np.ascontiguousarray(mask, dtype=np.uint8)
             nz, ny, nx = m.shape
             u = np.ascontiguousarray(u_nodes, dtype=np.float64).reshape(-1)
-            _check(lib().lbm_st7_create(C.byref(p), m.reshape(-1), nx, ny, nz, u, c0, C.byref(h)))
+            fn = L.lbm_st7_create if lattice == 7 else L.lbm_st19_create
+            _check(fn(C.byref(p), m.reshape(-1), nx, ny, nz, u, c0, C.byref(h)))
         self._h = h
+        self.directions = L.lbm_st7_directions(h)
         c, st, ms = C.c_int(), C.c_longlong(), C.c_double()
         _check(lib().lbm_st7_info(h, C.byref(c), C.byref(st), C.byref(ms)))
         self.count = c.value
@@ -396,13 +407,14 @@ class Solute:
         return c
 
     def populations(self):
-        """g as the next step reads it, [(count+1), 7] (column 0 unused)."""
-        g = np.zeros((self.count + 1) * 7)
+        """g as the next step reads it, [(count+1), 7] (column 0 unused) or,
+        for D3Q19, [(count+1), 19] in the solute program's direction order."""
+        g = np.zeros((self.count + 1) * self.directions)
         _check(lib().lbm_st7_get_populations(self._h, g))
-        return g.reshape(-1, 7)
+        return g.reshape(-1, self.directions)
 
     def set_state(self, g, c):
-        """Restores g [(count+1), 7] and C [(count+1)]; the next step takes C as given."""
+        """Restores g [(count+1), 7 or 19] and C [(count+1)]; the next step takes C as given."""
         arr = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
         _check(lib().lbm_st7_set_state(self._h, arr(g), arr(c)))
 
@@ -496,6 +508,17 @@ class ColourGradient:
 
     def set_cap_a(self, cap_a):
         _check(lib().lbm_cg_set_cap_a(self._h, float(cap_a)))
+
+    def input_update(self, path):
+        """input_update (CG3:5765-5925): the INPUT file at `path` read again;
+        its wall colour, CapA and flux thresholds apply from the next
+        collision, its body force from this step's macro step.  Returns the
+        file as a dict (n_max, the output intervals and the permeability are
+        the caller's)."""
+        inp = CGInput()
+        _check(lib().lbm_read_cg_input(os.fsencode(path), C.byref(inp)))
+        _check(lib().lbm_cg_input_update(self._h, C.byref(inp)))
+        return inp.as_dict()
 
     def set_faces(self, rho, vel, active=True):
         """Face densities and normal velocities (xp, xn, yp, yn, zp, zn) and

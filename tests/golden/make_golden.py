@@ -42,6 +42,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "jianhui-lbm_b200"))
+sys.path.insert(0, os.path.dirname(HERE))  # tests/: helpers
 
 import oracle  # noqa: E402
 from lbm_b200 import geometry as G  # noqa: E402
@@ -318,6 +319,28 @@ CG_GEOMETRY_RUNS = {
 }
 
 
+# Runs with input_dynamic (the INPUT file read again every 100 steps,
+# input_update): name -> the line overrides of each version, in the order the
+# program opens the file (at start, then at steps 0, 100, 200, 300).  Base:
+# 400 steps, reports every 50, phase VTK every 100, the stabiliser holding the
+# force back to step 150 (the update at step 0 turns it on, gxs = gx),
+# checkpoints at the end.  Step 100: force doubled, CapA 2e-3, wall colour
+# 0.5.  Step 200: reports every 25, single-phase permeability 1500 mD, flux
+# thresholds 0.9 / 0.02, phase VTK every 50.  Step 300: n_max 350, velocity
+# VTK every 50.
+CG_DYNAMIC_BASE = dict(L4=400, L27=50, L29=-1, L30=-1, L31=100, L36="1 150", L45=0, L66="1 100")
+CG_DYNAMIC_RUNS = {
+    "cg_outputs_dyn.npz": [
+        {},
+        {},
+        dict(L8="2.0e-5 0.0 0.0", L21="2.0e-3", L20="0.5"),
+        dict(L8="2.0e-5 0.0 0.0", L21="2.0e-3", L20="0.5", L27=25, L23="1500.0", L39="0.9 0.02", L31=50),
+        dict(L8="2.0e-5 0.0 0.0", L21="2.0e-3", L20="0.5", L27=25, L23="1500.0", L39="0.9 0.02", L31=50,
+             L4=350, L29=50),
+    ],
+}
+
+
 # Seed of oracle/mpishim/seeded_rand.h (LBM_FIXTURE_SEED): the colour-gradient
 # program built with it draws the random numbers that lbm_cg --seed draws.
 FIXTURE_SEED = 20261203
@@ -342,19 +365,28 @@ CG_SEEDED_RUNS = {
 }
 
 
-def run_cg_program(workdir, input_txt, mask, psi, args=(), seeded=False):
+def run_cg_program(workdir, input_txt, mask, psi, args=(), seeded=False, versions=None):
+    """versions: the texts the k-th opening of INPUT.dat reads (a named pipe,
+    tests/helpers.py InputVersions), for a run with input_dynamic."""
     import subprocess
 
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_cg3_main_seeded" if seeded else "ref_cg3_main")
     G.write_ascii(os.path.join(workdir, "mask.dat"), mask)
     with open(os.path.join(workdir, "phase.dat"), "w") as f:
         f.write(phase_text(psi))
-    with open(os.path.join(workdir, "INPUT.dat"), "w") as f:
-        f.write(input_txt)
-    subprocess.run([exe, "INPUT.dat", *args], cwd=workdir, check=True, capture_output=True)
+    if versions is None:
+        with open(os.path.join(workdir, "INPUT.dat"), "w") as f:
+            f.write(input_txt)
+        subprocess.run([exe, "INPUT.dat", *args], cwd=workdir, check=True, capture_output=True)
+        return
+    from helpers import InputVersions
+
+    with InputVersions(os.path.join(workdir, "INPUT.dat"), versions) as iv:
+        subprocess.run([exe, "INPUT.dat", *args], cwd=workdir, check=True, capture_output=True, timeout=600)
+        print("input openings served:", iv.served)
 
 
-def collect_cg(workdir, prefix):
+def collect_cg(workdir, prefix, fg_width=7):
     out = {}
     for name in sorted(os.listdir(workdir)):
         if not name.startswith(prefix):
@@ -362,18 +394,20 @@ def collect_cg(workdir, prefix):
         key = name[len(prefix):]
         data = open(os.path.join(workdir, name), "rb").read()
         if key.startswith("LBM_checkpoint_"):
-            width = {"rho": 1, "velocity": 3, "f": 19, "psi": 1, "rhor": 1, "rhob": 1, "fg": 7}[key.split("_")[2]]
+            width = {"rho": 1, "velocity": 3, "f": 19, "psi": 1, "rhor": 1, "rhob": 1, "fg": fg_width}[key.split("_")[2]]
             out[key] = digest(np.frombuffer(data, dtype=np.float64).reshape(-1, width)[1:])
         else:
             out[key] = data
     return out
 
 
-def save_cg(fname, mask, psi, input_txt, files, seed=None):
+def save_cg(fname, mask, psi, input_txt, files, seed=None, versions=None):
     blob = {"mask": pack(mask), "shape": np.array(mask.shape), "phase": np.frombuffer(phase_text(psi).encode(), np.uint8),
             "input": np.frombuffer(input_txt.encode(), np.uint8), "names": np.array(sorted(files))}
     if seed is not None:
         blob["seed"] = np.array(seed, dtype=np.uint64)
+    for k, v in enumerate(versions or ()):
+        blob[f"input_version_{k}"] = np.frombuffer(v.encode(), np.uint8)
     for k, v in files.items():
         blob[k] = np.frombuffer(v, np.uint8) if isinstance(v, bytes) else np.array(v)
     np.savez_compressed(os.path.join(HERE, fname), **blob)
@@ -415,6 +449,14 @@ def cg_program_outputs(only=None):
             run_cg_program(d, text, mask, psi, seeded=True)
             files = collect_cg(d, "out_")
         save_cg(fname, mask, psi, text, files, seed=FIXTURE_SEED)
+    for fname, steps in CG_DYNAMIC_RUNS.items():
+        if only and only not in fname:
+            continue
+        texts = [cg_input_text(**{**CG_DYNAMIC_BASE, **kv}) for kv in steps]
+        with tempfile.TemporaryDirectory() as d:
+            run_cg_program(d, texts[0], mask, psi, versions=texts)
+            files = collect_cg(d, "out_")
+        save_cg(fname, mask, psi, texts[0], files, versions=texts)
     for fname, (geometry, kv) in CG_GEOMETRY_RUNS.items():
         if only and only not in fname:
             continue
@@ -484,7 +526,7 @@ def solute_input(**kv):
     return "\n".join(lines) + "\n"
 
 
-def st7_fixture(out=None):
+def st7_fixture(out=None, program="ref_st7_slab"):
     """The reference's own slab programs at two ranks (multi-process MPI
     stand-in): the slab single-phase program makes the flow of a 16x10x8
     sphere pack and writes Velocity_for_solute_100.<rank>.bin; the solute
@@ -492,12 +534,13 @@ def st7_fixture(out=None):
     advects and diffuses for 61 steps and backs up the concentration every 20
     steps.  Stored: mask, initial concentration, the velocity records (slab
     order, ranks concatenated), rank sizes, and the concentration at steps
-    20, 40, 60 (slab order)."""
+    20, 40, 60 (slab order).  program = "ref_st19_slab" runs the D3Q19
+    solute program on the same inputs instead (st19_slab.npz)."""
     import tempfile
 
-    sp, st = oracle.slab_program("ref_sp_slab"), oracle.slab_program("ref_st7_slab")
+    sp, st = oracle.slab_program("ref_sp_slab"), oracle.slab_program(program)
     if not (sp and st):
-        raise SystemExit("oracle/_ref/ref_sp_slab and ref_st7_slab are needed (make -C oracle ref)")
+        raise SystemExit(f"oracle/_ref/ref_sp_slab and {program} are needed (make -C oracle ref)")
     mask = G.overlapping_spheres(ST7_SHAPE, 0.6, 2.5, seed=ST7_SEED)
     nx, ny, nz = ST7_SHAPE
     c0 = np.random.default_rng(5).uniform(0, 1, mask.shape).astype(np.float32)
@@ -523,7 +566,7 @@ def st7_fixture(out=None):
     print("st7_slab", mask.shape, [v.size // 3 for v in vel])
 
 
-def st7_program_outputs():
+def st7_program_outputs(program="ref_st7_slab", tag="st7", variants=True):
     """The solute program itself at two ranks (multi-process MPI stand-in):
     every file it writes, for the drop-in driver's byte-for-byte test.  The
     slab single-phase program first makes the flow of the st7_slab geometry
@@ -535,13 +578,15 @@ def st7_program_outputs():
     (st7_outputs_dis.npz) and along z with a y window (st7_outputs_dis3.npz);
     and a restart from the step-40 checkpoint (copied to
     the unprefixed names Backup_init reads) runs 31 more steps
-    (st7_outputs_restart.npz)."""
+    (st7_outputs_restart.npz).  program = "ref_st19_slab", tag = "st19",
+    variants = False: the D3Q19 solute program, Out_Mode 1 run and restart
+    only (st19_outputs.npz, st19_outputs_restart.npz)."""
     import shutil
     import tempfile
 
-    sp, st = oracle.slab_program("ref_sp_slab"), oracle.slab_program("ref_st7_slab")
+    sp, st = oracle.slab_program("ref_sp_slab"), oracle.slab_program(program)
     if not (sp and st):
-        raise SystemExit("oracle/_ref/ref_sp_slab and ref_st7_slab are needed (make -C oracle ref)")
+        raise SystemExit(f"oracle/_ref/ref_sp_slab and {program} are needed (make -C oracle ref)")
     mask = G.overlapping_spheres(ST7_SHAPE, 0.6, 2.5, seed=ST7_SEED)
     nx, ny, nz = ST7_SHAPE
     c0 = np.random.default_rng(5).uniform(0, 1, mask.shape).astype(np.float32)
@@ -557,9 +602,12 @@ def st7_program_outputs():
         open(os.path.join(d, "phase.dat"), "w").write(phase)
         # dispersion statistics along x every 20 steps (written after step 10)
         # and along z every 40, both layouts of the run above
-        runs = {"st7_outputs.npz": ("./st_", dict(L29=1)), "st7_outputs_b.npz": ("./sb_", dict(L29=0)),
-                "st7_outputs_dis.npz": ("./sd_", dict(L29=1, L33="1 20", L39=10)),
-                "st7_outputs_dis3.npz": ("./sz_", dict(L29=0, L33="3 40", L39=-1, L40="0 1 0", L42="8 2"))}
+        runs = {f"{tag}_outputs.npz": ("./st_", dict(L29=1))}
+        if variants:
+            runs.update({"st7_outputs_b.npz": ("./sb_", dict(L29=0)),
+                         "st7_outputs_dis.npz": ("./sd_", dict(L29=1, L33="1 20", L39=10)),
+                         "st7_outputs_dis3.npz": ("./sz_", dict(L29=0, L33="3 40", L39=-1, L40="0 1 0",
+                                                                 L42="8 2"))})
         for fname, (prefix, kv) in runs.items():
             base = dict(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=60, L7="0.0 0.5", L23=ST7_D,
                         L28=20, L30=40, L32=20, L33="0 1000", L36=prefix, L45=40, L47=100)
@@ -567,7 +615,7 @@ def st7_program_outputs():
             text = solute_input(**base)
             open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
             assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
-            save_st7(fname, mask, phase, text, vel, collect_cg(d, prefix[2:]))
+            save_st7(fname, mask, phase, text, vel, collect_cg(d, prefix[2:], fg_width=19 if tag == "st19" else 7))
         for r in range(ST7_NRANKS):
             for what in ("psi", "fg"):
                 shutil.copy(os.path.join(d, f"st_LBM_checkpoint_{what}_40.{r}.bin_input"),
@@ -576,7 +624,8 @@ def st7_program_outputs():
                             L28=10, L29=1, L30=-1, L32=30, L33="0 1000", L36="./rs_", L45=-1, L46=40, L47=100)
         open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
         assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
-        save_st7("st7_outputs_restart.npz", mask, phase, text, vel, collect_cg(d, "rs_"))
+        save_st7(f"{tag}_outputs_restart.npz", mask, phase, text, vel,
+                 collect_cg(d, "rs_", fg_width=19 if tag == "st19" else 7))
 
 
 def save_st7(fname, mask, phase, text, vel, files):
@@ -636,10 +685,15 @@ def main():
     ap.add_argument("--cg-outputs", action="store_true")
     ap.add_argument("--only", default=None, help="--cg-outputs: runs whose fixture name contains this")
     ap.add_argument("--st7-outputs", action="store_true")
+    ap.add_argument("--st19", action="store_true", help="D3Q19 solute program fixtures")
     a = ap.parse_args()
     oracle.build()
     if a.st7_outputs:
         st7_program_outputs()
+        return
+    if a.st19:
+        st7_fixture(os.path.join(HERE, "st19_slab.npz"), program="ref_st19_slab")
+        st7_program_outputs(program="ref_st19_slab", tag="st19", variants=False)
         return
     if a.cg_outputs:
         cg_program_outputs(a.only)

@@ -85,7 +85,7 @@ def test_phase_file_reads_as_float(L, tmp_path):
     (dict(L64="1 0"), "rel_perm_id_dir"),
     (dict(L58="4 1 2000"), "pressure_change2"),
     (dict(L58="1 2 0"), "pressure_change2"),
-    (dict(L66="1 1000"), "input_dynamic"),
+    (dict(L66="1 0"), "input_dynamic"),
     (dict(L31=0), "frePsi"),
 ])
 def test_cg_driver_refuses_options_outside_its_scope(L, tmp_path, lines, field):
@@ -118,3 +118,42 @@ def test_st7_input_field_order_and_slab_partition(L, tmp_path):
     assert sizes == [g["file:Velocity_for_solute_100.%d.bin" % r].size // 24 for r in range(2)]
     st = np.load(os.path.join(GOLDEN, "st7_slab.npz"))
     assert sizes == [int(v) for v in st["rank_nodes"]]
+
+
+def test_input_versions_serve_one_text_per_opening(tmp_path):
+    """The named pipe behind the input_dynamic test: each opening of the file
+    by another process reads the next version whole, the last one repeats."""
+    import subprocess
+    import sys
+
+    from helpers import InputVersions
+
+    path = str(tmp_path / "INPUT.dat")
+    reader = ("import sys, time\n"
+              "for k in range(4):\n"
+              "    print(open(sys.argv[1]).read().splitlines()[0], flush=True)\n"
+              "    time.sleep(0.01)\n")
+    with InputVersions(path, ["a\nx\n", "b\ny\n", "c\nz\n"]) as iv:
+        r = subprocess.run([sys.executable, "-c", reader, path], capture_output=True, text=True, timeout=60)
+        assert iv.served == 4
+    assert r.stdout.split() == ["a", "b", "c", "c"]
+    assert not os.path.exists(path)
+
+
+def test_cg_dynamic_fixture_versions_parse(L, tmp_path):
+    """The versions of cg_outputs_dyn.npz carry the values input_update reads
+    (CG3:5780-5820): n_max, force, wall colour, CapA, permeability, the
+    report / output intervals and the flux thresholds."""
+    g = np.load(os.path.join(GOLDEN, "cg_outputs_dyn.npz"))
+    got = []
+    for k in range(5):
+        p = tmp_path / f"v{k}.dat"
+        p.write_bytes(g[f"input_version_{k}"].tobytes())
+        d = L.read_cg_input(str(p))
+        got.append((d["n_max"], d["gx"], d["contact_angle"], d["cap_a"], d["permeability"], d["fre_re"],
+                    d["fre_ve"], d["fre_psi"], d["rel_perm_psi"], d["rel_perm_psi2"], d["input_dynamic"],
+                    d["update_fre"]))
+    assert got[0] == got[1] == (400, 1e-5, 0.70711, 1e-3, 2500.0, 50, -1, 100, 0.99, 0.01, 1, 100)
+    assert got[2] == (400, 2e-5, 0.5, 2e-3, 2500.0, 50, -1, 100, 0.99, 0.01, 1, 100)
+    assert got[3] == (400, 2e-5, 0.5, 2e-3, 1500.0, 25, -1, 50, 0.9, 0.02, 1, 100)
+    assert got[4] == (350, 2e-5, 0.5, 2e-3, 1500.0, 25, 50, 50, 0.9, 0.02, 1, 100)

@@ -32,6 +32,11 @@ variants of INPUT_cg.dat on 14x12x10 spheres with a blob phase field:
   cg_outputs_imb.npz,    imbibition / drainage control (rel_perm_id_dir)
   cg_outputs_drain.npz   over 50 target saturations with random phase faces,
                          same seeded program.
+  cg_outputs_dyn.npz     input_dynamic: the INPUT file read again every 100
+                         steps (input_update), its versions served in order
+                         through a named pipe: force, CapA, wall colour,
+                         report / output intervals, permeability, flux
+                         thresholds and n_max changed during the run.
 The driver, run on the same inputs at FP64, must write the same files: text
 and VTK byte for byte except the wall-clock lines of Results.txt, the
 checkpoints bit for bit (rows 1..).
@@ -145,3 +150,19 @@ def test_cg_driver_f32_reports_match(L, tmp_path, fixture):
     bf_w = np.loadtxt(golden["bodyforce.txt"].tobytes().decode().splitlines())
     bf_g = np.loadtxt((tmp_path / "out_bodyforce.txt").read_text().splitlines())
     assert np.allclose(bf_g[:, :2], bf_w[:, :2], atol=3e-3)  # saturation
+
+
+def test_cg_driver_reads_its_input_again(L, tmp_path):
+    """input_dynamic (CG3:859-861, 5765-5925): the driver opens INPUT.dat at
+    the same steps as the program and takes the same values from it."""
+    from helpers import InputVersions
+
+    golden = np.load(os.path.join(GOLDEN, "cg_outputs_dyn.npz"))
+    prepare(tmp_path, golden)
+    os.unlink(tmp_path / "INPUT.dat")
+    keys = sorted((k for k in golden.files if k.startswith("input_version_")), key=lambda k: int(k.rsplit("_", 1)[1]))
+    versions = [golden[k].tobytes().decode() for k in keys]
+    with InputVersions(str(tmp_path / "INPUT.dat"), versions) as iv:
+        run_driver(L, tmp_path)
+        assert iv.served == len(versions)
+    compare(tmp_path, golden, "out_")
