@@ -347,7 +347,7 @@ def run_ours(a):
         b64 = f.memory()["bytes_per_lu"]
     clk.__exit__(None, None, None)
     t_e2e = allmax(pg, t_e2e)
-    e2e_value = world * count * a.steps / t_e2e / 1e6
+    e2e_value = None if a.skip_e2e else world * count * a.steps / t_e2e / 1e6
     # in reference order lbm_create uploads the mask (one byte per cell) and
     # builds the compaction and the pull table on the device
     h2d = mask.size
@@ -693,7 +693,8 @@ def run_cg(a):
 def run_solute(a):
     """D3Q7 solute transport on the config-2 geometry (256^3 spheres, 5.87 M
     fluid nodes) advected by the FP32 flow after 300 steps: solute MLUPS in
-    FP32 and FP64, against the 2*6*s + 6*4 + 3*s bytes per update."""
+    FP32 and FP64, against the 2*6*s + 6*4 + 3*s bytes per update; the D3Q19
+    solute step beside it (2*19*s + 18*4 + 3*s bytes per update)."""
     world, rank, local, pg = dist_setup()
     import lbm_b200
 
@@ -705,11 +706,13 @@ def run_solute(a):
     clk = ClockSampler(local).__enter__()
     with lbm_b200.SinglePhase(mask, NU, (GX, 0.0, 0.0), precision="f32", device=local) as flow:
         flow.step(300)
-        for prec in ("f32", "f64"):
-            with lbm_b200.Solute(None, c0, 0.01, flow=flow, precision=prec, device=local) as s:
-                s.step(a.warmup)
-                s.step(steps)
-                out[prec] = (s.last_step_ms() / steps, s.count, float(s.concentration()[1:].sum()))
+        for lat in (7, 19):
+            for prec in ("f32", "f64"):
+                with lbm_b200.Solute(None, c0, 0.01, flow=flow, precision=prec, device=local, lattice=lat) as s:
+                    s.step(a.warmup)
+                    s.step(steps)
+                    key = prec if lat == 7 else f"{prec}_q19"
+                    out[key] = (s.last_step_ms() / steps, s.count, float(s.concentration()[1:].sum()))
     clk.__exit__(None, None, None)
     if rank != 0:
         return 0
@@ -726,6 +729,14 @@ def run_solute(a):
                          "bytes_per_lu": b32},
             "fp64": {"mlups": n / (ms64 * 1e-3) / 1e6, "gbs": n * b64 / (ms64 * 1e-3) / 1e9, "bytes_per_lu": b64},
             "mass_rel_diff_f32_vs_f64": abs(m32 - m64) / abs(m64), "clocks": clk.summary()}
+    (q32, _, n32), (q64, _, n64) = out["f32_q19"], out["f64_q19"]
+    c32, c64 = 2 * 19 * 4 + 18 * 4 + 3 * 4, 2 * 19 * 8 + 18 * 4 + 3 * 8
+    line["d3q19"] = {"what": "the D3Q19 solute program's step (lbm_st19_create_from_flow), same flow and C0",
+                     "f32": {"mlups": n / (q32 * 1e-3) / 1e6, "gbs": n * c32 / (q32 * 1e-3) / 1e9,
+                             "frac": n * c32 / (q32 * 1e-3) / 1e9 / peak, "bytes_per_lu": c32},
+                     "fp64": {"mlups": n / (q64 * 1e-3) / 1e6, "gbs": n * c64 / (q64 * 1e-3) / 1e9,
+                              "frac": n * c64 / (q64 * 1e-3) / 1e9 / peak, "bytes_per_lu": c64},
+                     "mass_rel_diff_f32_vs_f64": abs(n32 - n64) / abs(n64)}
     emit(line)
     return 0
 
