@@ -464,7 +464,7 @@ def run_batch(a):
         t_batch = time.perf_counter() - t0
         info = b.info()
         trace = b.trace()
-    singles, t_single, t_single_create, per_inst = [], 0.0, 0.0, []
+    singles, t_single, t_single_create, per_inst, creates = [], 0.0, 0.0, [], []
     for (mask, nu, g) in inst:
         tc = time.perf_counter()
         with lbm_b200.SinglePhase(mask, nu, g, precision="f32", device=local) as s:
@@ -473,6 +473,7 @@ def run_batch(a):
             dt = time.perf_counter() - t0
             t_single += dt
             t_single_create += t0 - tc
+            creates.append(t0 - tc)
             singles.append(d)
             per_inst.append((s.count, d["step"], dt))
     # FP64 check of a seeded sample of the instances: the bit-exact FP64
@@ -502,6 +503,9 @@ def run_batch(a):
             "mlups_batched": info["node_steps"] / t_batch / 1e6,
             "converged": sum(r["status"] == 0 for r in res), "max_rel_perm_diff_vs_one_at_a_time": dk,
             "with_creation": {"batched_s": t_batch_create + t_batch, "one_at_a_time_s": t_single_create + t_single,
+                              "batch_create_s": t_batch_create, "one_at_a_time_create_s": t_single_create,
+                              "one_at_a_time_create_s_first_median_max": [creates[0], float(np.median(creates)),
+                                                                          max(creates)] if creates else None,
                               "batched_solves_per_s": len(inst_all) / (t_batch_create + t_batch),
                               "one_at_a_time_solves_per_s": len(inst_all) / (t_single_create + t_single),
                               "what": "host masks to converged results: lbm_batch_create (indexing, upload, pool) "
