@@ -280,10 +280,12 @@ LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes
  * read the int32 table.  The two give identical results; the compact form
  * moves fewer bytes but waits on more dependent loads, and lbm_autotune
  * times both.  The other kernels (reductions, exports, faces) always read
- * the int32 table. */
+ * the int32 table.  The compact form (18*2.125 bytes per node of device
+ * memory) is built when it is first chosen or asked about, not at creation. */
 LBM_API lbm_status lbm_set_table_mode(lbm_handle* h, int compact);
 /* current mode, table bytes per node the step reads, and the share of
- * (group, direction) pairs that fall back to the int32 table */
+ * (group, direction) pairs that fall back to the int32 table (asking for
+ * the share builds the compact form if it was not built yet) */
 LBM_API lbm_status lbm_table_info(lbm_handle* h, int* compact, double* table_bytes_per_node,
                                   double* wide_fraction);
 

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lbm_internal.h"
@@ -59,6 +60,52 @@ struct DevBuf {
   }
 };
 
+// Allocator whose value-less construct leaves the element uninitialised, so
+// that resizing a byte vector that is overwritten at once does not first
+// zero it on one thread.
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = UninitAlloc<U>;
+  };
+  UninitAlloc() = default;
+  template <class U>
+  UninitAlloc(const UninitAlloc<U>&) {}
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    if constexpr (sizeof...(A) == 0)
+      ::new ((void*)p) U;
+    else
+      ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+};
+
+// Copies the caller's mask into dst and counts its pore cells (value 0) in
+// one pass split over a few threads: at 256^3 a serial copy and a serial
+// count took 2-8 and 5-8 ms of lbm_create.
+long long copy_mask_count_pores(const uint8_t* src, size_t cells, uint8_t* dst) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+  const size_t min_part = size_t(1) << 20;
+  const int parts = (int)std::max<size_t>(1, std::min<size_t>((size_t)nt, cells / min_part));
+  std::vector<long long> pores(parts, 0);
+  auto work = [&](int t) {
+    const size_t lo = cells * t / parts, hi = cells * (t + 1) / parts;
+    std::memcpy(dst + lo, src + lo, hi - lo);
+    long long c = 0;
+    for (size_t i = lo; i < hi; i++) c += (src[i] == 0);
+    pores[t] = c;
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < parts; t++) th.emplace_back(work, t);
+  work(0);
+  for (auto& x : th) x.join();
+  long long total = 0;
+  for (long long c : pores) total += c;
+  return total;
+}
+
 }  // namespace lbm
 
 using namespace lbm;
@@ -66,7 +113,7 @@ using namespace lbm;
 struct lbm_handle {
   lbm_params prm{};
   Store kind = Store::F32;
-  std::vector<uint8_t> mask;
+  std::vector<uint8_t, UninitAlloc<uint8_t>> mask;
   Geometry geo;
   MrtConstants mrt{};
   int device = 0;
@@ -86,9 +133,8 @@ struct lbm_handle {
   bool ct_ok = false;
   bool ct_on = false;  // the int32 table unless chosen (lbm_set_table_mode, lbm_autotune)
   double ct_wide_frac = 1.0;
-  // field export: device buffers kept between calls, pinned staging
+  // field export: device buffers kept between calls
   DevBuf x_rint, x_uint, x_rref, x_uref;
-  PinnedStage stage;
   int cur = 0;
   long long step = 0;
   bool given_macro = true;  // next step / reduce takes rho, u from rho_given / u_given
@@ -177,7 +223,11 @@ lbm_status upload_layout(lbm_handle* h) {
   h->last_p = g.count > 0 ? g.int_of[g.count] : -1;
   h->drop_graphs();
   h->cell_idx_valid = false;
-  return build_compact_table(h);
+  // the compact form is built when it is first chosen (lbm_set_table_mode,
+  // lbm_autotune) or asked about (lbm_table_info); a new layout rebuilds it
+  // only when it is in use
+  h->ct_ok = false;
+  return h->ct_on ? build_compact_table(h) : LBM_OK;
 }
 
 // Host copies of the compaction and node order, built on first need.
@@ -555,7 +605,9 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
   LBM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   LBM_CUDA_TRY(cudaEventCreate(&h->ev0));
   LBM_CUDA_TRY(cudaEventCreate(&h->ev1));
-  h->mask.assign(mask, mask + (size_t)nx * ny * nz);
+  const size_t ncells = (size_t)nx * ny * nz;
+  h->mask.resize(ncells);
+  const long long pores = copy_mask_count_pores(mask, ncells, h->mask.data());
   if (!build_mrt_constants(p->nu, &h->mrt)) return fail(LBM_ERR_ARG, "moment matrix inversion failed");
   if (h->kind == Store::F64) {
     if (!mi_pattern_matches(&h->mrt.MI[0][0]))
@@ -578,9 +630,7 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
   const bool on_device = ord == LBM_ORDER_REFERENCE && full_window && !bc_active(p->bc);
   if (on_device) {
     // count only; numbering and table are built on the device
-    const size_t cells = (size_t)nx * ny * nz;
-    long long pores = 0;
-    for (size_t c = 0; c < cells; c++) pores += (h->mask[c] == 0);
+    const size_t cells = ncells;
     Geometry& g = h->geo;
     g.nx = nx;
     g.ny = ny;
@@ -605,11 +655,12 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
     h->ordering = LBM_ORDER_REFERENCE;
     h->last_p = h->geo.count - 1;
     LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));  // before the scratch is freed
-    if ((st = build_compact_table(h.get())) != LBM_OK) return st;
   } else if ((st = layout(h.get(), ord)) != LBM_OK) {
     return st;
   }
   if ((st = init_state(h.get())) != LBM_OK) return st;
+  // the process's staging memory for field reads (pinned once per device)
+  LBM_CUDA_TRY(stage_pool_prime());
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   *out = h.release();
   if (p->ordering == LBM_ORDER_AUTO) {
@@ -751,8 +802,8 @@ lbm_status lbm_get_fields(lbm_handle* h, double* rho, double* u) {
   LBM_CUDA_TRY(cudaMemsetAsync(uref.p, 0, uref.bytes, h->stream));
   LBM_CUDA_TRY(launch_export_macro(rint.as<double>(), uint_.as<double>(), h->ref_of.as<int32_t>(), n, npad,
                                    rref.as<double>(), uref.as<double>(), h->stream));
-  if (rho) LBM_CUDA_TRY(d2h_staged(h->stage, rho, rref.p, rref.bytes, h->stream));
-  if (u) LBM_CUDA_TRY(d2h_staged(h->stage, u, uref.p, uref.bytes, h->stream));
+  if (rho) LBM_CUDA_TRY(d2h_staged(rho, rref.p, rref.bytes, h->stream));
+  if (u) LBM_CUDA_TRY(d2h_staged(u, uref.p, uref.bytes, h->stream));
   LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return LBM_OK;
 }
@@ -770,7 +821,7 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f) {
   if ((st = finalize_faces(h, &n_main, &bnd_f)) != LBM_OK) return st;
   LBM_CUDA_TRY(launch_export_pop(h->kind, h->pop[h->cur].p, h->table.as<int32_t>(), h->ref_of.as<int32_t>(), n,
                                  h->geo.npad, h->fp16_scale, out.as<double>(), h->stream, n_main, bnd_f));
-  LBM_CUDA_TRY(d2h_staged(h->stage, f, out.p, out.bytes, h->stream));
+  LBM_CUDA_TRY(d2h_staged(f, out.p, out.bytes, h->stream));
   return LBM_OK;
 }
 
@@ -842,7 +893,7 @@ lbm_status lbm_set_table_mode(lbm_handle* h, int compact) {
   lbm_status st = check_handle(h);
   if (st != LBM_OK) return st;
   if (compact != 0 && compact != 1) return fail(LBM_ERR_ARG, "lbm_set_table_mode: mode must be 0 or 1");
-  if (compact && !h->ct_ok) return fail(LBM_ERR_STATE, "lbm_set_table_mode: no compact table for this layout");
+  if (compact && !h->ct_ok && (st = build_compact_table(h)) != LBM_OK) return st;
   if (h->ct_on != (compact == 1)) h->drop_graphs();
   h->ct_on = compact == 1;
   return LBM_OK;
@@ -850,6 +901,11 @@ lbm_status lbm_set_table_mode(lbm_handle* h, int compact) {
 
 lbm_status lbm_table_info(lbm_handle* h, int* compact, double* table_bytes_per_node_out, double* wide_fraction) {
   if (!h) return fail(LBM_ERR_ARG, "null handle");
+  if (wide_fraction && !h->ct_ok) {
+    lbm_status st = check_handle(h);
+    if (st == LBM_OK) st = build_compact_table(h);
+    if (st != LBM_OK) return st;
+  }
   if (compact) *compact = (h->ct_ok && h->ct_on) ? 1 : 0;
   if (table_bytes_per_node_out) *table_bytes_per_node_out = table_bytes_per_node(h);
   if (wide_fraction) *wide_fraction = h->ct_wide_frac;
@@ -917,6 +973,7 @@ lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* 
   };
   for (int oi = 0; oi < 4; oi++) {
     if ((st = layout(h, orders[oi])) != LBM_OK) return st;
+    if (!h->ct_ok && (st = build_compact_table(h)) != LBM_OK) return st;
     for (int bi = 0; bi < 4; bi++)
       for (int ct = 0; ct < (h->ct_ok ? 2 : 1); ct++) {
         Cand c{orders[oi], blocks[bi], ct, 0.0};
@@ -931,6 +988,7 @@ lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* 
   bool best_ct = h->ct_on;
   for (Cand& c : cands) {
     if ((st = layout(h, c.o)) != LBM_OK) return st;
+    if (c.ct == 1 && !h->ct_ok && (st = build_compact_table(h)) != LBM_OK) return st;
     if ((st = time_cand(c, 4 * trial_steps, &c.ml)) != LBM_OK) return st;
     if (c.ml > best) {
       best = c.ml;
@@ -940,6 +998,7 @@ lbm_status lbm_autotune(lbm_handle* h, int trial_steps, int* ordering_out, int* 
     }
   }
   if ((st = layout(h, best_o)) != LBM_OK) return st;
+  if (best_ct && !h->ct_ok && (st = build_compact_table(h)) != LBM_OK) return st;
   h->block = best_b;
   h->ct_on = best_ct && h->ct_ok;
   h->drop_graphs();

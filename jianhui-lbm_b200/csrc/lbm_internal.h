@@ -161,8 +161,8 @@ struct BcLists {
 };
 void bc_node_lists(const lbm_boundary& bc, const Geometry& g, BcLists* out);
 
-// Two pinned staging buffers for device -> pageable host copies (allocated
-// on first use, owned by a handle; one copy at a time).
+// Two pinned staging buffers for device -> pageable host copies; copies
+// borrow them from a process-wide pool per device (transfer.cpp).
 struct PinnedStage {
   static constexpr size_t kChunk = size_t(16) << 20;
   void* buf[2] = {nullptr, nullptr};
@@ -173,8 +173,12 @@ struct PinnedStage {
   ~PinnedStage();
 };
 // Copies `bytes` from device memory `src` to host memory `dst` in order on
-// `st` and returns when the host copy is complete.
-cudaError_t d2h_staged(PinnedStage& s, void* dst, const void* src, size_t bytes, cudaStream_t st);
+// `st` (a stream of the current device) and returns when the host copy is
+// complete.
+cudaError_t d2h_staged(void* dst, const void* src, size_t bytes, cudaStream_t st);
+// Pins one stage for the current device if its pool has none yet (so that
+// the process's first field read does not pay for it).
+cudaError_t stage_pool_prime();
 
 // Mask and box of a single-phase handle (for solvers coupled to it).
 const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz);
