@@ -657,6 +657,11 @@ def run_cg(a):
     mask, psi = W.config3()
     kw = dict(nu_l=0.1, nu_g=0.1, psi_solid=0.70711, cap_a=1e-3, g=(1e-5, 0.0, 0.0), body_force_phase=-1,
               flux_psi=0.99, flux_umax=0.01)
+    if a.cg_faces:
+        # Sub_BC 1 pressure faces on both x faces, no body force
+        kw["g"] = (0.0, 0.0, 0.0)
+        kw["boundary"] = lbm_b200.Boundary.make(sub_bc=1, in_bc=1, pressure=(1, 1, 0, 0, 0, 0),
+                                                rho=(1.0, 1.004, 1.0, 1.0, 1.0, 1.0))
     steps = a.cg_steps
     out = {}
     clk = ClockSampler(local).__enter__()
@@ -678,7 +683,9 @@ def run_cg(a):
     line = {"metric": "colour-gradient fluid MLUPS (FP32)", "value": n / (ms32 * 1e-3) / 1e6, "unit": "MLUPS",
             "n_gpus": world, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "128^3 random cylinders r=3, porosity 0.6, blob phase field S_w=0.5, nu ratio 1, "
-                                   "CapA=1e-3, psi_solid=cos45, gx=1e-5 on the non-wetting phase", "steps": steps,
+                                   "CapA=1e-3, psi_solid=cos45, " +
+                                   ("Sub_BC 1 pressure faces rho 1.004 (x-) / 1.0 (x+), no body force" if a.cg_faces
+                                    else "gx=1e-5 on the non-wetting phase"), "steps": steps,
                        "fluid_nodes": n},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_source": peak_src, "bytes_per_lu": cg_bytes},
@@ -748,6 +755,7 @@ def run_solute(a):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cg-steps", type=int, default=20000)
+    ap.add_argument("--cg-faces", action="store_true", help="cg: pressure faces on x instead of the body force")
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg2-accuracy", "batch", "serve", "cg", "solute"],
                     help="cfg2 = the headline single-domain bench; cfg2-accuracy = its FP32 error against the "
                          "bit-exact FP64 kernel at the stop test; batch / serve = configs 4 / 5")
