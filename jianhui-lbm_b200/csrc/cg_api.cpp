@@ -442,6 +442,9 @@ lbm_status lbm_cg_create_bc(const lbm_cg_params* p, const lbm_boundary* bc, cons
     LBM_CUDA_TRY(h->corder.alloc(order.size()));
     LBM_CUDA_TRY(cudaMemcpyAsync(h->corder.p, order.data(), order.size(), cudaMemcpyHostToDevice, h->stream));
   } else {
+    if (!cg_block_pattern_matches(&h->MI[0][0]))
+      return fail(LBM_ERR_STATE, "colour-gradient M^-1 does not have the pattern the FP32 kernel was built for; "
+                                 "rebuild the library");
     LBM_CUDA_TRY(cg_set_mi_f32(&h->MI[0][0], h->stream));
   }
   BcLists bl;

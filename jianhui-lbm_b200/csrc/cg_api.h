@@ -86,6 +86,8 @@ cudaError_t cg_bc_faces(bool f64, const CgBcArgs& a, cudaStream_t st);
 
 cudaError_t cg_set_mi_f64(const double* mi, cudaStream_t st);
 cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st);
+// whether the FP32 back-transform's build-time zero pattern fits this inverse
+bool cg_block_pattern_matches(const double* mi);
 cudaError_t cg_colour_f64(const CgArgs& a, cudaStream_t st);
 cudaError_t cg_colour_f32(const CgArgs& a, cudaStream_t st);
 cudaError_t cg_collide_f64(const CgArgs& a, cudaStream_t st);

@@ -34,6 +34,13 @@ __host__ __device__ constexpr int of_row(int q) {
                 : (q == 8 ? 10 : q == 9 ? 9 : q == 10 ? 8 : q == 11 ? 15 : q == 12 ? 18 : q == 13 ? 17
                                : q == 14 ? 16 : q == 15 ? 11 : q == 16 ? 14 : q == 17 ? 13 : 12);
 }
+// Moments of even degree (they depend only on f_0 and the opposite-pair
+// sums) and of odd degree (only on the pair differences), in the column
+// order of the FP32 back-transform blocks: 0, 1, 2, 9 .. 15 and 3 .. 8,
+// 16, 17, 18.
+__host__ __device__ constexpr int even_moment(int c) { return c < 3 ? c : c + 6; }
+__host__ __device__ constexpr int odd_moment(int c) { return c < 6 ? c + 3 : c + 10; }
+
 // the scaled CG moment basis (CG3:63-83) as polynomials of e
 __host__ __device__ constexpr int mcoef(int k, int q) {
   const int x = ex(q), y = ey(q), z = ez(q);

@@ -1,7 +1,10 @@
 // Colour-gradient kernels in FP32: f stored as deviations f - w, FP32
 // arithmetic, colour sums in direction order.
+#include <cmath>
+
 #include "cg_api.h"
 #include "cg_kernels_impl.cuh"
+#include "mi_pattern.h"
 
 namespace lbm {
 
@@ -18,10 +21,29 @@ __device__ __forceinline__ float cg_mi<false>(int q, int j) {
 // directions adjacent).  So f*_0 and h_i = (f*_{2i-1} + f*_{2i})/2 come from
 // the even moments and g_i = (f*_{2i-1} - f*_{2i})/2 from the odd ones:
 // 10x10 + 9x9 products instead of 19x19.
-__host__ __device__ constexpr int kEven(int c) { return c < 3 ? c : c + 6; }   // 0, 1, 2, 9 .. 15
-__host__ __device__ constexpr int kOdd(int c) { return c < 6 ? c + 3 : c + 10; }  // 3 .. 8, 16, 17, 18
+__host__ __device__ constexpr int kEven(int c) { return cg::even_moment(c); }  // 0, 1, 2, 9 .. 15
+__host__ __device__ constexpr int kOdd(int c) { return cg::odd_moment(c); }    // 3 .. 8, 16, 17, 18
 __constant__ float c_MIe[10 * 10];
 __constant__ float c_MIo[9 * 9];
+
+// The back-transform below skips the entries of the two blocks that the
+// build-time pattern (mi_pattern.h, gen_mi_pattern.cpp) marks as zero; this
+// checks that the inverse computed at run time has no larger entry there.
+bool cg_block_pattern_matches(const double* mi) {
+  for (int i = 0; i < 10; i++)
+    for (int c = 0; c < 10; c++) {
+      const int k = kEven(c);
+      const double v = i == 0 ? mi[k] : 0.5 * (mi[(2 * i - 1) * kQ + k] + mi[(2 * i) * kQ + k]);
+      if (!((cg_even_block_row(i) >> c) & 1u) && std::fabs(v) > 1e-12) return false;
+    }
+  for (int i = 1; i <= 9; i++)
+    for (int c = 0; c < 9; c++) {
+      const int k = kOdd(c);
+      const double v = 0.5 * (mi[(2 * i - 1) * kQ + k] - mi[(2 * i) * kQ + k]);
+      if (!((cg_odd_block_row(i - 1) >> c) & 1u) && std::fabs(v) > 1e-12) return false;
+    }
+  return true;
+}
 
 cudaError_t cg_set_mi_f32(const double* mi, cudaStream_t st) {
   float m[kQ * kQ], me[100], mo[81];
@@ -201,20 +223,24 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
     ml[k] = m - S * (m - meq[k]) + (1.f - 0.5f * S) * MG[k];
   }
 
-  // back-transform by parity blocks
+  // back-transform by parity blocks, without the blocks' zero entries (105
+  // of 181 products remain)
   {
     float v = 0.f;
 #pragma unroll
-    for (int c = 0; c < 10; c++) v += c_MIe[c] * ml[kEven(c)];
+    for (int c = 0; c < 10; c++)
+      if ((cg_even_block_row(0) >> c) & 1u) v += c_MIe[c] * ml[kEven(c)];
     fd[x] = v;
   }
 #pragma unroll
   for (int i = 1; i <= 9; i++) {
     float h = 0.f, g = 0.f;
 #pragma unroll
-    for (int c = 0; c < 10; c++) h += c_MIe[i * 10 + c] * ml[kEven(c)];
+    for (int c = 0; c < 10; c++)
+      if ((cg_even_block_row(i) >> c) & 1u) h += c_MIe[i * 10 + c] * ml[kEven(c)];
 #pragma unroll
-    for (int c = 0; c < 9; c++) g += c_MIo[(i - 1) * 9 + c] * ml[kOdd(c)];
+    for (int c = 0; c < 9; c++)
+      if ((cg_odd_block_row(i - 1) >> c) & 1u) g += c_MIo[(i - 1) * 9 + c] * ml[kOdd(c)];
     fd[(size_t)cg::row(2 * i - 1) * npad + x] = h + g;
     fd[(size_t)cg::row(2 * i) * npad + x] = h - g;
   }
