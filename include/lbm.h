@@ -182,7 +182,9 @@ LBM_API lbm_status lbm_read_mask(const char* path, int nx, int ny, int nz, int d
 /* Builds the fluid-node compaction (SP3:1018-1071), the pull neighbour table
  * with halfway bounce-back resolved (equivalent of nei_loc, SP3:1099-1151),
  * the MRT constants (Comput_MI SP3:838, init SP3:1278) and the device state.
- * The mask is copied; the caller keeps ownership. */
+ * The mask is copied; the caller keeps ownership.  The first creation on a
+ * device also pins 32 MiB of host memory for the process's field and
+ * population reads (shared by every handle, kept until the process ends). */
 LBM_API lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, int nz,
                       lbm_handle** out);
 
@@ -237,7 +239,9 @@ LBM_API lbm_status lbm_info(lbm_handle* h, int* count, double* porosity, long lo
 
 /* rho[(count+1)] and u[(count+1)*3] in reference id order (row 0 zero);
  * either pointer may be NULL.  Same values comput_macro_variables leaves in
- * the reference's rho/u arrays. */
+ * the reference's rho/u arrays.  Large host arrays are filled from pinned
+ * staging by several threads, and transparent huge pages are requested for
+ * them (madvise; their contents are not otherwise touched). */
 LBM_API lbm_status lbm_get_fields(lbm_handle* h, double* rho, double* u);
 
 /* Post-streaming populations f[(count+1)*19], reference id order -- the

@@ -173,12 +173,29 @@ __global__ void __launch_bounds__(128) cg_bc_faces_kernel(CgBcArgs a) {
   if (b >= a.nface) return;
   const int x = a.nodes[b];
   T* __restrict__ f = static_cast<T*>(a.f);
-  double F[kQ];
-  cg_pull_full<T, DEV>(f, a.table, a.npad, x, F);
   const double* __restrict__ S = a.rec;
   const size_t ns = (size_t)a.nsnap;
-  for (int o = a.op_off[b]; o < a.op_off[b + 1]; o++) {
-    const BcOp op = a.ops[o];
+  // the first operation and the neighbour's recorded rho and u it reads are
+  // loaded before the pull, so that their chain of loads (op_off -> ops ->
+  // record) overlaps the node's (nodes -> table -> f) instead of following it
+  const int o0 = a.op_off[b], o1 = a.op_off[b + 1];
+  BcOp first{};
+  double p_rn = 0.0, p_ux = 0.0, p_uy = 0.0, p_uz = 0.0;
+  if (o0 < o1) {
+    first = a.ops[o0];
+    if (first.kind == kBcPressureNbU || first.kind == kBcPressureNeq || first.kind == kBcVelocityNbRho) {
+      const size_t nb = (size_t)(first.nb < 0 ? 0 : first.nb);  // the rule's recorded neighbour
+      p_rn = S[kQ * ns + nb];
+      p_ux = S[(kQ + 1) * ns + nb];
+      p_uy = S[(kQ + 2) * ns + nb];
+      p_uz = S[(kQ + 3) * ns + nb];
+    }
+  }
+  double F[kQ];
+  cg_pull_full<T, DEV>(f, a.table, a.npad, x, F);
+  for (int o = o0; o < o1; o++) {
+    const bool pre = o == o0;
+    const BcOp op = pre ? first : a.ops[o];
     const double rb = a.face_rho[op.face];
     const double ubx = a.face_u[op.face][0], uby = a.face_u[op.face][1], ubz = a.face_u[op.face][2];
     const size_t nb = (size_t)(op.nb < 0 ? 0 : op.nb);
@@ -188,7 +205,8 @@ __global__ void __launch_bounds__(128) cg_bc_faces_kernel(CgBcArgs a) {
         for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, rb, 0.0, 0.0, 0.0);
         break;
       case kBcPressureNbU: {
-        const double ux = S[(kQ + 1) * ns + nb], uy = S[(kQ + 2) * ns + nb], uz = S[(kQ + 3) * ns + nb];
+        const double ux = pre ? p_ux : S[(kQ + 1) * ns + nb], uy = pre ? p_uy : S[(kQ + 2) * ns + nb],
+                     uz = pre ? p_uz : S[(kQ + 3) * ns + nb];
 #pragma unroll
         for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, rb, ux, uy, uz);
         break;
@@ -213,8 +231,9 @@ __global__ void __launch_bounds__(128) cg_bc_faces_kernel(CgBcArgs a) {
         break;
       }
       case kBcPressureNeq: {
-        const double ux = S[(kQ + 1) * ns + nb], uy = S[(kQ + 2) * ns + nb], uz = S[(kQ + 3) * ns + nb];
-        const double rn = S[kQ * ns + nb];
+        const double ux = pre ? p_ux : S[(kQ + 1) * ns + nb], uy = pre ? p_uy : S[(kQ + 2) * ns + nb],
+                     uz = pre ? p_uz : S[(kQ + 3) * ns + nb];
+        const double rn = pre ? p_rn : S[kQ * ns + nb];
 #pragma unroll
         for (int k = 0; k < kQ; k++) {
           const double f4 = op.nb4 >= 0 ? S[k * ns + (size_t)op.nb4] : 0.0;
@@ -235,7 +254,7 @@ __global__ void __launch_bounds__(128) cg_bc_faces_kernel(CgBcArgs a) {
         }
         break;
       case kBcVelocityNbRho: {
-        const double rn = S[kQ * ns + nb];
+        const double rn = pre ? p_rn : S[kQ * ns + nb];
 #pragma unroll
         for (int k = 0; k < kQ; k++) F[k] = cg_feq(k, rn, ubx, uby, ubz);
         break;

@@ -10,6 +10,7 @@
 #include <sys/mman.h>
 #endif
 
+#include "host_copy.h"
 #include "lbm_internal.h"
 
 namespace lbm {
@@ -59,27 +60,6 @@ PinnedStage* borrow_stage(int dev) {
 void return_stage(int dev, PinnedStage* s) {
   std::lock_guard<std::mutex> lk(g_stage_mu);
   free_stages()[dev].push_back(s);
-}
-
-// Host copy out of the staging buffer split over up to 16 threads: one
-// thread writes fresh pageable memory (page faults, the kernel zeroing each
-// page) at well under the DMA's rate.
-void copy_parallel(char* dst, const char* src, size_t bytes) {
-  static const int threads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  constexpr size_t kMinSplit = size_t(1) << 20;
-  const int nt = (int)std::min<size_t>((size_t)threads, std::max<size_t>(1, bytes / kMinSplit));
-  if (nt == 1) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  const size_t part = (bytes / nt + 63) & ~size_t(63);
-  std::vector<std::thread> workers;
-  for (int t = 1; t < nt; t++) {
-    const size_t off = std::min(bytes, t * part), len = std::min(bytes, (t + 1) * part) - off;
-    workers.emplace_back([=] { std::memcpy(dst + off, src + off, len); });
-  }
-  std::memcpy(dst, src, std::min(bytes, part));
-  for (auto& w : workers) w.join();
 }
 
 // Asks for transparent huge pages on the 2 MiB-aligned interior of a large
@@ -146,7 +126,7 @@ cudaError_t d2h_staged(void* dst, const void* src, size_t bytes, cudaStream_t st
       const size_t j = i - 1;
       e = cudaEventSynchronize(s.ev[j & 1]);
       if (e != cudaSuccess) break;
-      copy_parallel(d8 + j * PinnedStage::kChunk, static_cast<const char*>(s.buf[j & 1]), len(j));
+      host_copy::copy_parallel(d8 + j * PinnedStage::kChunk, static_cast<const char*>(s.buf[j & 1]), len(j));
     }
   }
   // no DMA into the stage may be in flight when another copy borrows it
