@@ -367,6 +367,16 @@ lbm_status lbm_cg_create_bc(const lbm_cg_params* p, const lbm_boundary* bc, cons
   compact_reference(mask, nx, ny, nz, &g);
   if (g.count == 0) return fail(LBM_ERR_ARG, "geometry has no pore cells");
   order_nodes(mask, LBM_ORDER_REFERENCE, &g);
+  // with pressure/velocity faces: the nodes a rule reads, then the nodes a
+  // rule writes, after all others (each class in reference order), so that
+  // the face passes' threads take consecutive nodes.  The reference's order
+  // runs x fastest, which puts the nodes of an x face about a row of x
+  // apart: there each of the passes' loads was a DRAM access of its own
+  // (56 MB read per pass for 19 K face nodes on 128^3).
+  if (bc) {
+    BcPlan plan;
+    bc_partition(mask, *bc, &g, &plan);
+  }
   build_pull_table(mask, &g);
   if (!build_cg_inverse(h->MI)) return fail(LBM_ERR_ARG, "colour-gradient basis inversion failed");
 

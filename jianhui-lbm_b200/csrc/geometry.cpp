@@ -373,19 +373,34 @@ void bc_node_lists(const lbm_boundary& bc, const Geometry& g, BcLists* out) {
   *out = BcLists{};
   if (!bc_active(bc) || g.count == 0) return;
   const std::vector<BcRaw> prog = bc_program(bc, &g);
-  // written nodes in order of their first operation, read nodes in order of
-  // first use; both as internal indices
+  // written nodes and read nodes, each in ascending internal index (the
+  // face passes run a thread per listed node; with the colour-gradient
+  // solver's node classes, bc_partition, these are consecutive runs).  Nodes
+  // are independent (a rule writes its own node and reads the record), so
+  // only each node's own operations keep their program order.
   std::vector<int32_t> face_of((size_t)g.count + 1, -1), snap_of((size_t)g.count + 1, -1);
+  std::vector<int32_t> targets, reads;  // reference ids
   for (const BcRaw& r : prog) {
     if (face_of[r.target] < 0) {
-      face_of[r.target] = (int32_t)out->nodes.size();
-      out->nodes.push_back(g.int_of[r.target]);
+      face_of[r.target] = 0;
+      targets.push_back(r.target);
     }
     for (int32_t id : {r.op.nb, r.op.nb4})
       if (id > 0 && snap_of[id] < 0) {
-        snap_of[id] = (int32_t)out->snap_nodes.size();
-        out->snap_nodes.push_back(g.int_of[id]);
+        snap_of[id] = 0;
+        reads.push_back(id);
       }
+  }
+  auto by_internal = [&](int32_t a, int32_t b) { return g.int_of[a] < g.int_of[b]; };
+  std::sort(targets.begin(), targets.end(), by_internal);
+  std::sort(reads.begin(), reads.end(), by_internal);
+  for (size_t i = 0; i < targets.size(); i++) {
+    face_of[targets[i]] = (int32_t)i;
+    out->nodes.push_back(g.int_of[targets[i]]);
+  }
+  for (size_t i = 0; i < reads.size(); i++) {
+    snap_of[reads[i]] = (int32_t)i;
+    out->snap_nodes.push_back(g.int_of[reads[i]]);
   }
   const size_t nf = out->nodes.size();
   out->op_off.assign(nf + 1, 0);
