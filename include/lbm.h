@@ -391,6 +391,10 @@ LBM_API void lbm_cg_destroy(lbm_cg_handle* h);
 LBM_API lbm_status lbm_cg_set_body_force(lbm_cg_handle* h, double gx, double gy, double gz, int timing);
 /* rel_perm_ift's surface-tension change (CG3:892-893) */
 LBM_API lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a);
+/* The initial velocity of init (inivx, inivy, inivz, CG3:2357-2400): every
+ * node starts from feq(1, u0) of CG3's feq and the first collision takes
+ * rho = 1, u = u0.  Only before the first step (LBM_ERR_STATE otherwise). */
+LBM_API lbm_status lbm_cg_set_initial_velocity(lbm_cg_handle* h, double ux, double uy, double uz);
 /* Comput_Perm / Comput_Saturation window (CG3:5156-5227, 5307-5361):
  * window = per_xn, per_xp, per_yn, per_yp, per_zn, per_zp; the fluxes and the
  * saturation count are divided by its volume, and the porosity (lbm_cg_info,

@@ -648,7 +648,10 @@ lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, int ny, 
   lbm_status st;
   if ((st = alloc_device(h.get())) != LBM_OK) return st;
   if (on_device) {
+    // the indexing's scratch (5 bytes per cell) lives in the second
+    // population array, which nothing reads before the first step writes it
     SetupScratch scratch;
+    scratch.borrow(h->pop[1].p, h->pop[1].bytes, (long long)nx * ny * nz, h->geo.count);
     if ((st = device_index_reference(h->mask.data(), nx, ny, nz, h->geo.count, h->table.as<int32_t>(), h->geo.npad,
                                      0, h->ref_of.as<int32_t>(), scratch, h->stream)) != LBM_OK)
       return st;

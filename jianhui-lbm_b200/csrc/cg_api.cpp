@@ -181,6 +181,7 @@ cudaError_t face_passes(lbm_cg_handle* h, int c, int given, bool pending) {
   if (pending) e = cg_bc_faces(h->f64, b, h->stream);
   if (e == cudaSuccess && h->cp.faces) {
     b.given = given == 1;
+    for (int d = 0; d < 3; d++) b.u0[d] = h->cp.u0[d];
     e = cg_bc_record(h->f64, b, h->stream);
   }
   return e;
@@ -307,6 +308,7 @@ lbm_status cg_reduce_raw(lbm_cg_handle* h, double r[8], double* rho_out, double*
   ra.n = h->geo.count;
   ra.npad = h->geo.npad;
   ra.given = h->given == 1;
+  for (int d = 0; d < 3; d++) ra.u0[d] = h->cp.u0[d];
   for (int d = 0; d < 3; d++) ra.g[d] = h->cp.gm[d];  // the pending macro step's force
   ra.flux_psi = h->prm.flux_psi;
   ra.flux_umax = h->prm.flux_umax;
@@ -702,6 +704,45 @@ lbm_status lbm_cg_set_cap_a(lbm_cg_handle* h, double cap_a) {
   return LBM_OK;
 }
 
+// feq of the colour-gradient program on the host (CG3:2503-2540), the same
+// operations as cg_feq in cg_faithful.cu: row k of M^-1 applied to the
+// equilibrium moments, summed from j = 0.
+static double cg_feq_host(const double (&mi)[kQ][kQ], int k, double rho, double ux, double uy, double uz) {
+  const double rho_0 = 1.0;
+  double meq[kQ] = {};
+  meq[0] = rho;
+  meq[3] = rho_0 * ux;
+  meq[5] = rho_0 * uy;
+  meq[7] = rho_0 * uz;
+  meq[1] = rho_0 * (ux * ux + uy * uy + uz * uz);
+  meq[9] = rho_0 * (2 * ux * ux - uy * uy - uz * uz);
+  meq[11] = rho_0 * (uy * uy - uz * uz);
+  meq[13] = rho_0 * ux * uy;
+  meq[14] = rho_0 * uy * uz;
+  meq[15] = rho_0 * ux * uz;
+  double feq = 0.0;
+  for (int j = 0; j < kQ; j++) feq = feq + mi[k][j] * meq[j];
+  return feq;
+}
+
+lbm_status lbm_cg_set_initial_velocity(lbm_cg_handle* h, double ux, double uy, double uz) {
+  lbm_status st = cg_check(h);
+  if (st != LBM_OK) return st;
+  if (h->given != 1) return fail(LBM_ERR_STATE, "lbm_cg_set_initial_velocity: only before the first step");
+  // init (CG3:2357-2400): u = (inivx, inivy, inivz) and f = feq(1, u) at
+  // every node; the first collision takes rho = 1, u = u0
+  double f0[kQ];
+  for (int q = 0; q < kQ; q++) f0[q] = cg_feq_host(h->MI, cg::of_row(q), 1.0, ux, uy, uz);
+  LBM_CUDA_TRY(launch_init_uniform(h->f64 ? Store::F64 : Store::F32, h->f[h->cur].p, h->table.as<int32_t>(),
+                                   h->geo.count, h->geo.npad, 1.0, f0, h->stream));
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->cp.u0[0] = ux;
+  h->cp.u0[1] = uy;
+  h->cp.u0[2] = uz;
+  drop_graphs(h);
+  return LBM_OK;
+}
+
 lbm_status lbm_cg_input_update(lbm_cg_handle* h, const lbm_cg_input* in) {
   lbm_status st = cg_check(h);
   if (st != LBM_OK) return st;
@@ -1036,8 +1077,6 @@ lbm_status lbm_cg_create_from_input_seeded(const char* input_path, int precision
   if (in.mix_psi_thickness > 0 && in.mix_psi_thickness >= in.nx)
     return fail(LBM_ERR_ARG, "mix_psi_thickness must be smaller than nx");
   if (in.lattice_v != 0) return fail(LBM_ERR_ARG, "lattice_v: self-defined lattice velocity is not supported");
-  if (in.inivx != 0 || in.inivy != 0 || in.inivz != 0)
-    return fail(LBM_ERR_ARG, "initial velocity: only a fluid at rest is supported");
   if (in.rel_perm_id_dir < 0 || in.rel_perm_id_dir > 2)
     return fail(LBM_ERR_ARG, "rel_perm_id_dir: 0 (off), 1 (imbibition) or 2 (drainage)");
   if (in.rel_perm_id_dir > 0 && in.rel_perm_chan_num <= 0)
@@ -1143,6 +1182,14 @@ lbm_status lbm_cg_create_from_input_seeded(const char* input_path, int precision
   // the mixture injects at the x- face (CG3:2854-2855)
   if (in.mix_psi_thickness > 0 && in.psi_xn > 0) {
     if ((st = lbm_cg_set_zero_sigma(h, in.zero_sigma_thickness)) != LBM_OK) {
+      lbm_cg_destroy(h);
+      return st;
+    }
+  }
+  // the initial velocity of init (CG3:2357-2362); a restart's checkpoint
+  // replaces the state afterwards, as Backup_init does after init
+  if (in.inivx != 0 || in.inivy != 0 || in.inivz != 0) {
+    if ((st = lbm_cg_set_initial_velocity(h, in.inivx, in.inivy, in.inivz)) != LBM_OK) {
       lbm_cg_destroy(h);
       return st;
     }

@@ -13,6 +13,7 @@ struct CgParams {
                  // right after a force change that precedes a collision)
   int body_force_phase;
   double flux_psi;
+  double u0[3];  // velocity of the initial state (inivx..z, CG3:2357-2362): rho = 1, u = u0
   // viscosity interpolation (CG3 init, delta = 0.1)
   double wl, wg, lg0, l1, l2, g1, g2, delta;
   // pressure/velocity faces: rules on at this step, face densities and
@@ -48,6 +49,7 @@ struct CgReduceArgs {
   const void* psi;
   int n, npad;
   int given;
+  double u0[3];  // u of the initial state
   double g[3];
   double flux_psi, flux_umax;
   double* rho_out;  // optional [npad] internal order
@@ -76,7 +78,8 @@ struct CgBcArgs {
   const int32_t* snap_nodes;  // [nsnap] nodes the rules read
   double* rec;              // [23][nsnap]: f_0..f_18 (CG order), rho, ux, uy, uz
   int nsnap;
-  int given;                // record pass: rho = 1, u = 0 (initial state)
+  int given;                // record pass: rho = 1, u = u0 (initial state)
+  double u0[3];
   double gm[3];             // record pass: force of the macro step
   double face_rho[6];       // xp, xn, yp, yn, zp, zn
   double face_u[6][3];

@@ -136,7 +136,9 @@ __global__ void __launch_bounds__(128) cg_bc_record_kernel(CgBcArgs a) {
   double rho, ux, uy, uz;
   if (a.given) {
     rho = 1.0;
-    ux = uy = uz = 0.0;
+    ux = a.u0[0];
+    uy = a.u0[1];
+    uz = a.u0[2];
   } else {
     double r = F[0];
 #pragma unroll

@@ -120,7 +120,9 @@ __global__ void __launch_bounds__(256) cg_collide_fast_kernel(CgArgs a) {
   if (a.given) {
     drho = 0.f;
     rho = 1.f;
-    ux = uy = uz = 0.f;
+    ux = (float)a.p.u0[0];
+    uy = (float)a.p.u0[1];
+    uz = (float)a.p.u0[2];
   } else {
     float r = f0, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll

@@ -65,7 +65,9 @@ __global__ void __launch_bounds__(256) cg_collide_kernel(CgArgs a) {
   T rho, ux, uy, uz, drho = T(0);
   if (a.given) {
     rho = T(1);
-    ux = uy = uz = T(0);
+    ux = T(a.p.u0[0]);
+    uy = T(a.p.u0[1]);
+    uz = T(a.p.u0[2]);
   } else {
     T r = FAITHFUL ? f[0] : f[0];
 #pragma unroll
@@ -279,7 +281,9 @@ __global__ void __launch_bounds__(256) cg_reduce_kernel(CgReduceArgs a) {
     T rho, ux, uy, uz;
     if (a.given) {
       rho = T(1);
-      ux = uy = uz = T(0);
+      ux = T(a.u0[0]);
+      uy = T(a.u0[1]);
+      uz = T(a.u0[2]);
     } else {
       T f[kQ];
 #pragma unroll

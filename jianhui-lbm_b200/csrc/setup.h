@@ -15,8 +15,14 @@ struct SetupScratch {
   long long cells_cap = 0;
   int coor_cap = 0;
   size_t temp_bytes = 0;
+  bool borrowed = false;  // the arrays live in a caller's buffer (see borrow)
   ~SetupScratch() { release(); }
   lbm_status reserve(long long cells, int nodes);
+  // Places the arrays in [base, base + bytes) of a device buffer that is not
+  // in use until the indexing has finished (a solver's second population
+  // array), saving their allocation and release; false when they do not fit
+  // (then reserve allocates them).
+  bool borrow(void* base, size_t bytes, long long cells, int nodes);
   void release();
 };
 

@@ -69,7 +69,32 @@ int grid_for(long long items) {
 
 }  // namespace
 
+bool SetupScratch::borrow(void* base, size_t bytes, long long cells, int nodes) {
+  if (!base || cells_cap || coor_cap || borrowed) return false;
+  size_t tb = 0;
+  if (cub::DeviceScan::ExclusiveSum(nullptr, tb, (int32_t*)nullptr, (int32_t*)nullptr, (int)cells) != cudaSuccess)
+    return false;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t need = up(sizeof(int32_t) * (size_t)cells) + up((size_t)cells) + up(tb) +
+                      up(sizeof(int32_t) * (size_t)std::max(nodes, 1));
+  if (need > bytes) return false;
+  char* p = static_cast<char*>(base);
+  cell_id = reinterpret_cast<int32_t*>(p);
+  p += up(sizeof(int32_t) * (size_t)cells);
+  mask = reinterpret_cast<uint8_t*>(p);
+  p += up((size_t)cells);
+  temp = p;
+  p += up(tb);
+  coor_x = reinterpret_cast<int32_t*>(p);
+  cells_cap = cells;
+  coor_cap = nodes;
+  temp_bytes = tb;
+  borrowed = true;
+  return true;
+}
+
 lbm_status SetupScratch::reserve(long long cells, int nodes) {
+  if (borrowed) return (cells <= cells_cap && nodes <= coor_cap) ? LBM_OK : fail(LBM_ERR_STATE, "setup scratch too small");
   if (cells > cells_cap) {
     if (cell_id) cudaFree(cell_id);
     cell_id = nullptr;
@@ -97,8 +122,10 @@ lbm_status SetupScratch::reserve(long long cells, int nodes) {
 }
 
 void SetupScratch::release() {
-  for (void* p : {(void*)cell_id, (void*)mask, temp, (void*)coor_x})
-    if (p) cudaFree(p);
+  if (!borrowed)
+    for (void* p : {(void*)cell_id, (void*)mask, temp, (void*)coor_x})
+      if (p) cudaFree(p);
+  borrowed = false;
   cell_id = nullptr;
   mask = nullptr;
   temp = nullptr;

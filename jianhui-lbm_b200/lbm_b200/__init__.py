@@ -285,6 +285,7 @@ _SIGNATURES = {
     "lbm_cg_set_body_force": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int], C.c_int),
     "lbm_cg_set_cap_a": ([C.c_void_p, C.c_double], C.c_int),
     "lbm_cg_input_update": ([C.c_void_p, C.POINTER(CGInput)], C.c_int),
+    "lbm_cg_set_initial_velocity": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
     "lbm_cg_create_bc": ([C.POINTER(CGParams), C.POINTER(Boundary), _U8P, _F64P, C.c_int, C.c_int, C.c_int,
                           C.POINTER(C.c_void_p)], C.c_int),
     "lbm_cg_set_faces": ([C.c_void_p, _F64P, _F64P, C.c_int], C.c_int),
@@ -508,6 +509,11 @@ class ColourGradient:
 
     def set_cap_a(self, cap_a):
         _check(lib().lbm_cg_set_cap_a(self._h, float(cap_a)))
+
+    def set_initial_velocity(self, u0):
+        """Start from feq(1, u0) with u = u0 in the first collision (inivx..z,
+        CG3:2357-2400); only before the first step."""
+        _check(lib().lbm_cg_set_initial_velocity(self._h, float(u0[0]), float(u0[1]), float(u0[2])))
 
     def input_update(self, path):
         """input_update (CG3:5765-5925): the INPUT file at `path` read again;

@@ -302,6 +302,9 @@ CG_RUNS = {
                                 L29=-1, L30=-1, L31=-1),
     # Sub_BC 3 velocity (density of the inner neighbour) on the x faces
     "cg_outputs_vel3.npz": dict(L8="0.0 0.0 0.0", L12="1 0.002 1 0.002", L35=3, L29=-1, L30=-1, L31=-1),
+    # initial velocity (inivx..z): every node starts from feq(1, u0), the
+    # first collision takes u = u0; reports every 25 steps, phase VTK every 50
+    "cg_outputs_iniv.npz": dict(L22="1.0e-3 -5.0e-4 2.0e-4", L27=25, L29=-1, L30=-1, L45=0),
     # capillary-pressure stepping with the face pressures along x (Sub_BC 1)
     "cg_outputs_cap_pre.npz": dict(L4=250, L6=1, L8="0.0 0.0 0.0", L9="1 1.0 1 1.0", L35=1, L27=10, L28=0,
                                    L29=-1, L30=-1, L31=-1, L58="1 1 30", L59="1.0 1.006 2e-5 3 2", L60="1e-2"),

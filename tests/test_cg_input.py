@@ -80,7 +80,6 @@ def test_phase_file_reads_as_float(L, tmp_path):
     (dict(L7=1, L17="0 -1"), "psi_xp"),
     (dict(L68=20), "mix_psi_thickness"),
     (dict(L33="1 1.0 2.0"), "lattice_v"),
-    (dict(L22="1e-3 0 0"), "initial velocity"),
     (dict(L64="3 5"), "rel_perm_id_dir"),
     (dict(L64="1 0"), "rel_perm_id_dir"),
     (dict(L58="4 1 2000"), "pressure_change2"),

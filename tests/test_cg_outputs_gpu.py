@@ -32,6 +32,8 @@ variants of INPUT_cg.dat on 14x12x10 spheres with a blob phase field:
   cg_outputs_imb.npz,    imbibition / drainage control (rel_perm_id_dir)
   cg_outputs_drain.npz   over 50 target saturations with random phase faces,
                          same seeded program.
+  cg_outputs_iniv.npz    a non-zero initial velocity (inivx..z): feq(1, u0)
+                         at every node, u = u0 in the first collision;
   cg_outputs_dyn.npz     input_dynamic: the INPUT file read again every 100
                          steps (input_update), its versions served in order
                          through a named pipe: force, CapA, wall colour,
@@ -114,7 +116,7 @@ FACES = ["cg_outputs_pre1.npz", "cg_outputs_pre2.npz", "cg_outputs_pre0.npz", "c
 @pytest.mark.parametrize("fixture", ["cg_outputs.npz", "cg_outputs_sched.npz", "cg_outputs_ramp.npz",
                                      "cg_outputs_psi.npz", "cg_outputs_cap.npz", "cg_outputs_mix.npz",
                                      "cg_outputs_psi2.npz", "cg_outputs_rand.npz", "cg_outputs_rand_buf.npz",
-                                     "cg_outputs_imb.npz", "cg_outputs_drain.npz"] + FACES)
+                                     "cg_outputs_imb.npz", "cg_outputs_drain.npz", "cg_outputs_iniv.npz"] + FACES)
 def test_cg_driver_writes_the_reference_files(L, fixture, tmp_path):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
