@@ -573,6 +573,12 @@ LBM_API lbm_status lbm_st19_create_from_flow(const lbm_st7_params* p, lbm_handle
  * 0 for a null handle. */
 LBM_API int lbm_st7_directions(lbm_st7_handle* h);
 /* collision + streaming + C = sum g (ST7:1345-1633), n times */
+/* Self-defined lattice velocity (lattice_v with dx, dt of the INPUT file,
+ * ST7:1259-1274, the D3Q19 program the same): tau_s = niu_s / (c_s^2 dt) + 1/2
+ * with c_s^2 = (dx/dt)^2 / 3, and the D3Q19 equilibrium's e.u and u.u terms
+ * divided by c2 = (dx/dt)^2 and c4 = c2^2 as the program divides them.  The
+ * default lattice is dx = dt = 1. */
+LBM_API lbm_status lbm_st7_set_lattice(lbm_st7_handle* h, double dx, double dt);
 LBM_API lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps);
 /* C per fluid node [(count+1)], reference id order, row 0 zero */
 LBM_API lbm_status lbm_st7_get_concentration(lbm_st7_handle* h, double* c);

@@ -113,7 +113,8 @@ int main(int argc, char** argv) {
   lbm_st7_input in;
   if (lbm_read_st7_input(argv[1], &in) != LBM_OK) return die("lbm_read_st7_input");
   // what the reference's loop does not run or this driver does not support
-  if (in.lattice_v != 0) return die_msg("lattice_v: self-defined lattice velocity is not supported");
+  if (in.lattice_v == 1 && !(in.dx_input > 0 && in.dt_input > 0))
+    return die_msg("lattice_v: dx and dt must be positive");
   if (in.sub_dis > 0 && in.fre_dis == 0) return die_msg("freDis = 0: the reference takes n % 0; use -1 or a positive interval");
   if (in.fre_re <= 0) return die_msg("freRe must be positive");
   if (in.fre_ve == 0 || in.fre_psi == 0 || in.fre_backup == 0)
@@ -163,6 +164,10 @@ int main(int argc, char** argv) {
   if ((lattice == 19 ? lbm_st19_create(&p, mask.data(), nx, ny, nz, u.data(), c0.data(), &h)
                      : lbm_st7_create(&p, mask.data(), nx, ny, nz, u.data(), c0.data(), &h)) != LBM_OK)
     return die("lbm_st7_create");
+  // init: dx = dt = 1 / Zoom (Zoom = 1), or the INPUT file's dx, dt with
+  // lattice_v (ST7:1259-1274)
+  const double dx = in.lattice_v == 1 ? in.dx_input : 1.0, dt = in.lattice_v == 1 ? in.dt_input : 1.0;
+  if (in.lattice_v == 1 && lbm_st7_set_lattice(h, dx, dt) != LBM_OK) return die("lbm_st7_set_lattice");
   if (in.mode_backup_ini != 0) {
     // Backup_init reads LBM_checkpoint_{psi,fg}_<m>.<rank>.bin_input from the
     // working directory, without the output prefix (ST7:3735-3740)
@@ -245,7 +250,7 @@ int main(int argc, char** argv) {
     u_max_e = v_max;
     u_ave_e = u_compt;
   }
-  const double c_s2 = 1.0 * 1.0 / 3, dt = 1.0, dx = 1.0;
+  const double lat_c = dx / dt, c_s2 = lat_c * lat_c / 3;
   // psi_total (ST7:1083-1105): every rank sums the initial concentration of
   // its pore cells (i, j, k order, the float values), rank 0 adds the ranks
   double psi_total = 0;

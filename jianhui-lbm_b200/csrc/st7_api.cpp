@@ -57,6 +57,7 @@ struct lbm_st7_handle {
   bool given = true;
   long long step = 0;
   double tau_s = 1.0;
+  double c2 = 1.0, c4 = 1.0;  // lat_c^2, lat_c^4 (lattice_v)
   double last_ms = 0;
   int nq = 7;  // 7: D3Q7 solute program, 19: D3Q19 solute program
   ~lbm_st7_handle() {
@@ -78,6 +79,8 @@ St7Args st7_args(lbm_st7_handle* h, bool given) {
   a.n = h->geo.count;
   a.npad = h->geo.npad;
   a.tau_s = h->tau_s;
+  a.c2 = h->c2;
+  a.c4 = h->c4;
   a.nq = h->nq;
   return a;
 }
@@ -200,6 +203,20 @@ lbm_status lbm_st19_create_from_flow(const lbm_st7_params* p, lbm_handle* flow, 
 }
 
 int lbm_st7_directions(lbm_st7_handle* h) { return h ? h->nq : 0; }
+
+lbm_status lbm_st7_set_lattice(lbm_st7_handle* h, double dx, double dt) {
+  if (!h) return fail(LBM_ERR_ARG, "null solute handle");
+  if (!(dx > 0) || !(dt > 0)) return fail(LBM_ERR_ARG, "lbm_st7_set_lattice: dx and dt must be positive");
+  // init with lattice_v (ST7:1259-1274; ST19 the same): lat_c = dx / dt,
+  // c_s^2 = lat_c^2 / 3, tau_s = niu_s / (c_s^2 dt) + 1/2; the D3Q19
+  // equilibrium divides by c2 = lat_c^2 and c4 = c2^2
+  const double lat_c = dx / dt;
+  const double c_s2 = lat_c * lat_c / 3;
+  h->tau_s = h->prm.diffusivity / (c_s2 * dt) + 0.5;
+  h->c2 = lat_c * lat_c;
+  h->c4 = h->c2 * h->c2;
+  return LBM_OK;
+}
 
 lbm_status lbm_st7_step(lbm_st7_handle* h, int nsteps) {
   if (!h || nsteps < 0) return fail(LBM_ERR_ARG, "lbm_st7_step: bad argument");

@@ -14,6 +14,7 @@ struct St7Args {
   void* c_out;            // optional [npad]: C of this step's macro
   int n, npad;
   double tau_s;
+  double c2, c4;          // lat_c^2 and lat_c^4 of the D3Q19 equilibrium (1 on the default lattice)
   int nq;                 // 7 (D3Q7, g as [6][npad]) or 19 (D3Q19, g as [19][npad])
 };
 

@@ -71,7 +71,10 @@ __device__ __forceinline__ double st19_edot(double ux, double uy, double uz) {
   return s;
 }
 
-template <typename T, bool GIVEN>
+// UNIT: the default lattice (lat_c = 1), where the program's divisions by
+// c2 = c4 = 1 are exact and left out; otherwise (lattice_v, ST19:1259-1268)
+// 3 e.u / c2, 4.5 (e.u)^2 / c4 and 1.5 u.u / c2 as the program writes them.
+template <typename T, bool GIVEN, bool UNIT>
 __global__ void __launch_bounds__(256) st19_step_kernel(St7Args a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= a.n) return;
@@ -96,7 +99,9 @@ __global__ void __launch_bounds__(256) st19_step_kernel(St7Args a) {
   const T uu = ux * ux + uy * uy + uz * uz;
   const T tau = T(a.tau_s);
   {
-    const T eq = T(weight(0)) * C * (T(1) - T(1.5) * uu);
+    const T eq = UNIT ? T(weight(0)) * C * (T(1) - T(1.5) * uu)
+                      : T(weight(0)) * C * (T(1) + T(3) * T(0) / T(a.c2) + T(4.5) * T(0) * T(0) / T(a.c4) -
+                                            T(1.5) * uu / T(a.c2));
     dst[x] = g[0] - (g[0] - eq) / tau;
   }
 #pragma unroll
@@ -120,7 +125,9 @@ __global__ void __launch_bounds__(256) st19_step_kernel(St7Args a) {
     if (q == 16) eu = (T)st19_edot<16>(ux, uy, uz);
     if (q == 17) eu = (T)st19_edot<17>(ux, uy, uz);
     if (q == 18) eu = (T)st19_edot<18>(ux, uy, uz);
-    const T eq = T(weight(q)) * C * (T(1) + T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu);
+    const T eq = UNIT ? T(weight(q)) * C * (T(1) + T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu)
+                      : T(weight(q)) * C * (T(1) + T(3) * eu / T(a.c2) + T(4.5) * eu * eu / T(a.c4) -
+                                            T(1.5) * uu / T(a.c2));
     dst[(size_t)q * npad + x] = g[q] - (g[q] - eq) / tau;
   }
 }
@@ -129,10 +136,12 @@ template <typename T>
 cudaError_t launch_step19(const St7Args& a, cudaStream_t st) {
   if (a.n == 0) return cudaSuccess;
   const int g = (a.n + 255) / 256;
+  const bool unit = a.c2 == 1.0 && a.c4 == 1.0;
   if (a.c_given != nullptr)
-    st19_step_kernel<T, true><<<g, 256, 0, st>>>(a);
+    unit ? st19_step_kernel<T, true, true><<<g, 256, 0, st>>>(a) : st19_step_kernel<T, true, false><<<g, 256, 0, st>>>(a);
   else
-    st19_step_kernel<T, false><<<g, 256, 0, st>>>(a);
+    unit ? st19_step_kernel<T, false, true><<<g, 256, 0, st>>>(a)
+         : st19_step_kernel<T, false, false><<<g, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 

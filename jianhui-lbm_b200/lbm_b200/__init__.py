@@ -310,6 +310,7 @@ _SIGNATURES = {
     "lbm_st19_create": ([C.c_void_p, _U8P, C.c_int, C.c_int, C.c_int, _F64P, _F64P, C.POINTER(C.c_void_p)], C.c_int),
     "lbm_st19_create_from_flow": ([C.c_void_p, C.c_void_p, _F64P, C.POINTER(C.c_void_p)], C.c_int),
     "lbm_st7_directions": ([C.c_void_p], C.c_int),
+    "lbm_st7_set_lattice": ([C.c_void_p, C.c_double, C.c_double], C.c_int),
     "lbm_st7_step": ([C.c_void_p, C.c_int], C.c_int),
     "lbm_st7_get_concentration": ([C.c_void_p, _F64P], C.c_int),
     "lbm_st7_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_double)], C.c_int),
@@ -398,6 +399,11 @@ class Solute:
         c, st, ms = C.c_int(), C.c_longlong(), C.c_double()
         _check(lib().lbm_st7_info(h, C.byref(c), C.byref(st), C.byref(ms)))
         self.count = c.value
+
+    def set_lattice(self, dx, dt):
+        """Self-defined lattice velocity (lattice_v, dx, dt): tau_s and the
+        D3Q19 equilibrium's c2 = (dx/dt)^2, c4 = c2^2 as the program sets them."""
+        _check(lib().lbm_st7_set_lattice(self._h, float(dx), float(dt)))
 
     def step(self, n=1):
         _check(lib().lbm_st7_step(self._h, int(n)))

@@ -569,7 +569,7 @@ def st7_fixture(out=None, program="ref_st7_slab"):
     print("st7_slab", mask.shape, [v.size // 3 for v in vel])
 
 
-def st7_program_outputs(program="ref_st7_slab", tag="st7", variants=True):
+def st7_program_outputs(program="ref_st7_slab", tag="st7", variants=True, only=None):
     """The solute program itself at two ranks (multi-process MPI stand-in):
     every file it writes, for the drop-in driver's byte-for-byte test.  The
     slab single-phase program first makes the flow of the st7_slab geometry
@@ -605,13 +605,20 @@ def st7_program_outputs(program="ref_st7_slab", tag="st7", variants=True):
         open(os.path.join(d, "phase.dat"), "w").write(phase)
         # dispersion statistics along x every 20 steps (written after step 10)
         # and along z every 40, both layouts of the run above
-        runs = {f"{tag}_outputs.npz": ("./st_", dict(L29=1))}
+        runs = {f"{tag}_outputs.npz": ("./st_", dict(L29=1)),
+                # self-defined lattice velocity dx = 1, dt = 2 (tau_s, the
+                # report's Peclet and Courant numbers, the dispersion
+                # statistics along x every 20 steps; for D3Q19 also the
+                # equilibrium's divisions by lat_c^2, lat_c^4)
+                f"{tag}_outputs_lat.npz": ("./sl_", dict(L29=1, L33="1 20", L35="1 1.0 2.0"))}
         if variants:
             runs.update({"st7_outputs_b.npz": ("./sb_", dict(L29=0)),
                          "st7_outputs_dis.npz": ("./sd_", dict(L29=1, L33="1 20", L39=10)),
                          "st7_outputs_dis3.npz": ("./sz_", dict(L29=0, L33="3 40", L39=-1, L40="0 1 0",
                                                                  L42="8 2"))})
         for fname, (prefix, kv) in runs.items():
+            if only and only not in fname:
+                continue
             base = dict(L1="mask.dat", L2="phase.dat", L3=f"{nx} {ny} {nz}", L4=60, L7="0.0 0.5", L23=ST7_D,
                         L28=20, L30=40, L32=20, L33="0 1000", L36=prefix, L45=40, L47=100)
             base.update(kv)
@@ -619,6 +626,8 @@ def st7_program_outputs(program="ref_st7_slab", tag="st7", variants=True):
             open(os.path.join(d, "INPUT_st.dat"), "w").write(text)
             assert oracle.run_ranks(st, ["INPUT_st.dat"], ST7_NRANKS, d) == [0] * ST7_NRANKS
             save_st7(fname, mask, phase, text, vel, collect_cg(d, prefix[2:], fg_width=19 if tag == "st19" else 7))
+        if only and only not in f"{tag}_outputs_restart.npz":
+            return
         for r in range(ST7_NRANKS):
             for what in ("psi", "fg"):
                 shutil.copy(os.path.join(d, f"st_LBM_checkpoint_{what}_40.{r}.bin_input"),
@@ -686,17 +695,19 @@ def main():
     ap.add_argument("--cg", action="store_true")
     ap.add_argument("--outputs", action="store_true")
     ap.add_argument("--cg-outputs", action="store_true")
-    ap.add_argument("--only", default=None, help="--cg-outputs: runs whose fixture name contains this")
+    ap.add_argument("--only", default=None,
+                    help="--cg-outputs / --st7-outputs / --st19: runs whose fixture name contains this")
     ap.add_argument("--st7-outputs", action="store_true")
     ap.add_argument("--st19", action="store_true", help="D3Q19 solute program fixtures")
     a = ap.parse_args()
     oracle.build()
     if a.st7_outputs:
-        st7_program_outputs()
+        st7_program_outputs(only=a.only)
         return
     if a.st19:
-        st7_fixture(os.path.join(HERE, "st19_slab.npz"), program="ref_st19_slab")
-        st7_program_outputs(program="ref_st19_slab", tag="st19", variants=False)
+        if not a.only:
+            st7_fixture(os.path.join(HERE, "st19_slab.npz"), program="ref_st19_slab")
+        st7_program_outputs(program="ref_st19_slab", tag="st19", variants=False, only=a.only)
         return
     if a.cg_outputs:
         cg_program_outputs(a.only)

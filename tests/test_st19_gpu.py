@@ -8,7 +8,9 @@ stand-in, oracle/_ref/ref_st19_slab), on the inputs of the D3Q7 fixtures:
   st19_outputs.npz          every file of a 61-step run (reports every 20,
                             velocity VTK every 40, concentration VTK every 20,
                             checkpoints every 40);
-  st19_outputs_restart.npz  the run restarted from the step-40 checkpoint.
+  st19_outputs_restart.npz  the run restarted from the step-40 checkpoint;
+  st19_outputs_lat.npz      a run with a self-defined lattice velocity
+                            (dx = 1, dt = 2) and dispersion statistics.
 FP64: bit for bit / byte for byte.  FP32: concentration within 1e-5 of the
 FP64 fixture after 61 steps.
 """
@@ -127,6 +129,16 @@ def test_st19_driver_writes_the_reference_files(L, tmp_path):
     prepare(tmp_path, golden)
     run_driver(L, tmp_path)
     compare(tmp_path, golden, "st_")
+
+
+def test_st19_driver_with_lattice_velocity(L, tmp_path):
+    """lattice_v with dx = 1, dt = 2: tau_s from c_s^2 = (dx/dt)^2 / 3 and the
+    equilibrium's divisions by c2, c4 (ST19:1259-1268, 1480), the reports'
+    Peclet and Courant numbers and the dispersion statistics in dx, dt."""
+    golden = np.load(os.path.join(GOLDEN, "st19_outputs_lat.npz"))
+    prepare(tmp_path, golden)
+    run_driver(L, tmp_path)
+    compare(tmp_path, golden, "sl_")
 
 
 def test_st19_driver_restart_matches_the_reference_restart(L, tmp_path):

@@ -5,8 +5,9 @@ wrote at two ranks from the flow the slab single-phase program made
 (Velocity_for_solute_100.<rank>.bin, stored with them): reports every 20
 steps, velocity VTK every 40, concentration VTK every 20 and per-rank
 checkpoints every 40 in both output layouts (Out_Mode 1 and 0), the
-dispersion statistics along x and along z, and a restart from the step-40
-checkpoint.  The driver, run on the same files with
+dispersion statistics along x and along z, a self-defined lattice velocity
+(lattice_v, dx = 1, dt = 2; st7_outputs_lat.npz), and a restart from the
+step-40 checkpoint.  The driver, run on the same files with
 --ranks 2 at FP64, must write the same files: text and VTK byte for byte
 except the wall-clock lines, the per-rank checkpoints bit for bit (rows 1..).
 """
@@ -74,7 +75,8 @@ def compare(tmp_path, golden, prefix):
 
 
 @pytest.mark.parametrize("fixture,prefix", [("st7_outputs.npz", "st_"), ("st7_outputs_b.npz", "sb_"),
-                                            ("st7_outputs_dis.npz", "sd_"), ("st7_outputs_dis3.npz", "sz_")])
+                                            ("st7_outputs_dis.npz", "sd_"), ("st7_outputs_dis3.npz", "sz_"),
+                                            ("st7_outputs_lat.npz", "sl_")])
 def test_st7_driver_writes_the_reference_files(L, fixture, prefix, tmp_path):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
