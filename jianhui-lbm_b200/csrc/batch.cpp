@@ -141,17 +141,15 @@ struct Pool {
     graphs.clear();
   }
 
-  // Step grid of a chain: one block per work item (block nodes of a
-  // stepping tile), rounded up to a power of two, at most the pool's full
-  // grid.  Any grid is correct (the kernel strides); this one neither idles
-  // blocks on a small stepping set nor starves a large one.
+  // Step grid of a chain: one block per stepping tile, rounded up to a power
+  // of two (one captured graph per grid), at most the pool's full grid.
   int chain_grid() const {
     long long tiles = 0;
     for (int i = 0; i < nslots; i++)
       if (slot_job[i] && h_state[i].active) tiles += h_inst[i].tile_end - h_inst[i].tile_begin;
-    const long long items = std::max(1LL, tiles * (kTile / block));
+    tiles = std::max(1LL, tiles);
     long long g = 1;
-    while (g < items) g <<= 1;
+    while (g < tiles) g <<= 1;
     return (int)std::min<long long>(g, grid);
   }
 

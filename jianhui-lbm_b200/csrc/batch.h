@@ -85,8 +85,8 @@ cudaError_t launch_batch_export_macro(Store kind, const void* pop, const int32_t
                                       cudaStream_t st);
 cudaError_t launch_batch_init(Store kind, void* pop, const int32_t* table, int cap, int begin, int n,
                               const InstParams& ip, cudaStream_t st);
-// Largest step grid of a pool: one block per work item (block nodes of a
-// tile) of every tile of the pool.
+// Largest step grid of a pool: one block per tile of the pool (a block steps
+// its tile in kTile / block passes).
 int batch_step_grid(int ntiles, int block);
 
 // The 18 table rows [18][g.count] of one instance placed at node `begin` of a

@@ -21,14 +21,13 @@
 
 namespace lbm {
 
-// Work item = BS nodes of a stepping tile (the tiles in the active list
-// order, kTile / BS items per tile); block b takes item b.  The host launches
-// at least as many blocks as there are stepping items (a power of two at or
-// above their count, chain_grid), and the list kernels fill the entries past
-// the stepping tiles with an empty node range, so a block needs no count of
-// the stepping tiles: its population gathers wait on the single broadcast
-// load of its own entry (the single-domain step waits on none), and the
-// blocks past the list read an empty entry and exit.
+// Block b steps tile b of the work list (the stepping tiles in list order):
+// kTile / BS passes of BS nodes, all on the one broadcast load of the tile's
+// entry (the single-domain step waits on none).  The host launches at least
+// as many blocks as there are stepping tiles (a power of two at or above
+// their count, chain_grid), and the list kernels fill the entries past the
+// stepping tiles with an empty node range, so a block needs no count of the
+// stepping tiles: the blocks past the list read an empty entry and exit.
 template <Store K, int BS>
 __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
   using T = typename Traits<K>::T;
@@ -37,14 +36,14 @@ __global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int cha
   const T* __restrict__ src = static_cast<const T*>(a.src_pop);
   T* __restrict__ dst = static_cast<T*>(a.dst_pop);
   const size_t cap = (size_t)a.cap;
-  {
-    const int it = blockIdx.x;
-    const int i = it / kSub;
-    if (i >= a.ntiles) return;
-    const TileWork w = a.work[i];
-    const int p = w.p0 + (it - i * kSub) * BS + threadIdx.x;
+  const int i = blockIdx.x;
+  if (i >= a.ntiles) return;
+  const TileWork w = a.work[i];
+  const float scale = w.fp16_scale, inv_scale = 1.0f / w.fp16_scale;
+#pragma unroll 1
+  for (int sub = 0; sub < kSub; sub++) {
+    const int p = w.p0 + sub * BS + threadIdx.x;
     if (p >= w.end) return;
-    const float scale = w.fp16_scale, inv_scale = 1.0f / w.fp16_scale;
     A f[kQ];
     f[0] = load_pop<K>(src + p, inv_scale);
 #pragma unroll
@@ -139,9 +138,8 @@ __global__ void __launch_bounds__(256) batch_work_kernel(BatchReduceArgs a, int 
 }
 
 cudaError_t launch_batch_list(const BatchReduceArgs& a, int step_grid, int block, cudaStream_t st) {
-  const int b = (block == 128 || block == 512) ? block : 256;
-  const int per_tile = kTile / b;
-  const int fill_to = std::min(a.ntiles, (step_grid + per_tile - 1) / per_tile);
+  (void)block;
+  const int fill_to = std::min(a.ntiles, step_grid);  // one block per tile
   batch_slot_scan_kernel<<<1, 1024, 0, st>>>(a);
   const int g = std::max(1, std::min((fill_to + 255) / 256, 4 * 148));
   batch_work_kernel<<<g, 256, 0, st>>>(a, fill_to);
@@ -291,12 +289,11 @@ static cudaError_t step_k(const BatchStepArgs& a, int block, int grid, int chain
 }
 
 int batch_step_grid(int ntiles, int block) {
-  // one block per work item of the whole pool: with every tile stepping no
-  // block loops (each item's gathers wait only on its own list entry); the
-  // chains of a partly stepping pool launch a power of two at or above their
-  // item count (chain_grid), the extra blocks find no item and exit
-  const int b = (block == 128 || block == 512) ? block : 256;
-  return (int)std::max(1LL, (long long)ntiles * (kTile / b));
+  // one block per tile of the whole pool; the chains of a partly stepping
+  // pool launch a power of two at or above their stepping tile count
+  // (chain_grid), the extra blocks find an empty entry and exit
+  (void)block;
+  return std::max(1, ntiles);
 }
 
 cudaError_t launch_batch_step(Store kind, const BatchStepArgs& a, int block, int grid, int chain_step,
