@@ -34,10 +34,11 @@ static Store store_of(int precision) {
   }
 }
 
-// feq of `feq` (SP3:1382-1394), lattice units.
-static double feq_ref(int q, double rho, const double* u) {
-  const double c2 = 1.0 * 1.0, c4 = c2 * c2;
-  const double eu = (double)cx(q) * u[0] + (double)cy(q) * u[1] + (double)cz(q) * u[2];
+// feq of `feq` (SP3:1382-1394) on the lattice L (elat = e lat_c).
+static double feq_ref(int q, double rho, const double* u, const Lattice& L) {
+  const double c2 = L.c2, c4 = L.c4;
+  const double ex = (double)cx(q) * L.c, ey = (double)cy(q) * L.c, ez = (double)cz(q) * L.c;
+  const double eu = ex * u[0] + ey * u[1] + ez * u[2];
   const double uv = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
   return weight(q) * rho * (1.0 + 3.0 * eu / c2 + 4.5 * eu * eu / c4 - 1.5 * uv / c2);
 }
@@ -116,6 +117,7 @@ struct lbm_handle {
   std::vector<uint8_t, UninitAlloc<uint8_t>> mask;
   Geometry geo;
   MrtConstants mrt{};
+  Lattice lat;  // self-defined lattice velocity (lbm_set_lattice); default lattice otherwise
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -299,7 +301,7 @@ lbm_status alloc_device(lbm_handle* h) {
 
 lbm_status init_state(lbm_handle* h) {
   double feq[kQ];
-  for (int q = 0; q < kQ; q++) feq[q] = feq_ref(q, 1.0, h->prm.u_init);
+  for (int q = 0; q < kQ; q++) feq[q] = feq_ref(q, 1.0, h->prm.u_init, h->lat);
   LBM_CUDA_TRY(launch_init_uniform(h->kind, h->pop[0].p, h->table.as<int32_t>(), h->geo.count, h->geo.npad,
                                    h->fp16_scale, feq, h->stream));
   LBM_CUDA_TRY(launch_fill_macro(h->kind, h->rho_given.p, h->u_given.p, h->geo.count, h->geo.npad, 1.0,
@@ -313,6 +315,16 @@ lbm_status init_state(lbm_handle* h) {
   return LBM_OK;
 }
 
+// The force as the step and reduce kernels take it: g itself for the FP64
+// reference kernel, dt g / lat_c for the kernels that work in units of lat_c
+// (g on the default lattice).
+void kernel_force(const lbm_handle* h, double* gx, double* gy, double* gz) {
+  const double s = (h->lat.on && h->kind != Store::F64) ? h->lat.dt / h->lat.c : 1.0;
+  *gx = h->lat.on ? h->prm.gx * s : h->prm.gx;
+  *gy = h->lat.on ? h->prm.gy * s : h->prm.gy;
+  *gz = h->lat.on ? h->prm.gz * s : h->prm.gz;
+}
+
 StepArgs step_args(lbm_handle* h, bool write) {
   StepArgs a{};
   a.src_pop = h->pop[h->cur].p;
@@ -324,9 +336,8 @@ StepArgs step_args(lbm_handle* h, bool write) {
   a.u_in = h->given_macro ? h->u_given.p : nullptr;
   a.rho_out = write ? h->rho_prev.p : nullptr;
   a.u_out = write ? h->u_prev.p : nullptr;
-  a.gx = h->prm.gx;
-  a.gy = h->prm.gy;
-  a.gz = h->prm.gz;
+  kernel_force(h, &a.gx, &a.gy, &a.gz);
+  a.lat = h->lat;
   a.s_v = h->mrt.s_v;
   a.s_o = h->mrt.s_o;
   a.fp16_scale = h->fp16_scale;
@@ -481,9 +492,8 @@ lbm_status reduce_raw(lbm_handle* h, double r[8], double* rho_out_int, double* u
   a.u_prev = (!h->given_macro && h->uprev_valid) ? h->u_prev.p : nullptr;
   a.last_p = h->last_p;
   a.window = h->geo.in_window.empty() ? nullptr : h->window.as<uint8_t>();
-  a.gx = h->prm.gx;
-  a.gy = h->prm.gy;
-  a.gz = h->prm.gz;
+  kernel_force(h, &a.gx, &a.gy, &a.gz);
+  a.lat = h->lat;
   a.fp16_scale = h->fp16_scale;
   a.rho_out = rho_out_int;
   a.u_out = u_out_int;
@@ -514,7 +524,7 @@ void fill_diag(lbm_handle* h, const double r[8], lbm_diag* d) {
     const bool full = w[0] < 0 && w[1] < 0 && w[2] < 0 && w[3] < 0 && w[4] < 0 && w[5] < 0;
     const int ext[3] = {g.nx, g.ny, g.nz};
     const int L = full ? ext[dir] : w[2 * dir + 1] - w[2 * dir] + 1;
-    const double c_s2 = 1.0 * 1.0 / 3, dx = 1.0;
+    const double c_s2 = h->lat.cs2, dx = h->lat.dx;
     dp = std::fabs(h->prm.bc.rho[2 * dir] - h->prm.bc.rho[2 * dir + 1]) * c_s2 / L / dx;
   }
   const double gg[3] = {h->prm.gx, h->prm.gy, h->prm.gz};
@@ -686,7 +696,8 @@ lbm_status lbm_create_from_input(const char* input_path, int precision, int orde
   if (st != LBM_OK) return st;
   if (parsed_out) *parsed_out = in;
   if (in.nnf_module != 0) return fail(LBM_ERR_ARG, "non-Newtonian module is not supported");
-  if (in.lattice_v != 0) return fail(LBM_ERR_ARG, "self-defined lattice velocity is not supported");
+  if (in.lattice_v == 1 && !(in.dx_input > 0 && in.dt_input > 0))
+    return fail(LBM_ERR_ARG, "lattice_v: dx and dt must be positive");
   std::vector<uint8_t> mask((size_t)in.nx * in.ny * in.nz);
   // the geometry path is relative to the working directory, as in the reference
   st = read_mask_file(in.geometry_file, in.nx, in.ny, in.nz, in.decbin, mask.data());
@@ -725,7 +736,33 @@ lbm_status lbm_create_from_input(const char* input_path, int precision, int orde
     p.window[4] = in.par_per_z ? in.per_zn : 0;
     p.window[5] = in.par_per_z ? in.per_zp : in.nz - 1;
   }
-  return lbm_create(&p, mask.data(), in.nx, in.ny, in.nz, out);
+  if ((st = lbm_create(&p, mask.data(), in.nx, in.ny, in.nz, out)) != LBM_OK) return st;
+  // self-defined lattice velocity (SP3:1286-1296; lattice_v == 1 as in the
+  // reference's init)
+  if (in.lattice_v == 1 && (st = lbm_set_lattice(*out, in.dx_input, in.dt_input)) != LBM_OK) {
+    lbm_destroy(*out);
+    *out = nullptr;
+  }
+  return st;
+}
+
+lbm_status lbm_set_lattice(lbm_handle* h, double dx, double dt) {
+  lbm_status st = check_handle(h);
+  if (st != LBM_OK) return st;
+  if (!(dx > 0) || !(dt > 0) || !std::isfinite(dx / dt)) return fail(LBM_ERR_ARG, "lbm_set_lattice: dx and dt must be positive");
+  if (h->bc.active)
+    return fail(LBM_ERR_ARG, "lbm_set_lattice: a self-defined lattice velocity with pressure/velocity faces is not supported");
+  if (h->step != 0 || !h->given_macro) return fail(LBM_ERR_STATE, "lbm_set_lattice: call before the first step");
+  MrtConstants m;
+  if (!build_mrt_constants(h->prm.nu, &m, dx, dt)) return fail(LBM_ERR_ARG, "moment matrix inversion failed");
+  h->lat = make_lattice(dx, dt);
+  h->mrt.s_v = m.s_v;
+  h->mrt.s_o = m.s_o;
+  for (int k = 0; k < kQ; k++) h->mrt.S[k] = m.S[k];
+  h->drop_graphs();
+  if ((st = init_state(h)) != LBM_OK) return st;
+  LBM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
 }
 
 void lbm_destroy(lbm_handle* h) {
@@ -1090,7 +1127,7 @@ static double sp_dp(const lbm_handle* h) {
   if (h->prm.bc.in_bc == 0) return 0.0;
   const int dir = (h->prm.perdir >= 1 && h->prm.perdir <= 3) ? h->prm.perdir - 1 : 0;
   const int ext[3] = {h->geo.nx, h->geo.ny, h->geo.nz};
-  const double c_s2 = 1.0 * 1.0 / 3, dx = 1.0;
+  const double c_s2 = h->lat.cs2, dx = h->lat.dx;
   return std::fabs(h->prm.bc.rho[2 * dir] - h->prm.bc.rho[2 * dir + 1]) * c_s2 / ext[dir] / dx;
 }
 

@@ -111,6 +111,41 @@ __device__ __forceinline__ void macro_faithful(const double (&f)[kQ], double hgx
   uz = (z + hgz) / r;
 }
 
+// j = sum_q e_q lat_c f_q of a self-defined lattice (SP3:2421-2426 with
+// elat = e lat_c): each product is rounded on its own, (-lat_c) f is exactly
+// -(lat_c f), and the products of zero components add +-0.
+__device__ __forceinline__ void lattice_momentum(const double (&f)[kQ], double c, double& jx, double& jy,
+                                                 double& jz) {
+  double x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll
+  for (int q = 0; q < kQ; q++) {
+    if (cx(q) == 1) x = x + c * f[q];
+    if (cx(q) == -1) x = x - c * f[q];
+    if (cy(q) == 1) y = y + c * f[q];
+    if (cy(q) == -1) y = y - c * f[q];
+    if (cz(q) == 1) z = z + c * f[q];
+    if (cz(q) == -1) z = z - c * f[q];
+  }
+  jx = x;
+  jy = y;
+  jz = z;
+}
+
+// macro_faithful on a self-defined lattice: u = (j + dt g / 2) / rho, the
+// caller passing hg = dt g / 2 as the reference rounds it.
+__device__ __forceinline__ void macro_faithful_lat(const double (&f)[kQ], double c, double hgx, double hgy,
+                                                   double hgz, double& rho, double& ux, double& uy, double& uz) {
+  double r = f[0];
+#pragma unroll
+  for (int q = 1; q < kQ; q++) r = r + f[q];
+  double x, y, z;
+  lattice_momentum(f, c, x, y, z);
+  rho = r;
+  ux = (x + hgx) / r;
+  uy = (y + hgy) / r;
+  uz = (z + hgz) / r;
+}
+
 // ----------------------------------------------------------------------------
 // Deviation-form macro step: f = w + delta, rho = 1 + sum delta, j = sum e delta
 // (sum w e = 0), u = (j + g/2) / rho.  s/d are the opposite-pair sums and
@@ -329,16 +364,21 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(ReduceArgs a) {
           f[q] = load_pop<K>(pop + __ldg(a.table + (size_t)(q - 1) * a.npad + p), inv_scale);
       }
       if constexpr (K == Store::F64) {
-        macro_faithful(f, a.gx / 2, a.gy / 2, a.gz / 2, rho, ux, uy, uz);
+        if (a.lat.on)
+          macro_faithful_lat(f, a.lat.c, a.lat.dt * a.gx / 2, a.lat.dt * a.gy / 2, a.lat.dt * a.gz / 2, rho, ux,
+                             uy, uz);
+        else
+          macro_faithful(f, a.gx / 2, a.gy / 2, a.gz / 2, rho, ux, uy, uz);
       } else {
+        // units of lat_c (g is dt g / lat_c), scaled back to the velocity
         PairSplit<A> ps;
         split_pairs(f, ps);
         A drho, r, x, y, z;
         macro_dev<A>(f, ps, A(a.gx / 2), A(a.gy / 2), A(a.gz / 2), drho, r, x, y, z);
         rho = r;
-        ux = x;
-        uy = y;
-        uz = z;
+        ux = (double)x * a.lat.c;
+        uy = (double)y * a.lat.c;
+        uz = (double)z * a.lat.c;
       }
     }
     if (a.rho_out) a.rho_out[p] = rho;

@@ -87,7 +87,26 @@ struct MrtConstants {
   double S[kQ];
   double s_v, s_o;
 };
-bool build_mrt_constants(double nu, MrtConstants* out);
+// Rates for a lattice of spacing dx and time step dt (the reference's init:
+// lat_c = dx / dt, c_s2 = lat_c^2 / 3, tau = nu / (c_s2 dt) + 0.5); dx = dt = 1
+// is the default lattice.
+bool build_mrt_constants(double nu, MrtConstants* out, double dx = 1.0, double dt = 1.0);
+
+// Self-defined lattice velocity (lattice_v with dx, dt; SP3:1286-1296,
+// 1326-1330, 1382-1394, 1423-1500, 2414-2439): the discrete velocities are
+// e lat_c, the equilibrium divides by c2 = lat_c^2 and c4 = c2^2, the Guo
+// force by c_s2 and c_s2^2, the forcing enters the moments as dt F and the
+// velocity as dt g / 2.  on = 0 is the default lattice (lat_c = dt = 1),
+// for which the kernels keep their unit-lattice arithmetic.
+struct Lattice {
+  int on = 0;
+  double c = 1.0;              // lat_c = dx / dt
+  double ic = 1.0;             // 1 / lat_c
+  double cs2 = 1.0 * 1.0 / 3;  // c_s^2 = lat_c^2 / 3
+  double c2 = 1.0, c4 = 1.0;   // lat_c^2, lat_c^4 (feq)
+  double dt = 1.0, dx = 1.0;
+};
+Lattice make_lattice(double dx, double dt);
 
 // ---------------------------------------------------------------- geometry
 struct Geometry {
@@ -232,6 +251,12 @@ struct StepArgs {
   const int32_t* ct_base;
   const uint16_t* ct_off;
   int nwarps;
+  // lattice of the step.  The FP64 reference kernel takes g above as given
+  // and does the reference's lattice arithmetic; the deviation-storage
+  // kernels work in units of lat_c (g above is dt g / lat_c, the macro
+  // arrays rho_in/u_in/u_out hold the velocity itself: read times 1/lat_c,
+  // written times lat_c)
+  Lattice lat;
 };
 cudaError_t launch_step(Store kind, const StepArgs& a, int block, cudaStream_t st);
 // Builds the compact pull table from `table` ([18][npad], n fluid nodes);
@@ -273,6 +298,7 @@ struct ReduceArgs {
   double* result;         // [8]
   int n_main;             // nodes [n_main, n) read their populations from bnd_f
   const double* bnd_f;    // [19][n - n_main] post-rule populations, or null
+  Lattice lat;            // as StepArgs::lat (gx.. follow the same convention)
 };
 // result: t1, t2, t3, umax2, Qx, Qy, Qz, mass
 cudaError_t launch_reduce(Store kind, const ReduceArgs& a, cudaStream_t st);

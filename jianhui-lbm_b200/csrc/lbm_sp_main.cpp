@@ -118,8 +118,11 @@ int main(int argc, char** argv) {
   { std::ofstream(f_vel, std::ios::out); }
 
   const double reso2k = in.reso * in.reso * 1000;
-  const double s_v = 1.0 / (in.in_vis / (1.0 * 1.0 / 3 * 1.0) + 0.5);
-  const double dt = 1.0, dx = 1.0;
+  // init's lattice (SP3:1286-1298): dx, dt of a self-defined lattice
+  // velocity, else 1; s_v = 1 / tau_f with tau_f = nu / (c_s^2 dt) + 0.5
+  const double dt = in.lattice_v == 1 ? in.dt_input : 1.0, dx = in.lattice_v == 1 ? in.dx_input : 1.0;
+  const double lat_c = dx / dt, c_s2 = lat_c * lat_c / 3;
+  const double s_v = 1 / (in.in_vis / (c_s2 * dt) + 0.5);
   double perm[3] = {0, 0, 0}, error_perm = 0, u_max = 0, error = 0, u_ave = 0, pre_u_ave = 0, Re = 0;
   int the = 0, tme = 0, tse = 0, th = 0, tm = 0, ts = 0;
   int u_max_ref = 0;

@@ -68,14 +68,14 @@ bool build_cg_inverse(double MI[kQ][kQ]) {
   return true;
 }
 
-// Rates of `init` (SP3:1289-1322): lattice units (dx = dt = 1, c_s^2 = 1/3).
-bool build_mrt_constants(double nu, MrtConstants* out) {
+// Rates of `init` (SP3:1286-1322) for a lattice of spacing dx and step dt.
+bool build_mrt_constants(double nu, MrtConstants* out, double dx, double dt) {
   for (int k = 0; k < kQ; k++)
     for (int q = 0; q < kQ; q++) out->M[k][q] = mcoef(k, q);
   for (int k = 0; k < kQ; k++)
     for (int q = 0; q < kQ; q++) out->MI[k][q] = out->M[k][q];
   if (!gauss_jordan_full_pivot<kQ>(out->MI)) return false;
-  const double lat_c = 1.0, dt = 1.0;
+  const double lat_c = dx / dt;
   const double c_s2 = lat_c * lat_c / 3;
   const double tau = nu / (c_s2 * dt) + 0.5;
   const double s_v = 1 / tau;
@@ -88,6 +88,19 @@ bool build_mrt_constants(double nu, MrtConstants* out) {
   out->s_v = s_v;
   out->s_o = s_o;
   return true;
+}
+
+Lattice make_lattice(double dx, double dt) {
+  Lattice l;
+  l.dx = dx;
+  l.dt = dt;
+  l.c = dx / dt;  // SP3:1292-1294
+  l.ic = 1.0 / l.c;
+  l.cs2 = l.c * l.c / 3;
+  l.c2 = l.c * l.c;  // feq (SP3:1387)
+  l.c4 = l.c2 * l.c2;
+  l.on = (l.c != 1.0 || dt != 1.0) ? 1 : 0;
+  return l;
 }
 
 }  // namespace lbm

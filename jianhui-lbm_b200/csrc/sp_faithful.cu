@@ -171,35 +171,46 @@ __host__ __device__ constexpr bool leads_pair(int q) {
   return q != 0 && (cx(q) > 0 || (cx(q) == 0 && (cy(q) > 0 || (cy(q) == 0 && cz(q) > 0))));
 }
 
-// f_eq of feq() (SP3:1382-1391; lat_c = 1 so c2 = c4 = 1):
-// w rho (1 + 3 eu + 4.5 eu eu - 1.5 uv).  For the opposite direction eu is
-// exactly -eu, so 3 eu changes sign and 4.5 eu eu is the same value.
-template <int Q>
-__device__ __forceinline__ void equilibrium_pair(double rho, double ux, double uy, double uz, double t_uv,
-                                                 double (&feq)[kQ]) {
+// f_eq of feq() (SP3:1382-1391): w rho (1 + 3 eu / c2 + 4.5 eu eu / c4 -
+// 1.5 uv / c2) with eu = e lat_c . u.  On the default lattice c2 = c4 = 1 and
+// the divisions are left out (LAT = false); e lat_c . u is e . (lat_c u),
+// each product (+-lat_c) u_a being exactly +-(lat_c u_a).  For the opposite
+// direction eu is exactly -eu, so 3 eu / c2 changes sign and 4.5 eu eu / c4
+// is the same value.
+template <bool LAT, int Q>
+__device__ __forceinline__ void equilibrium_pair(double rho, double cux, double cuy, double cuz, double t_uv,
+                                                 const Lattice& L, double (&feq)[kQ]) {
   if constexpr (leads_pair(Q)) {
-    const double eu = edot<Q>(ux, uy, uz);
-    const double t3 = 3.0 * eu, t45 = 4.5 * eu * eu;
+    const double eu = edot<Q>(cux, cuy, cuz);
+    double t3 = 3.0 * eu, t45 = 4.5 * eu * eu;
+    if constexpr (LAT) {
+      t3 = t3 / L.c2;
+      t45 = t45 / L.c4;
+    }
     const double wr = weight(Q) * rho;
     feq[Q] = wr * (1.0 + t3 + t45 - t_uv);
     feq[opp(Q)] = wr * (1.0 - t3 + t45 - t_uv);
   }
 }
-template <int... Q>
-__device__ __forceinline__ void equilibrium_(double rho, double ux, double uy, double uz, double (&feq)[kQ],
-                                             std::integer_sequence<int, Q...>) {
+template <bool LAT, int... Q>
+__device__ __forceinline__ void equilibrium_(double rho, double ux, double uy, double uz, const Lattice& L,
+                                             double (&feq)[kQ], std::integer_sequence<int, Q...>) {
   const double uv = ux * ux + uy * uy + uz * uz;
-  const double t_uv = 1.5 * uv;
+  double t_uv = 1.5 * uv;
+  if constexpr (LAT) t_uv = t_uv / L.c2;
   feq[0] = weight(0) * rho * (1.0 - t_uv);
-  (equilibrium_pair<Q>(rho, ux, uy, uz, t_uv, feq), ...);
+  const double cux = LAT ? L.c * ux : ux, cuy = LAT ? L.c * uy : uy, cuz = LAT ? L.c * uz : uz;
+  (equilibrium_pair<LAT, Q>(rho, cux, cuy, cuz, t_uv, L, feq), ...);
 }
 
-// Guo forcing GuoF[q] = w_q (lm0 + lm1) (SP3:1432-1510, c_l = lat_c = 1):
-//   lm0 = ((e_x - u_x) g_x + (e_y - u_y) g_y + (e_z - u_z) g_z) / c_s2
-//   lm1 = (e.u)(e.g) / (c_s2 c_s2)
+// Guo forcing GuoF[q] = w_q (lm0 + lm1) (SP3:1432-1510, c_l = lat_c):
+//   lm0 = ((e_x c_l - u_x) g_x + (e_y c_l - u_y) g_y + (e_z c_l - u_z) g_z) / c_s2
+//   lm1 = (e c_l . u)(e c_l . g) / (c_s2 c_s2)
 // (e.u)(e.g) is the same for q and its opposite (both factors change sign),
 // so lm1 is divided once per pair.  GX: g_y = g_z = 0, so lm0 depends on
-// e_x alone (three values) and lm1 vanishes for e_x = 0.
+// e_x alone (three values) and lm1 vanishes for e_x = 0.  The default
+// lattice (c_l = 1) uses the constants below; LAT = true takes c_l, c_s2
+// from the step's lattice (the GX form is not built for it).
 constexpr double kCs2 = 1.0 * 1.0 / 3;
 constexpr double kCs4 = kCs2 * kCs2;
 
@@ -230,10 +241,32 @@ __device__ __forceinline__ void guo_pair_any(double ux, double uy, double uz, do
     guo[o] = weight(Q) * (l0o + l1);
   }
 }
-template <bool GX, int... Q>
+template <int Q>
+__device__ __forceinline__ void guo_pair_lat(double cux, double cuy, double cuz, double cgx, double cgy, double cgz,
+                                             const double (&tx)[3], const double (&ty)[3], const double (&tz)[3],
+                                             double cs2, double cs4, double (&guo)[kQ]) {
+  if constexpr (leads_pair(Q)) {
+    constexpr int o = opp(Q);
+    const double l1 = (edot<Q>(cux, cuy, cuz) * edot<Q>(cgx, cgy, cgz)) / cs4;
+    const double l0q = ((tx[cx(Q) + 1] + ty[cy(Q) + 1]) + tz[cz(Q) + 1]) / cs2;
+    const double l0o = ((tx[cx(o) + 1] + ty[cy(o) + 1]) + tz[cz(o) + 1]) / cs2;
+    guo[Q] = weight(Q) * (l0q + l1);
+    guo[o] = weight(Q) * (l0o + l1);
+  }
+}
+template <bool GX, bool LAT, int... Q>
 __device__ __forceinline__ void guo_force_(double ux, double uy, double uz, double gx, double gy, double gz,
-                                           double (&guo)[kQ], std::integer_sequence<int, Q...>) {
-  if constexpr (GX) {
+                                           const Lattice& L, double (&guo)[kQ], std::integer_sequence<int, Q...>) {
+  if constexpr (LAT) {
+    static_assert(!GX, "the lattice form is built for the general force only");
+    const double c = L.c, cs2 = L.cs2, cs4 = L.cs2 * L.cs2;
+    // (e_a c_l - u_a) g_a for e_a = -1, 0, +1; 0 c_l - u_a is -u_a
+    const double tx[3] = {(-c - ux) * gx, (-ux) * gx, (c - ux) * gx};
+    const double ty[3] = {(-c - uy) * gy, (-uy) * gy, (c - uy) * gy};
+    const double tz[3] = {(-c - uz) * gz, (-uz) * gz, (c - uz) * gz};
+    guo[0] = weight(0) * (((tx[1] + ty[1]) + tz[1]) / cs2);
+    (guo_pair_lat<Q>(c * ux, c * uy, c * uz, c * gx, c * gy, c * gz, tx, ty, tz, cs2, cs4, guo), ...);
+  } else if constexpr (GX) {
     const double l0p = ((1.0 - ux) * gx) / kCs2;
     const double l0z = ((-ux) * gx) / kCs2;
     const double l0m = ((-1.0 - ux) * gx) / kCs2;
@@ -256,11 +289,14 @@ __device__ __forceinline__ void relax_eq(double& m, const double (&feq)[kQ], dou
     m = m - S * (m - moment_row<K>(feq));
   }
 }
-template <int K>
-__device__ __forceinline__ void relax_force(double& m, const double (&guo)[kQ], double sv, double so) {
+template <bool LAT, int K>
+__device__ __forceinline__ void relax_force(double& m, const double (&guo)[kQ], double sv, double so, double dt) {
   double fh = moment_row<K>(guo);
   if constexpr (!conserved_moment(K)) fh *= (1 - 0.5 * srate(K, sv, so));
-  m = m + fh;
+  if constexpr (LAT)
+    m = m + dt * fh;
+  else
+    m = m + fh;  // dt = 1
 }
 
 // Back-transform row Q: f*_Q = MI_Q . m, the non-zero entries in ascending j.
@@ -282,18 +318,18 @@ __device__ __forceinline__ double mi_row(const double (&m)[kQ], std::integer_seq
   return s;
 }
 
-template <bool GX, int... K>
+template <bool GX, bool LAT, int... K>
 __device__ __forceinline__ void collide_moments_(double (&m)[kQ], double rho, double ux, double uy, double uz,
                                                  const StepArgs& a, int p, std::integer_sequence<int, K...>) {
   {
     double feq[kQ];
-    equilibrium_(rho, ux, uy, uz, feq, QSeq{});
+    equilibrium_<LAT>(rho, ux, uy, uz, a.lat, feq, QSeq{});
     (relax_eq<K>(m[K], feq, a.s_v, a.s_o), ...);
   }
   {
     double guo[kQ];
-    guo_force_<GX>(ux, uy, uz, a.gx, a.gy, a.gz, guo, QSeq{});
-    (relax_force<K>(m[K], guo, a.s_v, a.s_o), ...);
+    guo_force_<GX, LAT>(ux, uy, uz, a.gx, a.gy, a.gz, a.lat, guo, QSeq{});
+    (relax_force<LAT, K>(m[K], guo, a.s_v, a.s_o, a.lat.dt), ...);
   }
   double* __restrict__ dst = static_cast<double*>(a.dst_pop) + p;
   const size_t np = (size_t)a.npad;
@@ -303,10 +339,10 @@ __device__ __forceinline__ void collide_moments_(double (&m)[kQ], double rho, do
 // Relaxation in moment space and back-transform for one node whose moments
 // m = M f (accumulated by the caller) and macro values are known; writes the
 // 19 post-collision populations of node p.
-template <bool GX>
+template <bool GX, bool LAT = false>
 __device__ __forceinline__ void collide_moments(double (&m)[kQ], double rho, double ux, double uy, double uz,
                                                 const StepArgs& a, int p) {
-  collide_moments_<GX>(m, rho, ux, uy, uz, a, p, QSeq{});
+  collide_moments_<GX, LAT>(m, rho, ux, uy, uz, a, p, QSeq{});
 }
 
 }  // namespace
@@ -345,17 +381,22 @@ __device__ __forceinline__ void macro_in_out(const StepArgs& a, int p, bool give
 constexpr int f64_min_blocks(int bs) { return bs == 64 ? 12 : 512 / bs; }
 
 // One node per thread.  The macro step of the reference (comput_macro_variables,
-// SP3:2414-2439) is rho = sum f and u = (j + g/2) / rho with the same sums as
-// moment rows 0, 3, 5, 7, so it reads them from the accumulated moments.
-template <int BS, bool GIVEN, bool WRITE, bool GX>
+// SP3:2414-2439) is rho = sum f and u = (j + dt g/2) / rho.  On the default
+// lattice rho and j are the sums of moment rows 0, 3, 5, 7, so it reads them
+// from the accumulated moments; with a self-defined lattice (LAT) j sums the
+// products e_a lat_c f_q, each rounded, in direction order, which the kernel
+// accumulates beside the moments.
+template <int BS, bool GIVEN, bool WRITE, bool GX, bool LAT>
 __global__ void __launch_bounds__(BS, f64_min_blocks(BS)) step_f64_faithful(StepArgs a) {
   const int p = blockIdx.x * BS + threadIdx.x;
   if (p >= a.n_main) return;
   double m[kQ];
+  double jx = 0.0, jy = 0.0, jz = 0.0;
   {
     double f[kQ];
     pull_f64(a, p, f);
     moments_by_column(m, f, QSeq{});
+    if constexpr (LAT && !GIVEN) lattice_momentum(f, a.lat.c, jx, jy, jz);
   }
   double rho, ux, uy, uz;
   if (GIVEN) {
@@ -365,6 +406,11 @@ __global__ void __launch_bounds__(BS, f64_min_blocks(BS)) step_f64_faithful(Step
     ux = u[p];
     uy = u[a.npad + p];
     uz = u[2 * a.npad + p];
+  } else if constexpr (LAT) {
+    rho = m[0];
+    ux = (jx + a.lat.dt * a.gx / 2) / rho;
+    uy = (jy + a.lat.dt * a.gy / 2) / rho;
+    uz = (jz + a.lat.dt * a.gz / 2) / rho;
   } else {
     rho = m[0];
     ux = (m[3] + a.gx / 2) / rho;
@@ -385,7 +431,7 @@ __global__ void __launch_bounds__(BS, f64_min_blocks(BS)) step_f64_faithful(Step
     pull_f64(a, p, f);
     snap_write(a.snap_dst, a.nsnap, p - a.snap_begin, f, rho, ux, uy, uz);
   }
-  collide_moments<GX>(m, rho, ux, uy, uz, a, p);
+  collide_moments<GX, LAT>(m, rho, ux, uy, uz, a, p);
 }
 
 // Face nodes: pull, the boundary rules, macro step, record, collision.  With
@@ -436,28 +482,30 @@ __global__ void reduce_final_kernel(const double* __restrict__ partials, int nbl
   block_reduce8(acc, result, smem);
 }
 
-template <int BS, bool GX>
+template <int BS, bool GX, bool LAT>
 static cudaError_t launch_f64_bs(const StepArgs& a, cudaStream_t st) {
   const int grid = (a.n_main + BS - 1) / BS;
   if (grid == 0) return cudaSuccess;
   const bool given = a.rho_in != nullptr, write = a.rho_out != nullptr;
   if (given && write)
-    step_f64_faithful<BS, true, true, GX><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, true, true, GX, LAT><<<grid, BS, 0, st>>>(a);
   else if (given)
-    step_f64_faithful<BS, true, false, GX><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, true, false, GX, LAT><<<grid, BS, 0, st>>>(a);
   else if (write)
-    step_f64_faithful<BS, false, true, GX><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, false, true, GX, LAT><<<grid, BS, 0, st>>>(a);
   else
-    step_f64_faithful<BS, false, false, GX><<<grid, BS, 0, st>>>(a);
+    step_f64_faithful<BS, false, false, GX, LAT><<<grid, BS, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 template <int BS>
 static cudaError_t launch_f64_force(const StepArgs& a, cudaStream_t st) {
-  // force along x only (every configuration of the benchmarks): the
-  // specialised Guo terms; any other force: the general ones
-  if (a.gy == 0.0 && a.gz == 0.0) return launch_f64_bs<BS, true>(a, st);
-  return launch_f64_bs<BS, false>(a, st);
+  // a self-defined lattice: the general lattice arithmetic; force along x
+  // only (every configuration of the benchmarks): the specialised Guo terms;
+  // any other force: the general ones
+  if (a.lat.on) return launch_f64_bs<BS, false, true>(a, st);
+  if (a.gy == 0.0 && a.gz == 0.0) return launch_f64_bs<BS, true, false>(a, st);
+  return launch_f64_bs<BS, false, false>(a, st);
 }
 
 cudaError_t launch_step_f64(const StepArgs& a, int block, cudaStream_t st) {

@@ -115,23 +115,27 @@ __global__ void __launch_bounds__(BS) step_dev_kernel(StepArgs a) {
   PairSplit<A> ps;
   split_pairs(f, ps);
   A drho, rho, ux, uy, uz;
+  // velocities in units of lat_c (1 on the default lattice, where the
+  // scalings below are exact)
   if (GIVEN) {
     const Mac* r = static_cast<const Mac*>(a.rho_in);
     const Mac* u = static_cast<const Mac*>(a.u_in);
+    const A ic = A(a.lat.ic);
     rho = (A)r[p];
     drho = rho - A(1);
-    ux = (A)u[p];
-    uy = (A)u[a.npad + p];
-    uz = (A)u[2 * a.npad + p];
+    ux = (A)u[p] * ic;
+    uy = (A)u[a.npad + p] * ic;
+    uz = (A)u[2 * a.npad + p] * ic;
   } else {
     macro_dev<A>(f, ps, A(0.5 * a.gx), A(0.5 * a.gy), A(0.5 * a.gz), drho, rho, ux, uy, uz);
   }
   if (WRITE) {
+    const A c = A(a.lat.c);
     static_cast<Mac*>(a.rho_out)[p] = (Mac)rho;
     Mac* u = static_cast<Mac*>(a.u_out);
-    u[p] = (Mac)ux;
-    u[a.npad + p] = (Mac)uy;
-    u[2 * a.npad + p] = (Mac)uz;
+    u[p] = (Mac)(ux * c);
+    u[a.npad + p] = (Mac)(uy * c);
+    u[2 * a.npad + p] = (Mac)(uz * c);
   }
   if (a.snap_dst != nullptr && p >= a.snap_begin) {
     double full[kQ];

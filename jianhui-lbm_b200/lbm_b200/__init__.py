@@ -254,6 +254,7 @@ _SIGNATURES = {
     "lbm_last_step_ms": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
     "lbm_memory": ([C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_double)], C.c_int),
     "lbm_set_table_mode": ([C.c_void_p, C.c_int], C.c_int),
+    "lbm_set_lattice": ([C.c_void_p, C.c_double, C.c_double], C.c_int),
     "lbm_table_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "lbm_reduce_noalloc": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                             C.c_void_p, C.c_void_p], C.c_int),
@@ -1013,6 +1014,12 @@ class SinglePhase:
         v = C.c_double()
         _check(lib().lbm_last_step_ms(self._h, C.byref(v)))
         return v.value
+
+    def set_lattice(self, dx, dt):
+        """Self-defined lattice velocity (lattice_v, dx, dt): lat_c = dx/dt,
+        tau = nu / (c_s^2 dt) + 1/2 with c_s^2 = lat_c^2 / 3.  Before the
+        first step; the state restarts from the initial equilibrium."""
+        _check(lib().lbm_set_lattice(self._h, float(dx), float(dt)))
 
     def set_table_mode(self, compact):
         """1: compact pull table (default), 0: the int32 table; identical results."""

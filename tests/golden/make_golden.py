@@ -10,6 +10,7 @@ random generator at test time):
   sp_outputs.npz  the reference program itself (oracle/_ref/ref_sp3_main)
                 run on an INPUT.dat: every file it writes  (--outputs)
   sp_outputs_bc.npz  the same with pressure faces on x (Sub_BC 2, in_BC 1)  (--outputs)
+  sp_outputs_lat*.npz  the same with a self-defined lattice velocity  (--outputs)
   cg_small.npz  colour-gradient reference, see cg_small()  (--cg)
   cg_outputs*.npz  the colour-gradient program (oracle/_ref/ref_cg3_main) on
                 INPUT_cg.dat variants: every file it writes, and a restart from
@@ -177,7 +178,7 @@ def collect(workdir, prefix="out_"):
     return out
 
 
-def program_outputs():
+def program_outputs(only=None):
     """The reference program run end to end on 14x12x10 spheres: 251 steps
     (n_max=250) writing every output family (reports every 50 steps, VTK
     every 100, checkpoints every 100 and at the end, solute velocity at 200).
@@ -189,14 +190,22 @@ def program_outputs():
     so a restarted run has dt = dx = inf and stops at its first report with
     NaN."""
     mask = G.overlapping_spheres((14, 12, 10), 0.6, 2.5, seed=21)
-    in_a = input_text(L1="mask.dat", L2="14 12 10", L3=250, L17=1, L18=50, L20=100, L21=100, L32=100, L34=200)
-    save_program_outputs("sp_outputs.npz", mask, in_a)
+    base = dict(L1="mask.dat", L2="14 12 10", L3=250, L17=1, L18=50, L20=100, L21=100, L32=100, L34=200)
+    runs = [("sp_outputs.npz", input_text(**base))]
     # pressure faces on x (Sub_BC 2, in_BC 1: the permeability includes the
     # pressure gradient), no body force: reports every 50 steps, velocity VTK
     # at 150
-    in_b = input_text(L1="mask.dat", L2="14 12 10", L3=150, L4=7.5, L5=1, L6="0 0 0", L7="1 1.0 1 1.005", L17=1,
-                      L18=50, L20=150, L21=-1, L25=2, L32=-1, L34=-1)
-    save_program_outputs("sp_outputs_bc.npz", mask, in_b)
+    runs.append(("sp_outputs_bc.npz",
+                 input_text(L1="mask.dat", L2="14 12 10", L3=150, L4=7.5, L5=1, L6="0 0 0", L7="1 1.0 1 1.005",
+                            L17=1, L18=50, L20=150, L21=-1, L25=2, L32=-1, L34=-1)))
+    # self-defined lattice velocity: dx = 1, dt = 2 (lat_c = 1/2, tau = 1.5)
+    # and dx = 1, dt = 1/2 (lat_c = 2, tau = 0.75), with the template's
+    # initial velocity and three-component force
+    runs.append(("sp_outputs_lat.npz", input_text(**base, L23="1 1.0 2.0")))
+    runs.append(("sp_outputs_lat2.npz", input_text(**base, L23="1 1.0 0.5")))
+    for fname, text in runs:
+        if only is None or only in fname:
+            save_program_outputs(fname, mask, text)
 
 
 def save_program_outputs(fname, mask, input_txt):
@@ -696,7 +705,7 @@ def main():
     ap.add_argument("--outputs", action="store_true")
     ap.add_argument("--cg-outputs", action="store_true")
     ap.add_argument("--only", default=None,
-                    help="--cg-outputs / --st7-outputs / --st19: runs whose fixture name contains this")
+                    help="--outputs / --cg-outputs / --st7-outputs / --st19: runs whose fixture name contains this")
     ap.add_argument("--st7-outputs", action="store_true")
     ap.add_argument("--st19", action="store_true", help="D3Q19 solute program fixtures")
     a = ap.parse_args()
@@ -716,7 +725,7 @@ def main():
         cg_small()
         return
     if a.outputs:
-        program_outputs()
+        program_outputs(a.only)
         return
     if a.bc:
         bc_fixture()

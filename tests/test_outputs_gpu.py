@@ -3,7 +3,9 @@
 tests/golden/sp_outputs.npz holds every file the reference program wrote for
 one INPUT.dat (14x12x10 spheres, n_max=250, reports every 50 steps, VTK every
 100, checkpoints every 100 and at the end, solute velocity at 200);
-sp_outputs_bc.npz the same for pressure faces on x (Sub_BC 2, in_BC 1).  The
+sp_outputs_bc.npz the same for pressure faces on x (Sub_BC 2, in_BC 1);
+sp_outputs_lat.npz and sp_outputs_lat2.npz the same with a self-defined
+lattice velocity (dx, dt = 1, 2 and 1, 1/2: lat_c = 1/2 and 2).  The
 driver, run on the same INPUT.dat and mask at FP64, must write the same files:
 text and VTK byte for byte (except the wall-clock lines of Results.txt), the
 checkpoints and the solute velocity bit for bit (rows 1..; row 0 of the
@@ -89,7 +91,8 @@ def rows_digest(path, width):
     return hashlib.sha256(np.ascontiguousarray(a[1:]).tobytes()).hexdigest()
 
 
-@pytest.mark.parametrize("fixture", ["sp_outputs.npz", "sp_outputs_bc.npz"])
+@pytest.mark.parametrize("fixture", ["sp_outputs.npz", "sp_outputs_bc.npz", "sp_outputs_lat.npz",
+                                     "sp_outputs_lat2.npz"])
 def test_driver_writes_the_reference_files(L, fixture, tmp_path):
     golden = np.load(os.path.join(GOLDEN, fixture))
     prepare(tmp_path, golden)
@@ -139,3 +142,45 @@ def test_driver_f32_reports_match(L, golden, tmp_path):
     perm_w = np.loadtxt(golden["Permeability_error_local_Perm.txt"].tobytes().decode().splitlines())
     perm_g = np.loadtxt((tmp_path / "out_Permeability_error_local_Perm.txt").read_text().splitlines())
     assert np.allclose(perm_g[:, 0], perm_w[:, 0], rtol=1e-4, atol=0)
+
+
+@pytest.mark.parametrize("fixture", ["sp_outputs_lat.npz", "sp_outputs_lat2.npz"])
+@pytest.mark.parametrize("precision,rtol", [("f64fast", 2e-5), ("f32", 1e-4)])
+def test_driver_lattice_reports_match(L, fixture, precision, rtol, tmp_path):
+    """The deviation-storage kernels step a self-defined lattice in units of
+    lat_c (force dt g / lat_c, velocities scaled by lat_c on the way in and
+    out): the six-digit reports of FP64 in that form match the reference's
+    to the last digit, FP32's to its storage precision."""
+    golden = np.load(os.path.join(GOLDEN, fixture))
+    prepare(tmp_path, golden)
+    run_driver(L, tmp_path, "./", "--precision", precision)
+    want = np.loadtxt(golden["Velocity_ave_max.txt"].tobytes().decode().splitlines())
+    got = np.loadtxt((tmp_path / "out_Velocity_ave_max.txt").read_text().splitlines())
+    assert got.shape == want.shape
+    assert np.allclose(got[:, :2], want[:, :2], rtol=rtol, atol=0)
+    perm_w = np.loadtxt(golden["Permeability_error_local_Perm.txt"].tobytes().decode().splitlines())
+    perm_g = np.loadtxt((tmp_path / "out_Permeability_error_local_Perm.txt").read_text().splitlines())
+    assert np.allclose(perm_g[:, 0], perm_w[:, 0], rtol=rtol, atol=0)
+
+
+def test_lattice_with_faces_is_refused(L, tmp_path):
+    golden = np.load(os.path.join(GOLDEN, "sp_outputs_bc.npz"))
+    text = set_lines(golden["input"].tobytes().decode(), L23="1 1.0 2.0")
+    prepare(tmp_path, golden, text)
+    r = subprocess.run([L.driver_path(), "INPUT.dat"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode != 0
+    assert "lattice" in (r.stdout + r.stderr)
+
+
+def test_set_lattice_only_before_the_first_step(L):
+    from helpers import spheres
+
+    m = spheres((16, 14, 12), 0.5, 3.0, seed=2)
+    with L.SinglePhase(m, 1 / 6, (1e-5, 0.0, 0.0), precision="f64") as s:
+        s.set_lattice(1.0, 2.0)
+        s.step(3)
+        with pytest.raises(L.LbmError):
+            s.set_lattice(1.0, 1.0)
+    with L.SinglePhase(m, 1 / 6, (1e-5, 0.0, 0.0), precision="f32") as s:
+        with pytest.raises(L.LbmError):
+            s.set_lattice(0.0, 1.0)
