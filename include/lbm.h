@@ -191,8 +191,7 @@ LBM_API lbm_status lbm_create(const lbm_params* p, const uint8_t* mask, int nx, 
 /* Reads INPUT.dat and its geometry file and creates the solver (main SP3:258-555
  * at one rank), pressure/velocity faces (pre_*, vel_*, Sub_BC) included, and
  * a self-defined lattice velocity (lattice_v = 1 with dx, dt: lbm_set_lattice).
- * The non-Newtonian module, and a self-defined lattice velocity together with
- * pressure/velocity faces, return LBM_ERR_ARG. */
+ * The non-Newtonian module returns LBM_ERR_ARG. */
 LBM_API lbm_status lbm_create_from_input(const char* input_path, int precision, int ordering,
                                  lbm_handle** out, lbm_input* parsed_out);
 
@@ -200,13 +199,14 @@ LBM_API lbm_status lbm_create_from_input(const char* input_path, int precision, 
  * 1326-1330): lat_c = dx/dt, c_s^2 = lat_c^2 / 3, tau = nu / (c_s^2 dt) + 1/2;
  * the discrete velocities are e lat_c in the equilibrium (divided by
  * c2 = lat_c^2 and c4 = c2^2), the Guo force and the macro step, the force
- * enters the moments as dt F and the velocity as dt g / 2, and the pressure
- * term of the permeability uses c_s^2 and dx.  Velocities in and out (fields,
- * reductions, checkpoints) are the velocity itself.  LBM_PREC_F64 reproduces
- * the reference's arithmetic bit for bit; the other precisions step in units
- * of lat_c.  Call after lbm_create and before the first step: the state
- * restarts from the initial equilibrium on the new lattice.  The default
- * lattice is dx = dt = 1.  Pressure/velocity faces: LBM_ERR_ARG. */
+ * enters the moments as dt F and the velocity as dt g / 2, the face rules'
+ * equilibria use the same feq, and the pressure term of the permeability uses
+ * c_s^2 and dx.  Velocities in and out (fields, reductions, checkpoints, face
+ * velocities) are the velocity itself.  LBM_PREC_F64 reproduces the
+ * reference's arithmetic bit for bit; the other precisions step in units of
+ * lat_c.  Call after lbm_create and before the first step: the state restarts
+ * from the initial equilibrium on the new lattice.  The default lattice is
+ * dx = dt = 1. */
 LBM_API lbm_status lbm_set_lattice(lbm_handle* h, double dx, double dt);
 
 LBM_API void lbm_destroy(lbm_handle* h);

@@ -364,10 +364,12 @@ BcArgs bc_args(lbm_handle* h, const StepArgs& s, int c) {
   b.ops = h->bc_ops.as<BcOp>();
   b.mi = h->bc_mi.as<double>();
   const lbm_boundary& bc = h->prm.bc;
+  // face velocities in units of lat_c for the deviation-storage kernels
+  const bool scale = h->lat.on && h->kind != Store::F64;
   for (int f = 0; f < 6; f++) {
     b.face_rho[f] = bc.rho[f];
     b.face_u[f][0] = b.face_u[f][1] = b.face_u[f][2] = 0.0;
-    b.face_u[f][f / 2] = bc.vel[f];
+    b.face_u[f][f / 2] = scale ? bc.vel[f] * h->lat.ic : bc.vel[f];
   }
   b.bnd_f = nullptr;
   return b;
@@ -750,8 +752,6 @@ lbm_status lbm_set_lattice(lbm_handle* h, double dx, double dt) {
   lbm_status st = check_handle(h);
   if (st != LBM_OK) return st;
   if (!(dx > 0) || !(dt > 0) || !std::isfinite(dx / dt)) return fail(LBM_ERR_ARG, "lbm_set_lattice: dx and dt must be positive");
-  if (h->bc.active)
-    return fail(LBM_ERR_ARG, "lbm_set_lattice: a self-defined lattice velocity with pressure/velocity faces is not supported");
   if (h->step != 0 || !h->given_macro) return fail(LBM_ERR_STATE, "lbm_set_lattice: call before the first step");
   MrtConstants m;
   if (!build_mrt_constants(h->prm.nu, &m, dx, dt)) return fail(LBM_ERR_ARG, "moment matrix inversion failed");

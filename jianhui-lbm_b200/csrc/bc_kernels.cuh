@@ -14,11 +14,19 @@
 
 namespace lbm {
 
-// `feq` (SP3:1382-1394) with lat_c = 1, in the reference's operation order.
-__device__ __forceinline__ double bc_feq(int q, double rho, double ux, double uy, double uz) {
+// `feq` (SP3:1382-1394) in the reference's operation order: on the default
+// lattice lat_c = c2 = c4 = 1, on a self-defined one (L.on) elat = e lat_c and
+// the divisions by c2, c4.  The deviation-storage kernels pass the default
+// lattice: their velocities are in units of lat_c, where the two agree.
+__device__ __forceinline__ double bc_feq(int q, double rho, double ux, double uy, double uz, const Lattice& L) {
+  const double uv = ux * ux + uy * uy + uz * uz;
+  if (L.on) {
+    const double ex = (double)cx(q) * L.c, ey = (double)cy(q) * L.c, ez = (double)cz(q) * L.c;
+    const double eu = ex * ux + ey * uy + ez * uz;
+    return weight(q) * rho * (1.0 + 3.0 * eu / L.c2 + 4.5 * eu * eu / L.c4 - 1.5 * uv / L.c2);
+  }
   const double c2 = 1.0, c4 = 1.0;
   const double eu = (double)cx(q) * ux + (double)cy(q) * uy + (double)cz(q) * uz;
-  const double uv = ux * ux + uy * uy + uz * uz;
   return weight(q) * rho * (1.0 + 3.0 * eu / c2 + 4.5 * eu * eu / c4 - 1.5 * uv / c2);
 }
 
@@ -34,8 +42,8 @@ __device__ __forceinline__ void snap_write(double* snap, int nsnap, int slot, co
 }
 
 // The rules of face node b (index b = p - n_main) applied in program order to
-// its post-streaming populations F.
-__device__ __forceinline__ void bc_apply(const BcArgs& a, int b, double (&F)[kQ]) {
+// its post-streaming populations F, with the equilibria of lattice L.
+__device__ __forceinline__ void bc_apply(const BcArgs& a, int b, double (&F)[kQ], const Lattice& L) {
   const double* __restrict__ S = a.snap_src;
   const size_t ns = (size_t)a.s.nsnap;
   const int o1 = a.op_off[b + 1];
@@ -47,12 +55,12 @@ __device__ __forceinline__ void bc_apply(const BcArgs& a, int b, double (&F)[kQ]
     switch (op.kind) {
       case kBcPressureRest:
 #pragma unroll
-        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, rb, 0.0, 0.0, 0.0);
+        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, rb, 0.0, 0.0, 0.0, L);
         break;
       case kBcPressureNbU: {
         const double ux = S[(kQ + 1) * ns + nb], uy = S[(kQ + 2) * ns + nb], uz = S[(kQ + 3) * ns + nb];
 #pragma unroll
-        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, rb, ux, uy, uz);
+        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, rb, ux, uy, uz, L);
         break;
       }
       case kBcPressureMoment: {
@@ -82,26 +90,26 @@ __device__ __forceinline__ void bc_apply(const BcArgs& a, int b, double (&F)[kQ]
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
           const double f4 = op.nb4 >= 0 ? S[q * ns + (size_t)op.nb4] : 0.0;
-          F[q] = bc_feq(q, rb, ux, uy, uz) + f4 - bc_feq(q, rn, ux, uy, uz);
+          F[q] = bc_feq(q, rb, ux, uy, uz, L) + f4 - bc_feq(q, rn, ux, uy, uz, L);
         }
         break;
       }
       case kBcVelocityEq:
 #pragma unroll
-        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, 1.0, ubx, uby, ubz);
+        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, 1.0, ubx, uby, ubz, L);
         break;
       case kBcVelocityNeq:
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
           const int e = op.axis == 0 ? cx(q) : (op.axis == 1 ? cy(q) : cz(q));
           if (op.sign > 0 ? e < 0 : e > 0)
-            F[q] = bc_feq(opp(q), 1.0, ubx, uby, ubz) - F[opp(q)] + bc_feq(q, 1.0, ubx, uby, ubz);
+            F[q] = bc_feq(opp(q), 1.0, ubx, uby, ubz, L) - F[opp(q)] + bc_feq(q, 1.0, ubx, uby, ubz, L);
         }
         break;
       case kBcVelocityNbRho: {
         const double rn = S[kQ * ns + nb];
 #pragma unroll
-        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, rn, ubx, uby, ubz);
+        for (int q = 0; q < kQ; q++) F[q] = bc_feq(q, rn, ubx, uby, ubz, L);
         break;
       }
       default:

@@ -363,6 +363,8 @@ __device__ __forceinline__ void macro_in_out(const StepArgs& a, int p, bool give
     ux = u[p];
     uy = u[a.npad + p];
     uz = u[2 * a.npad + p];
+  } else if (a.lat.on) {
+    macro_faithful_lat(f, a.lat.c, a.lat.dt * a.gx / 2, a.lat.dt * a.gy / 2, a.lat.dt * a.gz / 2, rho, ux, uy, uz);
   } else {
     macro_faithful(f, a.gx / 2, a.gy / 2, a.gz / 2, rho, ux, uy, uz);
   }
@@ -435,15 +437,17 @@ __global__ void __launch_bounds__(BS, f64_min_blocks(BS)) step_f64_faithful(Step
 }
 
 // Face nodes: pull, the boundary rules, macro step, record, collision.  With
-// a.bnd_f set: only the populations after the rules (current state).
-template <bool GIVEN, bool FINAL>
+// a.bnd_f set: only the populations after the rules (current state).  LAT:
+// a self-defined lattice (the rules' equilibria, the macro step and the
+// collision on it).
+template <bool GIVEN, bool FINAL, bool LAT>
 __global__ void __launch_bounds__(128) bc_f64_faithful(BcArgs a) {
   const int b = blockIdx.x * 128 + threadIdx.x;
   const int p = a.s.n_main + b;
   if (p >= a.s.n) return;
   double f[kQ];
   pull_f64(a.s, p, f);
-  if (!GIVEN) bc_apply(a, b, f);
+  if (!GIVEN) bc_apply(a, b, f, a.s.lat);
   if (FINAL) {
     const size_t nb = (size_t)(a.s.n - a.s.n_main);
 #pragma unroll
@@ -455,20 +459,27 @@ __global__ void __launch_bounds__(128) bc_f64_faithful(BcArgs a) {
   snap_write(a.s.snap_dst, a.s.nsnap, p - a.s.snap_begin, f, rho, ux, uy, uz);
   double m[kQ];
   moments_by_column(m, f, QSeq{});
-  collide_moments<false>(m, rho, ux, uy, uz, a.s, p);
+  collide_moments<false, LAT>(m, rho, ux, uy, uz, a.s, p);
+}
+
+template <bool LAT>
+static void launch_bc_f64(const BcArgs& a, int grid, cudaStream_t st) {
+  if (a.bnd_f)
+    bc_f64_faithful<false, true, LAT><<<grid, 128, 0, st>>>(a);
+  else if (a.s.rho_in != nullptr)
+    bc_f64_faithful<true, false, LAT><<<grid, 128, 0, st>>>(a);
+  else
+    bc_f64_faithful<false, false, LAT><<<grid, 128, 0, st>>>(a);
 }
 
 cudaError_t launch_boundary_f64(const BcArgs& a, cudaStream_t st) {
   const int nb = a.s.n - a.s.n_main;
   if (nb <= 0) return cudaSuccess;
   const int grid = (nb + 127) / 128;
-  const bool given = a.s.rho_in != nullptr;
-  if (a.bnd_f)
-    bc_f64_faithful<false, true><<<grid, 128, 0, st>>>(a);
-  else if (given)
-    bc_f64_faithful<true, false><<<grid, 128, 0, st>>>(a);
+  if (a.s.lat.on)
+    launch_bc_f64<true>(a, grid, st);
   else
-    bc_f64_faithful<false, false><<<grid, 128, 0, st>>>(a);
+    launch_bc_f64<false>(a, grid, st);
   return cudaGetLastError();
 }
 

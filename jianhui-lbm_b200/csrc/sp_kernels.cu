@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(128) bc_dev_kernel(BcArgs a) {
 #pragma unroll
   for (int q = 1; q < kQ; q++)
     F[q] = to_full<K>(load_pop<K>(src + __ldg(s.table + (size_t)(q - 1) * s.npad + p), inv_scale), q);
-  if (!GIVEN) bc_apply(a, b, F);
+  // the rules on the default lattice: velocities here are in units of lat_c
+  if (!GIVEN) bc_apply(a, b, F, Lattice{});
   if (FINAL) {
     const size_t nb = (size_t)(s.n - s.n_main);
 #pragma unroll
@@ -183,20 +184,22 @@ __global__ void __launch_bounds__(128) bc_dev_kernel(BcArgs a) {
   if (GIVEN) {
     const Mac* r = static_cast<const Mac*>(s.rho_in);
     const Mac* u = static_cast<const Mac*>(s.u_in);
+    const A ic = A(s.lat.ic);
     rho = (A)r[p];
     drho = rho - A(1);
-    ux = (A)u[p];
-    uy = (A)u[s.npad + p];
-    uz = (A)u[2 * s.npad + p];
+    ux = (A)u[p] * ic;
+    uy = (A)u[s.npad + p] * ic;
+    uz = (A)u[2 * s.npad + p] * ic;
   } else {
     macro_dev<A>(f, ps, A(0.5 * s.gx), A(0.5 * s.gy), A(0.5 * s.gz), drho, rho, ux, uy, uz);
   }
   if (s.rho_out != nullptr) {
+    const A c = A(s.lat.c);
     static_cast<Mac*>(s.rho_out)[p] = (Mac)rho;
     Mac* u = static_cast<Mac*>(s.u_out);
-    u[p] = (Mac)ux;
-    u[s.npad + p] = (Mac)uy;
-    u[2 * s.npad + p] = (Mac)uz;
+    u[p] = (Mac)(ux * c);
+    u[s.npad + p] = (Mac)(uy * c);
+    u[2 * s.npad + p] = (Mac)(uz * c);
   }
   snap_write(s.snap_dst, s.nsnap, p - s.snap_begin, F, rho, ux, uy, uz);
   mrt_collide_dev<A>(f, ps, drho, rho, ux, uy, uz, A(s.gx), A(s.gy), A(s.gz), A(s.s_v), A(s.s_o));

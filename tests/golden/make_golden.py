@@ -195,14 +195,21 @@ def program_outputs(only=None):
     # pressure faces on x (Sub_BC 2, in_BC 1: the permeability includes the
     # pressure gradient), no body force: reports every 50 steps, velocity VTK
     # at 150
-    runs.append(("sp_outputs_bc.npz",
-                 input_text(L1="mask.dat", L2="14 12 10", L3=150, L4=7.5, L5=1, L6="0 0 0", L7="1 1.0 1 1.005",
-                            L17=1, L18=50, L20=150, L21=-1, L25=2, L32=-1, L34=-1)))
+    bc = dict(L1="mask.dat", L2="14 12 10", L3=150, L4=7.5, L5=1, L6="0 0 0", L7="1 1.0 1 1.005", L17=1, L18=50,
+              L20=150, L21=-1, L25=2, L32=-1, L34=-1)
+    runs.append(("sp_outputs_bc.npz", input_text(**bc)))
     # self-defined lattice velocity: dx = 1, dt = 2 (lat_c = 1/2, tau = 1.5)
     # and dx = 1, dt = 1/2 (lat_c = 2, tau = 0.75), with the template's
     # initial velocity and three-component force
     runs.append(("sp_outputs_lat.npz", input_text(**base, L23="1 1.0 2.0")))
     runs.append(("sp_outputs_lat2.npz", input_text(**base, L23="1 1.0 0.5")))
+    # the same lattices with faces: the pressure faces above at lat_c = 1/2,
+    # and a velocity inlet on x- (0.0005) with a pressure outlet on x+
+    # (Sub_BC 1; the unused p_xn = 1.002 still enters Comput_Perm's pressure
+    # term, SP3:3543-3556) at lat_c = 2, dt = 1/2
+    runs.append(("sp_outputs_bc_lat.npz", input_text(**bc, L23="1 1.0 2.0")))
+    vel = dict(bc, L7="1 1.0 0 1.002", L10="0 0.0 1 0.0005", L25=1, L23="1 1.0 0.5")
+    runs.append(("sp_outputs_vel_lat.npz", input_text(**vel)))
     for fname, text in runs:
         if only is None or only in fname:
             save_program_outputs(fname, mask, text)
