@@ -529,9 +529,13 @@ LBM_API lbm_status lbm_read_phase(const char* path, int nx, int ny, int nz, doub
  * phase (ini_Sat >= 0, with the window buffer ini_buf).  The reference draws
  * its random numbers from the C library seeded with the clock (CG3:2232,
  * 3321); here they come from the seeded generator of lbm_cg_set_random with
- * seed 0 (lbm_cg_create_from_input_seeded takes the seed).  A self-defined
- * lattice velocity, a non-zero initial velocity, drainage / imbibition
- * control and dynamic input are rejected with LBM_ERR_ARG naming the field. */
+ * seed 0 (lbm_cg_create_from_input_seeded takes the seed).  A non-zero
+ * initial velocity is applied (lbm_cg_set_initial_velocity); the imbibition /
+ * drainage control turns the phase faces on as the reference's init does,
+ * the control itself and the re-reads of input_dynamic are the caller's
+ * (lbm_cg runs both).  A self-defined lattice velocity, and settings the
+ * reference would divide by zero on (update_fre, freRe, frePsi = 0), are
+ * rejected with LBM_ERR_ARG naming the field. */
 LBM_API lbm_status lbm_cg_create_from_input(const char* input_path, int precision, lbm_cg_handle** out,
                                             lbm_cg_input* parsed_out);
 /* lbm_cg_create_from_input with the seed of the random initial phase and
