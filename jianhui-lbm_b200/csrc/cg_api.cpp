@@ -60,6 +60,11 @@ struct lbm_cg_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // with pressure/velocity faces: the face and record passes of a step run
+  // on `side`, beside the colour pass (ev_fork: the step's start on the main
+  // stream, ev_faces: rules applied, ev_rec: record written)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_faces = nullptr, ev_rec = nullptr;
   std::vector<uint8_t> mask;
   Geometry geo;
   double MI[kQ][kQ];
@@ -107,6 +112,9 @@ struct lbm_cg_handle {
       if (g) cudaGraphExecDestroy(g);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : {ev_fork, ev_faces, ev_rec})
+      if (e) cudaEventDestroy(e);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
   size_t s() const { return f64 ? 8 : 4; }
@@ -173,17 +181,19 @@ CgBcArgs bc_args(lbm_cg_handle* h, int c) {
 }
 
 // The rules of the step that produced state c (pending), then the record of
-// state c that this step's rules will read when they are on.
+// state c that this step's rules will read when they are on.  On the side
+// stream: ev_faces marks the rules applied, ev_rec the record written.
 cudaError_t face_passes(lbm_cg_handle* h, int c, int given, bool pending) {
-  if (h->bc_nface == 0) return cudaSuccess;
   CgBcArgs b = bc_args(h, c);
   cudaError_t e = cudaSuccess;
-  if (pending) e = cg_bc_faces(h->f64, b, h->stream);
+  if (pending) e = cg_bc_faces(h->f64, b, h->side);
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev_faces, h->side);
   if (e == cudaSuccess && h->cp.faces) {
     b.given = given == 1;
     for (int d = 0; d < 3; d++) b.u0[d] = h->cp.u0[d];
-    e = cg_bc_record(h->f64, b, h->stream);
+    e = cg_bc_record(h->f64, b, h->side);
   }
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev_rec, h->side);
   return e;
 }
 
@@ -194,12 +204,27 @@ cudaError_t resolve_faces(lbm_cg_handle* h) {
   return cg_bc_faces(h->f64, bc_args(h, h->cur), h->stream);
 }
 
+// One step.  With faces the step forks: the face pass (it writes only face
+// nodes' slots of state c) and the record pass (it reads state c) run on the
+// side stream while the colour pass (it reads the colour record and writes
+// psi, rho_r, rho_b) runs on the main stream; the collide pass waits for the
+// rules, and the step ends when the record is written too, so that the next
+// step (or any other reader or writer of the state) starts after both.
 cudaError_t one_cg_step(lbm_cg_handle* h, int c, int given, bool write_u, bool pending, bool colour_done = false) {
   const CgArgs a = cg_args(h, c, given, write_u);
-  cudaError_t e = face_passes(h, c, given, pending);
+  cudaError_t e = cudaSuccess;
+  const bool faces = h->bc_nface > 0;
+  if (faces) {
+    e = cudaEventRecord(h->ev_fork, h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+    if (e == cudaSuccess) e = face_passes(h, c, given, pending);
+  }
   if (e == cudaSuccess && !given && !colour_done) e = colour_pass(h, a);
+  if (e == cudaSuccess && faces) e = cudaStreamWaitEvent(h->stream, h->ev_faces, 0);
   if (e != cudaSuccess) return e;
-  return h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
+  e = h->f64 ? cg_collide_f64(a, h->stream) : cg_collide_f32(a, h->stream);
+  if (e == cudaSuccess && faces) e = cudaStreamWaitEvent(h->stream, h->ev_rec, 0);
+  return e;
 }
 
 bool same_params(const CgParams& a, const CgParams& b) {
@@ -464,6 +489,9 @@ lbm_status lbm_cg_create_bc(const lbm_cg_params* p, const lbm_boundary* bc, cons
   if (!bl.nodes.empty()) {
     h->bc_nface = (int)bl.nodes.size();
     h->bc_nsnap = (int)bl.snap_nodes.size();
+    LBM_CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    for (cudaEvent_t* ev : {&h->ev_fork, &h->ev_faces, &h->ev_rec})
+      LBM_CUDA_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
     LBM_CUDA_TRY(h->bc_nodes.alloc(bl.nodes.size() * sizeof(int32_t)));
     LBM_CUDA_TRY(h->bc_off.alloc(bl.op_off.size() * sizeof(int32_t)));
     LBM_CUDA_TRY(h->bc_ops.alloc(bl.ops.size() * sizeof(BcOp)));
