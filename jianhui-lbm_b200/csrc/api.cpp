@@ -121,6 +121,10 @@ struct lbm_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // with pressure/velocity faces the face kernel of a step runs on `side`
+  // beside the step kernel (ev_fork: the step's start, ev_bc: faces done)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_bc = nullptr;
   DevBuf pop[2], table, ref_of, window, rho_given, u_given, rho_prev, u_prev, partials, result;
   // pressure/velocity faces: plan, per-step records (ping-pong like pop),
   // operations, M^-1 for the moment rule, post-rule populations of the state
@@ -161,6 +165,9 @@ struct lbm_handle {
       if (g) cudaGraphExecDestroy(g);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_bc) cudaEventDestroy(ev_bc);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
   size_t mac_bytes() const { return (kind == Store::F64 || kind == Store::F64D) ? 8 : 4; }
@@ -248,6 +255,11 @@ void ensure_host_geometry(lbm_handle* h) {
 lbm_status upload_bc(lbm_handle* h) {
   const BcPlan& b = h->bc;
   if (!b.active) return LBM_OK;
+  if (!h->side) {
+    LBM_CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    LBM_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    LBM_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_bc, cudaEventDisableTiming));
+  }
   const int n = h->geo.count;
   const size_t nsnap = (size_t)std::max(n - b.snap_begin, 1), nbnd = (size_t)std::max(n - b.n_main, 1);
   for (auto& sb : h->snap) {
@@ -375,11 +387,20 @@ BcArgs bc_args(lbm_handle* h, const StepArgs& s, int c) {
   return b;
 }
 
-// One step: the step kernel over [0, n_main) and, with faces, the face kernel.
+// One step: the step kernel over [0, n_main) and, with faces, the face kernel
+// over [n_main, n).  The two write disjoint nodes of the new state and of the
+// record (the step kernel the nodes below n_main, the face kernel the rest)
+// and read only the previous step's, so the face kernel runs on the side
+// stream beside the step kernel and the step ends when both have.
 cudaError_t launch_full_step(lbm_handle* h, const StepArgs& a, int c) {
-  cudaError_t e = launch_step(h->kind, a, h->block, h->stream);
-  if (e != cudaSuccess || !h->bc.active) return e;
-  return launch_boundary(h->kind, bc_args(h, a, c), h->stream);
+  if (!h->bc.active) return launch_step(h->kind, a, h->block, h->stream);
+  cudaError_t e = cudaEventRecord(h->ev_fork, h->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+  if (e == cudaSuccess) e = launch_boundary(h->kind, bc_args(h, a, c), h->side);
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev_bc, h->side);
+  if (e == cudaSuccess) e = launch_step(h->kind, a, h->block, h->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, h->ev_bc, 0);
+  return e;
 }
 
 // Face nodes of the current state after their rules, for reductions and
