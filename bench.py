@@ -315,6 +315,9 @@ def run_ours(a):
     t_timed1 = time.time()
     ms = s.last_step_ms()
     diag = s.reduce()
+    # untimed: the field read path's kernels load once per process (lazy
+    # module loading), before the end-to-end leg rather than inside it
+    s.fields()
     s.close()
     ms_max = allmax(pg, ms)
     ms_step = ms_max / a.steps

@@ -290,6 +290,14 @@ LBM_API lbm_status lbm_last_step_ms(lbm_handle* h, double* ms);
  * bytes of lbm_table_info). */
 LBM_API lbm_status lbm_memory(lbm_handle* h, size_t* device_bytes, double* bytes_per_lu);
 
+/* Device memory of every solver (single-phase, colour-gradient, solute, node
+ * pool) comes from the device's default CUDA memory pool, and what a
+ * destroyed solver frees stays mapped in the process for the next solver
+ * (creating one then costs no new mappings).  This returns that cached memory
+ * to the driver, for every device the library allocated on; it waits for
+ * those devices to be idle. */
+LBM_API lbm_status lbm_release_cached_memory(void);
+
 /* Form of the pull table the step kernel reads (the reference's nei_loc,
  * SP3:1099-1151, as a pull table).  compact = 0 (default): the int32 table.
  * compact = 1: per aligned group of 32 nodes and direction one int32 base

@@ -47,13 +47,13 @@ struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
   }
   cudaError_t alloc(size_t b) {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
     p = nullptr;
     bytes = b;
-    return b ? cudaMalloc(&p, b) : cudaSuccess;
+    return b ? lbm::dev_alloc(&p, b) : cudaSuccess;
   }
   template <typename T>
   T* as() const {
@@ -933,6 +933,11 @@ lbm_status lbm_export_table(lbm_handle* h, int32_t* nei_loc) {
 lbm_status lbm_last_step_ms(lbm_handle* h, double* ms) {
   if (!h || !ms) return fail(LBM_ERR_ARG, "null argument");
   *ms = h->last_ms;
+  return LBM_OK;
+}
+
+lbm_status lbm_release_cached_memory(void) {
+  LBM_CUDA_TRY(dev_pool_trim());
   return LBM_OK;
 }
 

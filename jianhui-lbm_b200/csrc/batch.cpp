@@ -28,14 +28,14 @@ struct Buf {
   size_t bytes = 0;
   ~Buf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
     p = nullptr;
     bytes = 0;
   }
   cudaError_t alloc(size_t b) {
     release();
     bytes = b;
-    return b ? cudaMalloc(&p, b) : cudaSuccess;
+    return b ? lbm::dev_alloc(&p, b) : cudaSuccess;
   }
   template <typename T>
   T* as() const {

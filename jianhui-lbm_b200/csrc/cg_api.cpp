@@ -21,13 +21,13 @@ struct Dev {
   void* p = nullptr;
   size_t bytes = 0;
   ~Dev() {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
   }
   cudaError_t alloc(size_t b) {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
     p = nullptr;
     bytes = b;
-    return b ? cudaMalloc(&p, b) : cudaSuccess;
+    return b ? lbm::dev_alloc(&p, b) : cudaSuccess;
   }
   template <typename T>
   T* as() const {

@@ -199,6 +199,16 @@ cudaError_t d2h_staged(void* dst, const void* src, size_t bytes, cudaStream_t st
 // the process's first field read does not pay for it).
 cudaError_t stage_pool_prime();
 
+// Device memory of the solvers, from the current device's default memory
+// pool with its release threshold raised: what a destroyed solver frees
+// stays mapped in the process, and the next solver of a similar size takes
+// it without new mappings.  dev_free first waits for the device to go idle,
+// as cudaFree does, so that no launch in flight can still use the memory.
+cudaError_t dev_alloc(void** p, size_t bytes);
+void dev_free(void* p);
+// Returns the memory freed solvers left in the pools to the driver.
+cudaError_t dev_pool_trim();
+
 // Mask and box of a single-phase handle (for solvers coupled to it).
 const uint8_t* lbm_internal_mask(lbm_handle* h, int* nx, int* ny, int* nz);
 extern "C" const uint8_t* lbm_cg_internal_mask(lbm_cg_handle* h, int* nx, int* ny, int* nz);

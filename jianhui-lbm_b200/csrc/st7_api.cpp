@@ -17,13 +17,13 @@ struct Mem {
   void* p = nullptr;
   size_t bytes = 0;
   ~Mem() {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
   }
   cudaError_t alloc(size_t b) {
-    if (p) cudaFree(p);
+    if (p) lbm::dev_free(p);
     p = nullptr;
     bytes = b;
-    return b ? cudaMalloc(&p, b) : cudaSuccess;
+    return b ? lbm::dev_alloc(&p, b) : cudaSuccess;
   }
 };
 

@@ -135,4 +135,55 @@ cudaError_t d2h_staged(void* dst, const void* src, size_t bytes, cudaStream_t st
   return e;
 }
 
+namespace {
+std::mutex g_pool_mu;
+std::map<int, bool> g_pool_ready;  // device -> release threshold raised
+}  // namespace
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool_ready[dev]) {
+      cudaMemPool_t pool;
+      e = cudaDeviceGetDefaultMemPool(&pool, dev);
+      if (e != cudaSuccess) return e;
+      unsigned long long keep = ~0ull;  // never return freed memory to the driver while the process runs
+      e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+      g_pool_ready[dev] = true;
+    }
+  }
+  e = cudaMallocAsync(p, bytes, 0);
+  // usable on every stream once the allocation on the legacy stream is done
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  return e;
+}
+
+void dev_free(void* p) {
+  if (!p) return;
+  cudaDeviceSynchronize();
+  cudaFreeAsync(p, 0);
+}
+
+cudaError_t dev_pool_trim() {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  int cur = 0;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return e;
+  for (const auto& kv : g_pool_ready) {
+    if (!kv.second) continue;
+    cudaMemPool_t pool;
+    if ((e = cudaSetDevice(kv.first)) != cudaSuccess) break;
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) break;
+    if ((e = cudaDeviceGetDefaultMemPool(&pool, kv.first)) != cudaSuccess) break;
+    if ((e = cudaMemPoolTrimTo(pool, 0)) != cudaSuccess) break;
+  }
+  const cudaError_t e2 = cudaSetDevice(cur);
+  return e != cudaSuccess ? e : e2;
+}
+
 }  // namespace lbm

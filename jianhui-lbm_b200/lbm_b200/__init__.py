@@ -255,6 +255,7 @@ _SIGNATURES = {
     "lbm_memory": ([C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_double)], C.c_int),
     "lbm_set_table_mode": ([C.c_void_p, C.c_int], C.c_int),
     "lbm_set_lattice": ([C.c_void_p, C.c_double, C.c_double], C.c_int),
+    "lbm_release_cached_memory": ([], C.c_int),
     "lbm_table_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "lbm_reduce_noalloc": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                             C.c_void_p, C.c_void_p], C.c_int),
@@ -357,6 +358,12 @@ def write_checkpoint(flow, prefix, m):
 
 def read_checkpoint(flow, prefix, m):
     _check(lib().lbm_read_checkpoint(flow._h, os.fsencode(prefix), int(m)))
+
+
+def release_cached_memory():
+    """Returns the device memory destroyed solvers left cached in the
+    process's memory pools to the driver (lbm_release_cached_memory)."""
+    _check(lib().lbm_release_cached_memory())
 
 
 def driver_path(name="lbm_sp"):

@@ -67,3 +67,21 @@ def test_populations_read_matches_fields(L):
         f = s.populations().reshape(-1, 19)
         assert f.nbytes > (16 << 20)
         assert np.abs(f[1:].sum(axis=1) - rho[1:]).max() < 1e-5
+
+
+def test_pooled_device_memory_is_reused_and_released(L):
+    """A solver created after another one was destroyed takes its memory
+    from the process's pool (same results), and lbm_release_cached_memory
+    hands the cache back to the driver."""
+    import torch
+
+    m = spheres((96, 96, 96), 0.4, 4.0, seed=12)
+    out = []
+    for _ in range(2):
+        with L.SinglePhase(m, 0.1, (1e-5, 0.0, 0.0), precision="f32") as s:
+            s.step(30)
+            out.append(s.fields())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    free_cached = torch.cuda.mem_get_info()[0]
+    L.release_cached_memory()
+    assert torch.cuda.mem_get_info()[0] >= free_cached
