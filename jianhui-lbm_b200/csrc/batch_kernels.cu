@@ -28,8 +28,12 @@ namespace lbm {
 // their count, chain_grid), and the list kernels fill the entries past the
 // stepping tiles with an empty node range, so a block needs no count of the
 // stepping tiles: the blocks past the list read an empty entry and exit.
+// FP32 at 256 threads: 5 resident blocks per SM in 48 registers without
+// spills, as the single-domain step (16 sphere packs to the stop test:
+// 0.427-0.429 against 0.430-0.432 s at 4 blocks, alternating runs).
 template <Store K, int BS>
-__global__ void __launch_bounds__(BS) batch_step_kernel(BatchStepArgs a, int chain_step) {
+__global__ void __launch_bounds__(BS, (K == Store::F32 && BS == 256) ? 5 : 1)
+    batch_step_kernel(BatchStepArgs a, int chain_step) {
   using T = typename Traits<K>::T;
   using A = typename Traits<K>::A;
   constexpr int kSub = kTile / BS;
